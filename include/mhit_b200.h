@@ -1,0 +1,149 @@
+/*
+ * mhit_b200.h -- C ABI of libmhit_b200.so, a B200 (sm_100a) implementation of the MHIT36
+ * timestep loop (aroccon/MHIT36_mixedp, multi/main.f90:456-1042) on one GPU.
+ *
+ * The reference has no operator API: its hot path is the inline body of `do t=tstart,tfin`
+ * in program main, acting on module arrays (multi/module.f90:51-71) and `param` scalars
+ * (multi/module.f90:1-19, set by multi/readinput.f90:14-49).  Each entry point below names the
+ * block of that loop (or of its setup / I/O) it replaces, so a Fortran host can call it through
+ * ISO_C_BINDING in place of the loop body (see the bind(C) module in
+ * mhit36_mixedp_b200/fortran/mhit_gpu.f90).
+ *
+ * Conventions
+ *   - Arrays cross the boundary as host pointers to x-fastest (nx, ny, nz) float64 arrays with
+ *     no halo: Fortran u(1:nx, 2:ny+1, 2:nz+1) of the reference, the layout of its field files
+ *     (multi/readwrite.f90:28-46).
+ *   - Every function returns an int status: MHIT_OK (0) or a negative MHIT_ERR_* code.  The
+ *     library never calls exit(); mhit_last_error() describes the last failure of the calling
+ *     thread.
+ *   - One context = one box on one GPU with its own CUDA stream.  The library owns all device
+ *     memory; host pointers are borrowed only for the duration of a call.  Calls on one
+ *     context must not overlap; different contexts are independent.
+ */
+#ifndef MHIT_B200_H
+#define MHIT_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MHIT_ABI_VERSION 1
+
+/* status codes */
+#define MHIT_OK 0
+#define MHIT_ERR_ARG (-1)      /* bad argument, unsupported size */
+#define MHIT_ERR_CUDA (-2)     /* CUDA runtime failure (message in mhit_last_error) */
+#define MHIT_ERR_NAN (-3)      /* NaN in the velocity (the reference has no such check) */
+#define MHIT_ERR_CFL (-4)      /* CFL > 7 after a step: the reference stops (multi/main.f90:1006) */
+#define MHIT_ERR_IO (-5)       /* file missing, short read or write */
+#define MHIT_ERR_STATE (-6)    /* call out of order (e.g. particles on a context without them) */
+
+/* Poisson precision (multi/main.f90:844,853-912) */
+#define MHIT_POISSON_FP64 0    /* the intended FP64 solve of the main branch */
+#define MHIT_POISSON_FP32 1    /* this branch: rhs cast to FP32, FP32 transforms, FP32 pressure */
+
+/* Laplacian symbol of the spectral divide */
+#define MHIT_LAP_EXACT 0       /* exact integer k^2, as multi/main.f90:889 */
+#define MHIT_LAP_MODIFIED 1    /* (2-2cos(k dx))/dx^2: discrete divergence ~ round-off */
+
+/* tracer interpolation */
+#define MHIT_INTERP_LINEAR1D 0 /* per-component 1-D linear, multi/particles.f90:114-117 */
+#define MHIT_INTERP_TRILINEAR 1
+
+/* Parameters: the 18 values of input.inp (multi/readinput.f90:14-35) that act on a step,
+ * plus the grid size (compile-time `nx` in multi/module.f90:2) and the feature switches
+ * (compile-time phiflag/partflag in multi/main.f90:55,57). */
+typedef struct mhit_params {
+  int nx, ny, nz;            /* each in {16,32,64,128,192,256,512,1024} */
+  double dt, mu, rho;        /* input.inp lines 7-9 */
+  double f1, f2, f3, k0;     /* ABC forcing, lines 10-13 */
+  double radius, sigma, epsr;/* phase field, lines 14-16 */
+  int phiflag;               /* 1: ACDI phase field on */
+  int partflag;              /* 1: tracers on */
+  int npart;                 /* number of tracers (line 17) */
+  int poisson;               /* MHIT_POISSON_* */
+  int laplacian;             /* MHIT_LAP_* */
+  int interp;                /* MHIT_INTERP_* */
+  int yz_shift;              /* 1: the reference's labelling of y/z planes (forcing/tracers) */
+  int use_graph;             /* 1: replay steps from a captured CUDA graph */
+  int device;                /* CUDA device ordinal */
+} mhit_params;
+
+/* Run control lines of input.inp (multi/readinput.f90:14-19, 34-35). */
+typedef struct mhit_run {
+  int restart, tstart, tfin, dump, inflow, inphi, inpart;
+} mhit_run;
+
+typedef struct mhit_diag {
+  long long nstep;           /* steps taken by this context */
+  double gumax;              /* signed max of u,v,w after the last step (multi/main.f90:1001) */
+  double cfl;                /* gumax*dt/dx (multi/main.f90:1003) */
+  double mean[3];            /* mean of u,v,w removed by the last projection (:967-981) */
+  double maxdiv;             /* max |div u| of the current field (1/dx units) */
+  double ke;                 /* 0.5 <u.u> */
+  double dissipation;        /* 2 nu <S_ij S_ij>, post/compute_diss/main.f90:72-117, solver dx */
+  int flags;                 /* bit0 NaN seen, bit1 CFL > 7 */
+} mhit_diag;
+
+typedef struct mhit_ctx mhit_ctx;
+
+/* Library identification and the last error text of the calling thread. */
+int mhit_abi_version(void);
+const char* mhit_last_error(void);
+
+/* Defaults: nx=ny=nz=64, reference input.inp values (multi/input.inp), FP64 Poisson,
+ * exact k^2, linear1d, yz_shift=1, use_graph=1, device 0. */
+int mhit_params_default(mhit_params* p);
+
+/* Parse an input.inp file (positional, one value per line, Fortran list-directed reals such
+ * as 1.0d0 accepted).  Replaces subroutine readinput (multi/readinput.f90:4-81).  Grid size
+ * and switches in *p are left untouched; run may be NULL. */
+int mhit_read_input(const char* path, mhit_params* p, mhit_run* run);
+
+/* Allocate a context on p->device: fields, spectrum, tables (setup of multi/main.f90:186-310
+ * without MPI/cuDecomp).  Fields start at zero, gumax=1 and the first step is Euler
+ * (multi/main.f90:440-444). */
+int mhit_init(const mhit_params* p, mhit_ctx** out);
+void mhit_destroy(mhit_ctx* ctx);
+
+/* Set the state (replaces the initial-condition block multi/main.f90:322-415 and readfield).
+ * u,v,w: required.  phi: required iff phiflag.  Resets rhs_o, rhsphi_o, the mean, gumax=1 and
+ * the Euler first step. */
+int mhit_upload_fields(mhit_ctx* ctx, const double* u, const double* v, const double* w, const double* phi);
+
+/* Tracer table, column-major (npart, 12) as the reference's part(nplocmax,12)
+ * (multi/particles.f90:11-22): tag, x, y, z, u, v, w, phi, u1, v1, w1, phi1. */
+int mhit_upload_particles(mhit_ctx* ctx, const double* part, int npart);
+int mhit_download_particles(mhit_ctx* ctx, double* part, int npart);
+
+/* Advance nsteps timesteps (one pass of multi/main.f90:456-1007 each).  Returns MHIT_ERR_CFL
+ * or MHIT_ERR_NAN if the device flags were raised by any of these steps (checked once at the
+ * end of the call). */
+int mhit_step(mhit_ctx* ctx, int nsteps);
+
+/* Copy the current state to host arrays (any pointer may be NULL).  u,v,w carry the mean
+ * removal of multi/main.f90:977-981; p is the pressure of the last solve widened to FP64. */
+int mhit_download_fields(mhit_ctx* ctx, double* u, double* v, double* w, double* p, double* phi);
+
+/* Scalars of the last step plus max|div|, KE and dissipation of the current field. */
+int mhit_diagnostics(mhit_ctx* ctx, mhit_diag* d);
+
+/* Field files in the layout of multi/readwrite.f90 (raw float64, x fastest, no header).
+ * fieldn: 1 u, 2 v, 3 w, 4 p, 5 phi (multi/readwrite.f90:21-25).
+ * mhit_write_field writes <dir>/<name>_%08d.dat (writefield, :1-96); mhit_read_field reads
+ * the file at path into field fieldn (readfield/readfield_restart, :107-318). */
+int mhit_write_field(mhit_ctx* ctx, const char* dir, int t, int fieldn);
+int mhit_read_field(mhit_ctx* ctx, const char* path, int fieldn);
+
+/* Measurement helpers (no reference counterpart; the reference times with cpu_time,
+ * multi/main.f90:453,463,1009-1010).  mhit_time_steps runs nsteps on the context stream between
+ * two CUDA events and returns the elapsed milliseconds.  mhit_profile_step runs one step with
+ * an event pair around each kernel launch and returns per-stage milliseconds; names (may be
+ * NULL) receives static strings; *nstages is in/out (capacity / count). */
+int mhit_time_steps(mhit_ctx* ctx, int nsteps, double* ms);
+int mhit_profile_step(mhit_ctx* ctx, double* ms, const char** names, int* nstages);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MHIT_B200_H */

@@ -1,0 +1,250 @@
+"""Python host side of the MHIT36 B200 timestep library.
+
+Mirrors the reference's driver (``program main``, multi/main.f90) on one GPU: the parameters
+are the ``input.inp`` values read by ``readinput`` (multi/readinput.f90:14-35), the state is
+the module arrays of multi/module.f90:51-71 (x-fastest, no halo), field numbers follow
+``writefield``/``readfield`` (1 u, 2 v, 3 w, 4 p, 5 phi; multi/readwrite.f90:21-25), and a
+step is one pass of ``do t=tstart,tfin`` (multi/main.f90:456-1007).  Every call goes through
+the C ABI of ``libmhit_b200.so``; errors come back as ``MhitError`` subclasses carrying the
+library's status code (the reference ``stop``s on CFL > 7, multi/main.f90:1006 -- here that is
+``MhitCFLError``).
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+
+import numpy as np
+
+from . import _lib
+from ._lib import MhitDiag, MhitParams, MhitRun
+
+FIELD_U, FIELD_V, FIELD_W, FIELD_P, FIELD_PHI = 1, 2, 3, 4, 5
+
+
+class MhitError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+class MhitArgError(MhitError):
+    pass
+
+
+class MhitCudaError(MhitError):
+    pass
+
+
+class MhitNaNError(MhitError):
+    pass
+
+
+class MhitCFLError(MhitError):
+    pass
+
+
+class MhitIOError(MhitError):
+    pass
+
+
+class MhitStateError(MhitError):
+    pass
+
+
+_ERRS = {
+    _lib.MHIT_ERR_ARG: MhitArgError,
+    _lib.MHIT_ERR_CUDA: MhitCudaError,
+    _lib.MHIT_ERR_NAN: MhitNaNError,
+    _lib.MHIT_ERR_CFL: MhitCFLError,
+    _lib.MHIT_ERR_IO: MhitIOError,
+    _lib.MHIT_ERR_STATE: MhitStateError,
+}
+
+
+def _check(rc: int):
+    if rc != 0:
+        msg = _lib.load().mhit_last_error()
+        msg = msg.decode() if msg else ""
+        raise _ERRS.get(rc, MhitError)(rc, msg)
+
+
+def _dptr(a):
+    if a is None:
+        return None
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+@dataclasses.dataclass
+class Params:
+    """Step parameters: ``input.inp`` lines 7-17 plus grid size and switches."""
+    nx: int = 64
+    ny: int | None = None
+    nz: int | None = None
+    dt: float = 0.0002
+    mu: float = 0.006
+    rho: float = 1.0
+    f1: float = 1.0
+    f2: float = 1.0
+    f3: float = 1.0
+    k0: float = 2.0
+    radius: float = 0.5
+    sigma: float = 1.0
+    epsr: float = 1.0
+    phiflag: int = 0
+    partflag: int = 0
+    npart: int = 0
+    poisson: str = "fp64"
+    laplacian: str = "exact"
+    interp: str = "linear1d"
+    yz_shift: int = 1
+    use_graph: bool = True
+    device: int = 0
+
+    def __post_init__(self):
+        self.ny = self.ny or self.nx
+        self.nz = self.nz or self.nx
+
+    def to_c(self) -> MhitParams:
+        c = MhitParams()
+        _check(_lib.load().mhit_params_default(ctypes.byref(c)))
+        for f in ("nx", "ny", "nz", "phiflag", "partflag", "npart", "yz_shift", "device"):
+            setattr(c, f, int(getattr(self, f)))
+        for f in ("dt", "mu", "rho", "f1", "f2", "f3", "k0", "radius", "sigma", "epsr"):
+            setattr(c, f, float(getattr(self, f)))
+        c.poisson = _lib.POISSON[self.poisson]
+        c.laplacian = _lib.LAPLACIAN[self.laplacian]
+        c.interp = _lib.INTERP[self.interp]
+        c.use_graph = int(bool(self.use_graph))
+        return c
+
+    @property
+    def shape(self):
+        """numpy shape of a field: (nz, ny, nx) C order == Fortran (nx, ny, nz)."""
+        return (self.nz, self.ny, self.nx)
+
+
+def read_input(path: str, **overrides):
+    """Parse an ``input.inp`` (multi/readinput.f90:14-35) through the library.
+
+    Returns ``(Params, run)`` where run holds restart/tstart/tfin/dump/inflow/inphi/inpart.
+    Grid size and switches come from ``overrides`` (they are compile-time in the reference).
+    """
+    p = Params(**overrides)
+    c = p.to_c()
+    r = MhitRun()
+    _check(_lib.load().mhit_read_input(path.encode(), ctypes.byref(c), ctypes.byref(r)))
+    for f in ("dt", "mu", "rho", "f1", "f2", "f3", "k0", "radius", "sigma", "epsr"):
+        setattr(p, f, getattr(c, f))
+    p.npart = c.npart
+    run = {f: getattr(r, f) for f, _ in MhitRun._fields_}
+    return p, run
+
+
+class Solver:
+    """One box on one GPU: ``init`` -> ``upload`` -> ``step`` ... -> ``download``."""
+
+    def __init__(self, params: Params):
+        self.params = params
+        self._lib = _lib.load()
+        self._ctx = ctypes.c_void_p()
+        self._cp = params.to_c()
+        _check(self._lib.mhit_init(ctypes.byref(self._cp), ctypes.byref(self._ctx)))
+
+    # -------------------------------------------------------------- lifecycle
+    def close(self):
+        if self._ctx:
+            self._lib.mhit_destroy(self._ctx)
+            self._ctx = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _field(self, a, name):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        if a.shape != self.params.shape:
+            raise MhitArgError(_lib.MHIT_ERR_ARG, f"{name} has shape {a.shape}, expected {self.params.shape}")
+        return a
+
+    # -------------------------------------------------------------- state
+    def upload(self, u, v, w, phi=None):
+        """Set u, v, w (and phi): the fresh-start block of multi/main.f90:322-415."""
+        u, v, w = self._field(u, "u"), self._field(v, "v"), self._field(w, "w")
+        if phi is not None:
+            phi = self._field(phi, "phi")
+        _check(self._lib.mhit_upload_fields(self._ctx, _dptr(u), _dptr(v), _dptr(w), _dptr(phi)))
+
+    def upload_particles(self, part):
+        """Tracer table (npart, 12): tag, x, y, z, u, v, w, phi, u1, v1, w1, phi1."""
+        part = np.asfortranarray(part, dtype=np.float64)
+        if part.ndim != 2 or part.shape[1] != 12:
+            raise MhitArgError(_lib.MHIT_ERR_ARG, "particle table must be (npart, 12)")
+        self._np = part.shape[0]
+        _check(self._lib.mhit_upload_particles(self._ctx, _dptr(part), part.shape[0]))
+
+    def download_particles(self):
+        n = getattr(self, "_np", 0)
+        out = np.zeros((n, 12), dtype=np.float64, order="F")
+        _check(self._lib.mhit_download_particles(self._ctx, _dptr(out), n))
+        return out
+
+    def step(self, nsteps: int = 1):
+        """Advance nsteps (Euler on the first step after upload, then AB2)."""
+        _check(self._lib.mhit_step(self._ctx, int(nsteps)))
+
+    def download(self, fields=("u", "v", "w", "p", "phi")):
+        shp = self.params.shape
+        out = {}
+        ptrs = []
+        for f in ("u", "v", "w", "p", "phi"):
+            if f in fields and (f != "phi" or self.params.phiflag):
+                out[f] = np.empty(shp, dtype=np.float64)
+                ptrs.append(_dptr(out[f]))
+            else:
+                ptrs.append(None)
+        _check(self._lib.mhit_download_fields(self._ctx, *ptrs))
+        return out
+
+    def diagnostics(self) -> dict:
+        d = MhitDiag()
+        _check(self._lib.mhit_diagnostics(self._ctx, ctypes.byref(d)))
+        return {
+            "nstep": d.nstep, "gumax": d.gumax, "cfl": d.cfl, "mean": tuple(d.mean),
+            "maxdiv": d.maxdiv, "ke": d.ke, "dissipation": d.dissipation, "flags": d.flags,
+        }
+
+    # -------------------------------------------------------------- field files
+    def writefield(self, outdir: str, t: int, fieldn: int):
+        """``writefield(t, fieldn)``: <outdir>/{u,v,w,p,phi}_%08d.dat (multi/readwrite.f90:1-96)."""
+        _check(self._lib.mhit_write_field(self._ctx, outdir.encode(), int(t), int(fieldn)))
+
+    def readfield(self, path: str, fieldn: int):
+        """``readfield(fieldn)`` / ``readfield_restart`` (multi/readwrite.f90:107-318)."""
+        _check(self._lib.mhit_read_field(self._ctx, path.encode(), int(fieldn)))
+
+    # -------------------------------------------------------------- measurement
+    def time_steps(self, nsteps: int) -> float:
+        ms = ctypes.c_double()
+        _check(self._lib.mhit_time_steps(self._ctx, int(nsteps), ctypes.byref(ms)))
+        return ms.value
+
+    def profile_step(self) -> dict:
+        cap = 16
+        ms = (ctypes.c_double * cap)()
+        names = (ctypes.c_char_p * cap)()
+        n = ctypes.c_int(cap)
+        _check(self._lib.mhit_profile_step(self._ctx, ms, names, ctypes.byref(n)))
+        return {names[i].decode(): ms[i] for i in range(n.value) if ms[i] >= 0}
+
+
+def abi_version() -> int:
+    return _lib.load().mhit_abi_version()

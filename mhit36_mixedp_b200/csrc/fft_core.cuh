@@ -1,0 +1,200 @@
+// Shared-memory mixed-radix Stockham FFT over a tile of B independent columns.
+//
+// Replaces the cuFFT 1-D plans of the reference (multi/main.f90:187-205, executed at
+// :853,860,865,901,906,912).  Written from the DFT definition: a decimation-in-time
+// Stockham autosort (one radix-R register butterfly per thread per stage, in-place in shared
+// memory with a barrier between the read and the write half of each stage).
+//
+// Tile layout in shared memory: element (n, b) -- n along the transform, b the column --
+// lives at n*B + (b ^ (n % B)).  A row of B elements is exactly 128 bytes (B = 8 double2 or
+// 16 float2), so a warp touching whole rows is conflict-free, and the XOR swizzle keeps a
+// warp walking down one column (the x-direction loads) conflict-free as well.
+#pragma once
+#include "common.cuh"
+
+namespace mhit {
+
+template <int N> struct Radix;  // radix schedule per transform length
+template <> struct Radix<8>    { static constexpr int ns = 1; static constexpr int r[3] = {8, 0, 0}; };
+template <> struct Radix<16>   { static constexpr int ns = 2; static constexpr int r[3] = {4, 4, 0}; };
+template <> struct Radix<32>   { static constexpr int ns = 2; static constexpr int r[3] = {4, 8, 0}; };
+template <> struct Radix<64>   { static constexpr int ns = 2; static constexpr int r[3] = {8, 8, 0}; };
+template <> struct Radix<96>   { static constexpr int ns = 3; static constexpr int r[3] = {3, 4, 8}; };
+template <> struct Radix<128>  { static constexpr int ns = 2; static constexpr int r[3] = {8, 16, 0}; };
+template <> struct Radix<192>  { static constexpr int ns = 3; static constexpr int r[3] = {3, 8, 8}; };
+template <> struct Radix<256>  { static constexpr int ns = 2; static constexpr int r[3] = {16, 16, 0}; };
+template <> struct Radix<512>  { static constexpr int ns = 3; static constexpr int r[3] = {8, 8, 8}; };
+template <> struct Radix<1024> { static constexpr int ns = 3; static constexpr int r[3] = {8, 8, 16}; };
+
+template <int N> __host__ __device__ constexpr int max_radix() {
+  int m = 0;
+  for (int s = 0; s < Radix<N>::ns; ++s) m = Radix<N>::r[s] > m ? Radix<N>::r[s] : m;
+  return m;
+}
+
+// threads per tile: one butterfly of the largest radix per thread, clamped to [64, 512]
+template <int N, int B> __host__ __device__ constexpr int fft_threads() {
+  int t = N / max_radix<N>() * B;
+  return t < 64 ? 64 : (t > 512 ? 512 : t);
+}
+
+template <int B> __device__ __forceinline__ int sw(int n, int b) { return n * B + (b ^ (n & (B - 1))); }
+
+// ---------------------------------------------------------------- register butterflies
+template <typename T, bool INV> __device__ __forceinline__ void dft2(Cx<T>* a) {
+  Cx<T> t = a[0];
+  a[0] = t + a[1];
+  a[1] = t - a[1];
+}
+
+template <typename T, bool INV> __device__ __forceinline__ void dft3(Cx<T>* a) {
+  const T h = (T)0.5;
+  const T s3 = (T)0.86602540378443864676372317075294;  // sqrt(3)/2
+  Cx<T> s = a[1] + a[2];
+  Cx<T> d = a[1] - a[2];
+  Cx<T> m = a[0] - scale(s, h);
+  // (-+ i sqrt(3)/2) * d
+  Cx<T> r = INV ? cx<T>(-s3 * d.y, s3 * d.x) : cx<T>(s3 * d.y, -s3 * d.x);
+  a[0] = a[0] + s;
+  a[1] = m + r;
+  a[2] = m - r;
+}
+
+template <typename T, bool INV> __device__ __forceinline__ void dft4(Cx<T>* a) {
+  Cx<T> t0 = a[0] + a[2];
+  Cx<T> t1 = a[0] - a[2];
+  Cx<T> t2 = a[1] + a[3];
+  Cx<T> t3 = mul_mi<T, INV>(a[1] - a[3]);
+  a[0] = t0 + t2;
+  a[2] = t0 - t2;
+  a[1] = t1 + t3;
+  a[3] = t1 - t3;
+}
+
+template <typename T, bool INV> __device__ __forceinline__ void dft8(Cx<T>* a) {
+  const T r2 = (T)0.70710678118654752440084436210485;
+  Cx<T> e[4] = {a[0], a[2], a[4], a[6]};
+  Cx<T> o[4] = {a[1], a[3], a[5], a[7]};
+  dft4<T, INV>(e);
+  dft4<T, INV>(o);
+  // o[k] *= w8^k, w8 = exp(-+ 2 pi i / 8)
+  o[1] = INV ? cx<T>(r2 * (o[1].x - o[1].y), r2 * (o[1].x + o[1].y))
+             : cx<T>(r2 * (o[1].x + o[1].y), r2 * (o[1].y - o[1].x));
+  o[2] = mul_mi<T, INV>(o[2]);
+  o[3] = INV ? cx<T>(-r2 * (o[3].x + o[3].y), r2 * (o[3].x - o[3].y))
+             : cx<T>(r2 * (o[3].y - o[3].x), -r2 * (o[3].x + o[3].y));
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    a[k] = e[k] + o[k];
+    a[k + 4] = e[k] - o[k];
+  }
+}
+
+template <typename T, bool INV> __device__ __forceinline__ void dft16(Cx<T>* a) {
+  // 16 = 4 x 4: columns n1, rows n2; y[k2 + 4 k1]
+  const T c1 = (T)0.92387953251128675612818318939679;  // cos(pi/8)
+  const T s1 = (T)0.38268343236508977172845998403040;  // sin(pi/8)
+  const T r2 = (T)0.70710678118654752440084436210485;
+  Cx<T> b[4][4];
+#pragma unroll
+  for (int n1 = 0; n1 < 4; ++n1) {
+    Cx<T> t[4] = {a[n1], a[n1 + 4], a[n1 + 8], a[n1 + 12]};
+    dft4<T, INV>(t);
+#pragma unroll
+    for (int k2 = 0; k2 < 4; ++k2) b[n1][k2] = t[k2];
+  }
+  // twiddles w16^(n1*k2); for the inverse use the conjugate
+  const T sg = INV ? (T)1 : (T)-1;
+  auto tw = [&](Cx<T> v, T c, T s) { return cx<T>(v.x * c - v.y * (sg * s), v.x * (sg * s) + v.y * c); };
+  b[1][1] = tw(b[1][1], c1, s1);
+  b[1][2] = tw(b[1][2], r2, r2);
+  b[1][3] = tw(b[1][3], s1, c1);
+  b[2][1] = tw(b[2][1], r2, r2);
+  b[2][2] = mul_mi<T, INV>(b[2][2]);
+  b[2][3] = tw(b[2][3], -r2, r2);
+  b[3][1] = tw(b[3][1], s1, c1);
+  b[3][2] = tw(b[3][2], -r2, r2);
+  b[3][3] = tw(b[3][3], -c1, -s1);
+#pragma unroll
+  for (int k2 = 0; k2 < 4; ++k2) {
+    Cx<T> t[4] = {b[0][k2], b[1][k2], b[2][k2], b[3][k2]};
+    dft4<T, INV>(t);
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) a[k2 + 4 * k1] = t[k1];
+  }
+}
+
+template <typename T, bool INV, int R> __device__ __forceinline__ void dftR(Cx<T>* a) {
+  if constexpr (R == 2) dft2<T, INV>(a);
+  else if constexpr (R == 3) dft3<T, INV>(a);
+  else if constexpr (R == 4) dft4<T, INV>(a);
+  else if constexpr (R == 8) dft8<T, INV>(a);
+  else if constexpr (R == 16) dft16<T, INV>(a);
+}
+
+// ---------------------------------------------------------------- one Stockham stage
+// tw: table of exp(-2 pi i m / L) for m in [0, L); twstride = L / N.
+template <typename T, int N, int B, int NT, int R, bool INV>
+__device__ __forceinline__ void stockham_stage(Cx<T>* s, const Cx<T>* __restrict__ tw, int twstride, int p) {
+  constexpr int NB = N / R * B;
+  constexpr int BPT = (NB + NT - 1) / NT;
+  Cx<T> a[BPT][R];
+  const int tid = threadIdx.x;
+#pragma unroll
+  for (int m = 0; m < BPT; ++m) {
+    const int q = tid + m * NT;
+    if (NB % NT == 0 || q < NB) {
+      const int b = q % B, t = q / B;
+#pragma unroll
+      for (int r = 0; r < R; ++r) a[m][r] = s[sw<B>(t + r * (N / R), b)];
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int m = 0; m < BPT; ++m) {
+    const int q = tid + m * NT;
+    if (NB % NT == 0 || q < NB) {
+      const int b = q % B, t = q / B;
+      const int k = t % p;
+      if (p > 1) {
+        // w^(r k) with w = exp(-+ 2 pi i / (p R)); table index r*k*(N/(pR))*twstride
+        const int step = (N / (p * R)) * twstride;
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+          Cx<T> w = tw[r * k * step];
+          if (INV) w.y = -w.y;
+          a[m][r] = cmul(a[m][r], w);
+        }
+      }
+      dftR<T, INV, R>(a[m]);
+      const int j = (t / p) * p * R + k;
+#pragma unroll
+      for (int r = 0; r < R; ++r) s[sw<B>(j + r * p, b)] = a[m][r];
+    }
+  }
+  __syncthreads();
+}
+
+// Full transform of the N x B tile in s (unnormalised in both directions, as cuFFT).
+// Caller must __syncthreads() before (tile loaded); returns after a barrier.
+template <typename T, int N, int B, int NT, bool INV>
+__device__ __forceinline__ void fft_tile(Cx<T>* s, const Cx<T>* __restrict__ tw, int twstride) {
+  constexpr int NS = Radix<N>::ns;
+  int p = 1;
+  if constexpr (NS >= 1) {
+    constexpr int R = Radix<N>::r[0];
+    stockham_stage<T, N, B, NT, R, INV>(s, tw, twstride, p);
+    p *= R;
+  }
+  if constexpr (NS >= 2) {
+    constexpr int R = Radix<N>::r[1];
+    stockham_stage<T, N, B, NT, R, INV>(s, tw, twstride, p);
+    p *= R;
+  }
+  if constexpr (NS >= 3) {
+    constexpr int R = Radix<N>::r[2];
+    stockham_stage<T, N, B, NT, R, INV>(s, tw, twstride, p);
+  }
+}
+
+}  // namespace mhit

@@ -1,0 +1,225 @@
+// Projection and the per-step reductions: multi/main.f90:942-1007.
+//
+// k_correct     u** = u* - dt/rho (p(i) - p(i-1)) dxi (and v, w along y, z; :953-955) in place,
+//               with per-block partial sums (mean, :956-958) and maxima (:998-1000).
+// k_finalize    one block reduces the partials in a fixed order (run-to-run deterministic),
+//               writes mean = sum/nx/ny/nz (:967-969), gumax = max over components of
+//               (max - mean) -- equal to maxval(u - mean) because rounding is monotonic --,
+//               cfl = gumax dt dxi (:1003) and the NaN / CFL>7 flags (:1006).
+// The mean is not subtracted here: the next step's kernels and the download subtract it on
+// read, which saves a full read+write pass of u, v, w.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace mhit {
+
+constexpr int CNT = 256;
+
+template <typename T>
+__global__ void __launch_bounds__(CNT) k_correct(CorrectArgs a) {
+  const Geo& g = a.g;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const size_t ntot = (size_t)nx * ny * nz;
+  const T* __restrict__ p = static_cast<const T*>(a.p);
+  const double cc = g.dt / g.rho, dxi = g.dxi;
+  double su = 0.0, sv = 0.0, sw = 0.0;
+  double mu = -INFINITY, mv = -INFINITY, mw = -INFINITY;
+  const size_t stride = (size_t)gridDim.x * CNT;
+  for (size_t c = (size_t)blockIdx.x * CNT + threadIdx.x; c < ntot; c += stride) {
+    const int i = (int)(c % nx);
+    const size_t r = c / nx;
+    const int j = (int)(r % ny), k = (int)(r / ny);
+    const double pc = (double)p[c];
+    const double pxm = (double)p[c - i + wrapm(i, nx)];
+    const double pym = (double)p[lin(i, wrapm(j, ny), k, nx, ny)];
+    const double pzm = (double)p[lin(i, j, wrapm(k, nz), nx, ny)];
+    const double uu = a.u[c] - cc * (pc - pxm) * dxi;
+    const double vv = a.v[c] - cc * (pc - pym) * dxi;
+    const double ww = a.w[c] - cc * (pc - pzm) * dxi;
+    a.u[c] = uu;
+    a.v[c] = vv;
+    a.w[c] = ww;
+    su += uu;
+    sv += vv;
+    sw += ww;
+    mu = fmax(mu, uu);
+    mv = fmax(mv, vv);
+    mw = fmax(mw, ww);
+  }
+  // block reduction (fixed tree)
+  __shared__ double red[6][CNT / 32];
+  double vals[6] = {su, sv, sw, mu, mv, mw};
+#pragma unroll
+  for (int q = 0; q < 6; ++q) {
+    double x = vals[q];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double y = __shfl_down_sync(0xffffffffu, x, o);
+      x = q < 3 ? x + y : fmax(x, y);
+    }
+    if ((threadIdx.x & 31) == 0) red[q][threadIdx.x >> 5] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    const int q = threadIdx.x;
+    double x = red[q][0];
+    for (int wv = 1; wv < CNT / 32; ++wv) x = q < 3 ? x + red[q][wv] : fmax(x, red[q][wv]);
+    a.partials[(size_t)blockIdx.x * 6 + q] = x;
+  }
+}
+
+__global__ void __launch_bounds__(1024) k_finalize(const double* __restrict__ partials, int nblocks, Geo g,
+                                                   DevScalars* sc) {
+  __shared__ double red[6][32];
+  double vals[6] = {0.0, 0.0, 0.0, -INFINITY, -INFINITY, -INFINITY};
+  for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+      const double x = partials[(size_t)b * 6 + q];
+      vals[q] = q < 3 ? vals[q] + x : fmax(vals[q], x);
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < 6; ++q) {
+    double x = vals[q];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double y = __shfl_down_sync(0xffffffffu, x, o);
+      x = q < 3 ? x + y : fmax(x, y);
+    }
+    if ((threadIdx.x & 31) == 0) red[q][threadIdx.x >> 5] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double r[6];
+    const int nw = (blockDim.x + 31) / 32;
+    for (int q = 0; q < 6; ++q) {
+      double x = red[q][0];
+      for (int wv = 1; wv < nw; ++wv) x = q < 3 ? x + red[q][wv] : fmax(x, red[q][wv]);
+      r[q] = x;
+    }
+    const double nxd = g.nx, nyd = g.ny, nzd = g.nz;
+    int flag = 0;
+    for (int q = 0; q < 3; ++q) {
+      const double m = r[q] / nxd / nyd / nzd;  // multi/main.f90:967-969
+      sc->mean[q] = m;
+      r[3 + q] = r[3 + q] - m;
+      if (!(r[q] == r[q])) flag |= 1;
+    }
+    const double gumax = fmax(r[5], fmax(r[3], r[4]));  // :1001
+    sc->gumax = gumax;
+    sc->cfl = gumax * g.dt * g.dxi;
+    if (!(gumax == gumax)) flag |= 1;
+    if (sc->cfl > 7.0) flag |= 2;  // :1006
+    sc->flag |= flag;
+  }
+}
+
+int correct_blocks(const Geo& g) {
+  const size_t n = (size_t)g.nx * g.ny * g.nz;
+  size_t b = (n + CNT * 4 - 1) / (CNT * 4);
+  const size_t cap = 148 * 8;
+  return (int)(b < cap ? (b < 1 ? 1 : b) : cap);
+}
+
+cudaError_t launch_correct(const CorrectArgs& a, cudaStream_t st) {
+  if (a.fp32) k_correct<float><<<a.nblocks, CNT, 0, st>>>(a);
+  else k_correct<double><<<a.nblocks, CNT, 0, st>>>(a);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_finalize<<<1, 1024, 0, st>>>(a.partials, a.nblocks, a.g, a.sc);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------ diagnostics
+// max |div u| (the operator of :841-843 without rho/dt), kinetic energy, and the dissipation
+// 2 nu <S_ij S_ij> with central differences (post/compute_diss/main.f90:72-117).
+__global__ void __launch_bounds__(CNT) k_diag(DiagArgs a) {
+  const Geo& g = a.g;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const size_t ntot = (size_t)nx * ny * nz;
+  const double mu_ = a.sc->mean[0], mv_ = a.sc->mean[1], mw_ = a.sc->mean[2];
+  const double* __restrict__ U = a.u;
+  const double* __restrict__ V = a.v;
+  const double* __restrict__ W = a.w;
+  const double dxi = g.dxi, h = 0.5 / a.dxd;
+  double mdiv = 0.0, ke = 0.0, ss = 0.0;
+  const size_t stride = (size_t)gridDim.x * CNT;
+  for (size_t c = (size_t)blockIdx.x * CNT + threadIdx.x; c < ntot; c += stride) {
+    const int i = (int)(c % nx);
+    const size_t r = c / nx;
+    const int j = (int)(r % ny), k = (int)(r / ny);
+    const int ip = wrapp(i, nx), im = wrapm(i, nx), jp = wrapp(j, ny), jm = wrapm(j, ny);
+    const int kp = wrapp(k, nz), km = wrapm(k, nz);
+#define F(A, m, ii, jj, kk) (__ldg(A + lin(ii, jj, kk, nx, ny)) - m)
+    const double u0 = F(U, mu_, i, j, k), v0 = F(V, mv_, i, j, k), w0 = F(W, mw_, i, j, k);
+    const double div = (F(U, mu_, ip, j, k) - u0) * dxi + (F(V, mv_, i, jp, k) - v0) * dxi +
+                       (F(W, mw_, i, j, kp) - w0) * dxi;
+    mdiv = fmax(mdiv, fabs(div));
+    ke += u0 * u0 + v0 * v0 + w0 * w0;
+    const double dudx = (F(U, mu_, ip, j, k) - F(U, mu_, im, j, k)) * h;
+    const double dudy = (F(U, mu_, i, jp, k) - F(U, mu_, i, jm, k)) * h;
+    const double dudz = (F(U, mu_, i, j, kp) - F(U, mu_, i, j, km)) * h;
+    const double dvdx = (F(V, mv_, ip, j, k) - F(V, mv_, im, j, k)) * h;
+    const double dvdy = (F(V, mv_, i, jp, k) - F(V, mv_, i, jm, k)) * h;
+    const double dvdz = (F(V, mv_, i, j, kp) - F(V, mv_, i, j, km)) * h;
+    const double dwdx = (F(W, mw_, ip, j, k) - F(W, mw_, im, j, k)) * h;
+    const double dwdy = (F(W, mw_, i, jp, k) - F(W, mw_, i, jm, k)) * h;
+    const double dwdz = (F(W, mw_, i, j, kp) - F(W, mw_, i, j, km)) * h;
+#undef F
+    const double s12 = 0.5 * (dudy + dvdx), s13 = 0.5 * (dudz + dwdx), s23 = 0.5 * (dvdz + dwdy);
+    ss += dudx * dudx + dvdy * dvdy + dwdz * dwdz + 2.0 * (s12 * s12 + s13 * s13 + s23 * s23);
+  }
+  __shared__ double red[3][CNT / 32];
+  double vals[3] = {mdiv, ke, ss};
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    double x = vals[q];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double y = __shfl_down_sync(0xffffffffu, x, o);
+      x = q == 0 ? fmax(x, y) : x + y;
+    }
+    if ((threadIdx.x & 31) == 0) red[q][threadIdx.x >> 5] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    const int q = threadIdx.x;
+    double x = red[q][0];
+    for (int wv = 1; wv < CNT / 32; ++wv) x = q == 0 ? fmax(x, red[q][wv]) : x + red[q][wv];
+    a.partials[(size_t)blockIdx.x * 4 + q] = x;
+  }
+}
+
+__global__ void k_diag_finalize(const double* __restrict__ partials, int nblocks, Geo g, double nu, DevScalars* sc) {
+  if (threadIdx.x != 0) return;
+  double mdiv = 0.0, ke = 0.0, ss = 0.0;
+  for (int b = 0; b < nblocks; ++b) {
+    mdiv = fmax(mdiv, partials[(size_t)b * 4 + 0]);
+    ke += partials[(size_t)b * 4 + 1];
+    ss += partials[(size_t)b * 4 + 2];
+  }
+  const double n = (double)g.nx * g.ny * g.nz;
+  sc->diag[0] = mdiv;
+  sc->diag[1] = 0.5 * ke / n;
+  sc->diag[2] = 2.0 * nu * ss / n;
+}
+
+cudaError_t launch_diag(const DiagArgs& a, cudaStream_t st) {
+  k_diag<<<a.nblocks, CNT, 0, st>>>(a);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_diag_finalize<<<1, 32, 0, st>>>(a.partials, a.nblocks, a.g, a.nu, a.sc);
+  return cudaGetLastError();
+}
+
+__global__ void k_fill(double* p, size_t n, double v) {
+  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) p[c] = v;
+}
+
+cudaError_t launch_fill(double* p, size_t n, double v, cudaStream_t st) {
+  k_fill<<<148 * 4, 256, 0, st>>>(p, n, v);
+  return cudaGetLastError();
+}
+
+}  // namespace mhit

@@ -1,0 +1,351 @@
+// Pressure Poisson solve on one GPU: multi/main.f90:833-923 without cuFFT or cuDecomp.
+//
+//   k_div_fftx   rho/dt * div(u*) in FP64 (:833-843), cast to the Poisson precision (:844),
+//                and the x-direction R2C transform (:853) of a tile of B x-lines, fused.
+//   k_fft_cols   C2C transform along y (:860, :906) or along z fused with the spectral divide
+//                -rhs/k^2/(nx ny nz), zero mode := 0, and the inverse z transform
+//                (:865, :883-896, :901).  The transposes of :858,863,904,909 disappear: a
+//                tile is B adjacent kx columns of the x-fastest spectrum, read with stride.
+//   k_fftx_inv   C2R along x (:912) into the pressure array (FP32 or FP64).
+//
+// Spectrum layout: [z][y][kx], kx fastest, row pitch padded to a multiple of 16 complex so
+// every tile row starts on a 128-byte boundary.  Half-length real transforms: the x line of
+// nx reals is packed as nx/2 complex (even + i*odd), transformed, and untangled with the
+// exp(-2 pi i k/nx) twiddles (and the mirror image for C2R).
+#include "common.cuh"
+#include "fft_core.cuh"
+#include "kernels.h"
+
+namespace mhit {
+
+template <typename T> struct Tile;
+template <> struct Tile<double> { static constexpr int B = 8; };
+template <> struct Tile<float> { static constexpr int B = 16; };
+
+template <typename T> __device__ __forceinline__ void store2(T* p, T a, T b);
+template <> __device__ __forceinline__ void store2<double>(double* p, double a, double b) {
+  *reinterpret_cast<double2*>(p) = make_double2(a, b);
+}
+template <> __device__ __forceinline__ void store2<float>(float* p, float a, float b) {
+  *reinterpret_cast<float2*>(p) = make_float2(a, b);
+}
+
+constexpr int XPASS_THREADS = 256;
+
+// ------------------------------------------------------------------ forward x + divergence
+template <typename T, int M>
+__global__ void __launch_bounds__(XPASS_THREADS)
+k_div_fftx(const double* __restrict__ u, const double* __restrict__ v, const double* __restrict__ w,
+           Cx<T>* __restrict__ spec, const Cx<T>* __restrict__ twx, Geo g, double cdiv) {
+  constexpr int B = Tile<T>::B;
+  constexpr int NT = XPASS_THREADS;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  Cx<T>* s = reinterpret_cast<Cx<T>*>(smraw);
+  const int nx = 2 * M, ny = g.ny, nz = g.nz;
+  const int nlines = ny * nz;
+  const int line0 = blockIdx.x * B;
+
+  for (int e = threadIdx.x; e < M * B; e += NT) {
+    const int b = e / M, n = e - b * M;
+    const int line = line0 + b;
+    Cx<T> z;
+    z.x = (T)0;
+    z.y = (T)0;
+    if (line < nlines) {
+      const int k = line / ny, j = line - k * ny;
+      const int jp = wrapp(j, ny), kp = wrapp(k, nz);
+      const int i = 2 * n;
+      const size_t row = ((size_t)k * ny + j) * nx;
+      const size_t rowy = ((size_t)k * ny + jp) * nx;
+      const size_t rowz = ((size_t)kp * ny + j) * nx;
+      const double2 uu = __ldg(reinterpret_cast<const double2*>(u + row + i));
+      const double un = __ldg(u + row + (i + 2 == nx ? 0 : i + 2));
+      const double2 vv = __ldg(reinterpret_cast<const double2*>(v + row + i));
+      const double2 vp = __ldg(reinterpret_cast<const double2*>(v + rowy + i));
+      const double2 ww = __ldg(reinterpret_cast<const double2*>(w + row + i));
+      const double2 wp = __ldg(reinterpret_cast<const double2*>(w + rowz + i));
+      // multi/main.f90:841-843, summed in the reference's order
+      double r0 = cdiv * (uu.y - uu.x);
+      r0 = r0 + cdiv * (vp.x - vv.x);
+      r0 = r0 + cdiv * (wp.x - ww.x);
+      double r1 = cdiv * (un - uu.y);
+      r1 = r1 + cdiv * (vp.y - vv.y);
+      r1 = r1 + cdiv * (wp.y - ww.y);
+      z.x = (T)r0;
+      z.y = (T)r1;
+    }
+    s[sw<B>(n, b)] = z;
+  }
+  __syncthreads();
+  fft_tile<T, M, B, NT, false>(s, twx, 2);
+
+  // untangle: X[k] = (Z[k] + Z*[M-k])/2 - i/2 W^k (Z[k] - Z*[M-k]),  W = exp(-2 pi i/nx)
+  for (int e = threadIdx.x; e < (M / 2 + 1) * B; e += NT) {
+    const int kk = e / B, b = e - kk * B;
+    if (kk == 0) {
+      const Cx<T> z0 = s[sw<B>(0, b)];
+      s[sw<B>(0, b)] = cx<T>(z0.x + z0.y, (T)0);
+      s[sw<B>(M, b)] = cx<T>(z0.x - z0.y, (T)0);
+    } else {
+      const Cx<T> zk = s[sw<B>(kk, b)];
+      const Cx<T> zm = s[sw<B>(M - kk, b)];
+      const T h = (T)0.5;
+      {
+        const Cx<T> a = scale(zk + conj(zm), h);
+        const Cx<T> d = zk - conj(zm);
+        const Cx<T> t = cmul(twx[kk], d);  // W^k d
+        s[sw<B>(kk, b)] = cx<T>(a.x - h * t.y, a.y + h * t.x);  // a - i/2 t
+      }
+      if (kk != M - kk) {
+        const Cx<T> a = scale(zm + conj(zk), h);
+        const Cx<T> d = zm - conj(zk);
+        const Cx<T> t = cmul(twx[M - kk], d);
+        s[sw<B>(M - kk, b)] = cx<T>(a.x - h * t.y, a.y + h * t.x);
+      }
+    }
+  }
+  __syncthreads();
+  const int pitch = g.pitch;
+  for (int e = threadIdx.x; e < (M + 1) * B; e += NT) {
+    const int b = e / (M + 1), kx = e - b * (M + 1);
+    const int line = line0 + b;
+    if (line < nlines) spec[(size_t)line * pitch + kx] = s[sw<B>(kx, b)];
+  }
+}
+
+// ------------------------------------------------------------------ inverse x -> pressure
+template <typename T, int M>
+__global__ void __launch_bounds__(XPASS_THREADS)
+k_fftx_inv(const Cx<T>* __restrict__ spec, T* __restrict__ p, const Cx<T>* __restrict__ twx, Geo g) {
+  constexpr int B = Tile<T>::B;
+  constexpr int NT = XPASS_THREADS;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  Cx<T>* s = reinterpret_cast<Cx<T>*>(smraw);
+  const int nx = 2 * M;
+  const int nlines = g.ny * g.nz;
+  const int line0 = blockIdx.x * B;
+  const int pitch = g.pitch;
+  for (int e = threadIdx.x; e < (M + 1) * B; e += NT) {
+    const int b = e / (M + 1), kx = e - b * (M + 1);
+    const int line = line0 + b;
+    Cx<T> z;
+    z.x = (T)0;
+    z.y = (T)0;
+    if (line < nlines) z = spec[(size_t)line * pitch + kx];
+    s[sw<B>(kx, b)] = z;
+  }
+  __syncthreads();
+  // Z[k] = (X[k] + X*[M-k]) + i W^-k (X[k] - X*[M-k]); imaginary parts of X[0], X[M] ignored
+  for (int e = threadIdx.x; e < (M / 2 + 1) * B; e += NT) {
+    const int kk = e / B, b = e - kk * B;
+    if (kk == 0) {
+      const T a = s[sw<B>(0, b)].x, c = s[sw<B>(M, b)].x;
+      s[sw<B>(0, b)] = cx<T>(a + c, a - c);
+    } else {
+      const Cx<T> xk = s[sw<B>(kk, b)];
+      const Cx<T> xm = s[sw<B>(M - kk, b)];
+      {
+        const Cx<T> a = xk + conj(xm);
+        const Cx<T> d = xk - conj(xm);
+        const Cx<T> t = cmul(conj(twx[kk]), d);
+        s[sw<B>(kk, b)] = cx<T>(a.x - t.y, a.y + t.x);
+      }
+      if (kk != M - kk) {
+        const Cx<T> a = xm + conj(xk);
+        const Cx<T> d = xm - conj(xk);
+        const Cx<T> t = cmul(conj(twx[M - kk]), d);
+        s[sw<B>(M - kk, b)] = cx<T>(a.x - t.y, a.y + t.x);
+      }
+    }
+  }
+  __syncthreads();
+  fft_tile<T, M, B, NT, true>(s, twx, 2);
+  for (int e = threadIdx.x; e < M * B; e += NT) {
+    const int b = e / M, n = e - b * M;
+    const int line = line0 + b;
+    if (line < nlines) {
+      const Cx<T> z = s[sw<B>(n, b)];
+      store2<T>(p + (size_t)line * nx + 2 * n, z.x, z.y);
+    }
+  }
+}
+
+// ------------------------------------------------------------------ y / z column passes
+// MODE 0: forward, 1: inverse, 2: forward + spectral divide + inverse (z only)
+template <typename T, int N, int MODE>
+__global__ void __launch_bounds__(fft_threads<N, Tile<T>::B>())
+k_fft_cols(Cx<T>* __restrict__ spec, const Cx<T>* __restrict__ tw, Geo g, size_t stride_n,
+           size_t stride_outer, const double* __restrict__ k2x, const double* __restrict__ k2y,
+           const double* __restrict__ k2z, double ntot) {
+  constexpr int B = Tile<T>::B;
+  constexpr int NT = fft_threads<N, B>();
+  extern __shared__ __align__(16) unsigned char smraw[];
+  Cx<T>* s = reinterpret_cast<Cx<T>*>(smraw);
+  const int kx0 = blockIdx.x * B;
+  const int outer = blockIdx.y;
+  const int nkx = g.nkx;
+  Cx<T>* base = spec + (size_t)outer * stride_outer + kx0;
+  for (int e = threadIdx.x; e < N * B; e += NT) {
+    const int n = e / B, b = e - n * B;
+    Cx<T> z;
+    z.x = (T)0;
+    z.y = (T)0;
+    if (kx0 + b < nkx) z = base[(size_t)n * stride_n + b];
+    s[sw<B>(n, b)] = z;
+  }
+  __syncthreads();
+  fft_tile<T, N, B, NT, MODE == 1>(s, tw, 1);
+  if constexpr (MODE == 2) {
+    // multi/main.f90:889-895: phi3d = -phi3d/k2/(nx*ny*nz) in FP64, phi3d(1,1,1) = 0
+    const double ky2 = k2y[outer];
+    for (int e = threadIdx.x; e < N * B; e += NT) {
+      const int n = e / B, b = e - n * B;
+      const int kx = kx0 + b;
+      if (kx < nkx) {
+        const double k2 = (k2x[kx] + ky2) + k2z[n];
+        const Cx<T> z = s[sw<B>(n, b)];
+        double re = (-(double)z.x) / k2 / ntot;
+        double im = (-(double)z.y) / k2 / ntot;
+        if (kx == 0 && outer == 0 && n == 0) { re = 0.0; im = 0.0; }
+        s[sw<B>(n, b)] = cx<T>((T)re, (T)im);
+      }
+    }
+    __syncthreads();
+    fft_tile<T, N, B, NT, true>(s, tw, 1);
+  }
+  for (int e = threadIdx.x; e < N * B; e += NT) {
+    const int n = e / B, b = e - n * B;
+    if (kx0 + b < nkx) base[(size_t)n * stride_n + b] = s[sw<B>(n, b)];
+  }
+}
+
+// ------------------------------------------------------------------ host launchers
+template <typename KernelT>
+static cudaError_t prep_smem(KernelT kern, size_t smem) {
+  if (smem > 48 * 1024) return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  return cudaSuccess;
+}
+
+template <typename T, int M>
+static cudaError_t launch_xfwd_m(const PoissonArgs& a, cudaStream_t st) {
+  constexpr int B = Tile<T>::B;
+  const size_t smem = (size_t)(M + 1) * B * sizeof(Cx<T>);
+  auto kern = k_div_fftx<T, M>;
+  cudaError_t e = prep_smem(kern, smem);
+  if (e != cudaSuccess) return e;
+  const int nlines = a.g.ny * a.g.nz;
+  kern<<<(nlines + B - 1) / B, XPASS_THREADS, smem, st>>>(a.u, a.v, a.w, (Cx<T>*)a.spec, (const Cx<T>*)a.twx,
+                                                          a.g, a.cdiv);
+  return cudaGetLastError();
+}
+
+template <typename T, int M>
+static cudaError_t launch_xinv_m(const PoissonArgs& a, cudaStream_t st) {
+  constexpr int B = Tile<T>::B;
+  const size_t smem = (size_t)(M + 1) * B * sizeof(Cx<T>);
+  auto kern = k_fftx_inv<T, M>;
+  cudaError_t e = prep_smem(kern, smem);
+  if (e != cudaSuccess) return e;
+  const int nlines = a.g.ny * a.g.nz;
+  kern<<<(nlines + B - 1) / B, XPASS_THREADS, smem, st>>>((const Cx<T>*)a.spec, (T*)a.p, (const Cx<T>*)a.twx, a.g);
+  return cudaGetLastError();
+}
+
+template <typename T, int N, int MODE>
+static cudaError_t launch_cols_n(const PoissonArgs& a, int axis, cudaStream_t st) {
+  constexpr int B = Tile<T>::B;
+  constexpr int NT = fft_threads<N, B>();
+  const size_t smem = (size_t)N * B * sizeof(Cx<T>);
+  auto kern = k_fft_cols<T, N, MODE>;
+  cudaError_t e = prep_smem(kern, smem);
+  if (e != cudaSuccess) return e;
+  const Geo& g = a.g;
+  const int ntile = (g.nkx + B - 1) / B;
+  const size_t pitch = (size_t)g.pitch;
+  size_t stride_n, stride_outer;
+  int nouter;
+  const void* tw;
+  if (axis == 1) {  // along y, one tile per (kx tile, z)
+    stride_n = pitch;
+    stride_outer = (size_t)g.ny * pitch;
+    nouter = g.nz;
+    tw = a.twy;
+  } else {  // along z, one tile per (kx tile, y)
+    stride_n = (size_t)g.ny * pitch;
+    stride_outer = pitch;
+    nouter = g.ny;
+    tw = a.twz;
+  }
+  dim3 grid(ntile, nouter);
+  kern<<<grid, NT, smem, st>>>((Cx<T>*)a.spec, (const Cx<T>*)tw, g, stride_n, stride_outer, a.k2x, a.k2y, a.k2z,
+                               a.ntot);
+  return cudaGetLastError();
+}
+
+#define MHIT_XSIZES(X) X(8) X(16) X(32) X(64) X(96) X(128) X(256) X(512)
+#define MHIT_NSIZES(X) X(16) X(32) X(64) X(128) X(192) X(256) X(512) X(1024)
+
+template <typename T>
+static cudaError_t launch_xfwd(const PoissonArgs& a, cudaStream_t st) {
+  switch (a.g.nx / 2) {
+#define C(m) case m: return launch_xfwd_m<T, m>(a, st);
+    MHIT_XSIZES(C)
+#undef C
+  }
+  return cudaErrorInvalidValue;
+}
+template <typename T>
+static cudaError_t launch_xinv(const PoissonArgs& a, cudaStream_t st) {
+  switch (a.g.nx / 2) {
+#define C(m) case m: return launch_xinv_m<T, m>(a, st);
+    MHIT_XSIZES(C)
+#undef C
+  }
+  return cudaErrorInvalidValue;
+}
+template <typename T, int MODE>
+static cudaError_t launch_cols(const PoissonArgs& a, int axis, cudaStream_t st) {
+  const int n = axis == 1 ? a.g.ny : a.g.nz;
+  switch (n) {
+#define C(m) case m: return launch_cols_n<T, m, MODE>(a, axis, st);
+    MHIT_NSIZES(C)
+#undef C
+  }
+  return cudaErrorInvalidValue;
+}
+
+bool poisson_size_supported(int n, bool is_x) {
+  if (is_x) {
+    if (n % 2) return false;
+    switch (n / 2) {
+#define C(m) case m: return true;
+      MHIT_XSIZES(C)
+#undef C
+    }
+    return false;
+  }
+  switch (n) {
+#define C(m) case m: return true;
+    MHIT_NSIZES(C)
+#undef C
+  }
+  return false;
+}
+
+template <typename T>
+static cudaError_t poisson_stage_t(const PoissonArgs& a, int stage, cudaStream_t st) {
+  switch (stage) {
+    case PSTAGE_XFWD: return launch_xfwd<T>(a, st);
+    case PSTAGE_YFWD: return launch_cols<T, 0>(a, 1, st);
+    case PSTAGE_ZSOLVE: return launch_cols<T, 2>(a, 2, st);
+    case PSTAGE_YINV: return launch_cols<T, 1>(a, 1, st);
+    case PSTAGE_XINV: return launch_xinv<T>(a, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t poisson_stage(const PoissonArgs& a, int stage, cudaStream_t st) {
+  return a.fp32 ? poisson_stage_t<float>(a, stage, st) : poisson_stage_t<double>(a, stage, st);
+}
+
+}  // namespace mhit

@@ -1,0 +1,92 @@
+// Host-side launchers of the timestep kernels (internal to libmhit_b200.so).
+#pragma once
+#include <cuda_runtime.h>
+#include "common.cuh"
+
+namespace mhit {
+
+int set_cuda_error(cudaError_t e, const char* expr, const char* file, int line);
+
+// ---------------------------------------------------------------- Poisson
+enum { PSTAGE_XFWD = 0, PSTAGE_YFWD, PSTAGE_ZSOLVE, PSTAGE_YINV, PSTAGE_XINV, PSTAGE_COUNT };
+
+struct PoissonArgs {
+  Geo g;
+  bool fp32;
+  const double *u, *v, *w;  // u* (input of the divergence)
+  void* spec;               // Cx<T>[nz][ny][pitch]
+  void* p;                  // T[nz][ny][nx]
+  const void *twx, *twy, *twz;  // exp(-2 pi i m/n) tables, one per axis, in T
+  const double *k2x, *k2y, *k2z;
+  double cdiv;  // rho*dxi/dt
+  double ntot;  // nx*ny*nz
+};
+cudaError_t poisson_stage(const PoissonArgs& a, int stage, cudaStream_t st);
+bool poisson_size_supported(int n, bool is_x);
+
+// ---------------------------------------------------------------- phase field
+struct PhaseArgs {
+  Geo g;
+  const double* phi;    // phi^n
+  const double *u, *v, *w;
+  double* phin;         // phi^{n+1}
+  double* rphio;        // rhsphi_o (read, then overwritten)
+  const DevScalars* sc;
+  double alpha, beta;
+};
+cudaError_t launch_phase(const PhaseArgs& a, cudaStream_t st);
+
+// ---------------------------------------------------------------- momentum
+struct MomArgs {
+  Geo g;
+  const double *u, *v, *w;   // u^n (stored; mean subtracted on read)
+  double *un, *vn, *wn;      // u*
+  double *ru, *rv, *rw;      // rhs_o (read, then overwritten)
+  const double* phi;         // phi^{n+1} or nullptr
+  const double* tabs;        // sx,cx (nx) sy,cy (ny) sz,cz (nz)
+  const DevScalars* sc;
+  double alpha, beta;
+};
+cudaError_t launch_mom(const MomArgs& a, cudaStream_t st);
+
+// ---------------------------------------------------------------- projection + reductions
+struct CorrectArgs {
+  Geo g;
+  double *u, *v, *w;  // u* in, u** out (in place)
+  const void* p;      // float or double pressure
+  bool fp32;
+  double* partials;   // [nblocks][6]
+  int nblocks;
+  DevScalars* sc;
+};
+cudaError_t launch_correct(const CorrectArgs& a, cudaStream_t st);
+int correct_blocks(const Geo& g);
+
+// on-demand diagnostics of the current velocity: max|div|, KE, dissipation
+struct DiagArgs {
+  Geo g;
+  const double *u, *v, *w;
+  double* partials;  // [nblocks][4]
+  int nblocks;
+  DevScalars* sc;
+  double nu, dxd;    // viscosity and spacing used by the dissipation formula
+};
+cudaError_t launch_diag(const DiagArgs& a, cudaStream_t st);
+
+// ---------------------------------------------------------------- tracers
+struct TracerArgs {
+  Geo g;
+  double* part;  // SoA [12][npmax]: tag,x,y,z,u,v,w,phi,u1,v1,w1,phi1
+  int np, npmax;
+  const double *u, *v, *w;
+  const DevScalars* sc;
+  double alpha, beta, lx;
+  int interp;     // 0: 1-D linear (reference), 1: trilinear
+  int yz_shift;
+};
+cudaError_t launch_tracer(const TracerArgs& a, cudaStream_t st);
+
+// ---------------------------------------------------------------- utilities
+cudaError_t launch_fill(double* p, size_t n, double v, cudaStream_t st);
+
+}  // namespace mhit

@@ -1,0 +1,791 @@
+// C ABI of libmhit_b200.so: context management, the per-step launch sequence, CUDA-graph
+// replay, field/particle transfer, field files and the input.inp parser.
+//
+// One step (multi/main.f90:456-1007) is this launch sequence on the context stream:
+//   [tracers] k_tracer                       :477-508
+//   [phase]   k_phase                        :522-636
+//             k_mom                          :658-816
+//             k_div_fftx, k_fft_cols(y fwd),
+//             k_fft_cols(z fwd+solve+inv),
+//             k_fft_cols(y inv), k_fftx_inv  :833-923
+//             k_correct, k_finalize          :942-1007
+// Steps after the first are replayed from two captured CUDA graphs (one per parity of the
+// velocity ping-pong buffers), so a step costs one graph launch on the host.
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/mhit_b200.h"
+#include "common.cuh"
+#include "kernels.h"
+
+namespace mhit {
+
+static thread_local std::string g_err;
+
+int set_error(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+int set_cuda_error(cudaError_t e, const char* expr, const char* file, int line) {
+  char buf[512];
+  snprintf(buf, sizeof(buf), "CUDA error %d (%s) in %s at %s:%d", (int)e, cudaGetErrorString(e), expr, file, line);
+  g_err = buf;
+  return MHIT_ERR_CUDA;
+}
+
+}  // namespace mhit
+
+using namespace mhit;
+
+enum {
+  ST_TRACER = 0, ST_PHASE, ST_MOM, ST_XFWD, ST_YFWD, ST_ZSOLVE, ST_YINV, ST_XINV, ST_CORRECT, ST_COUNT
+};
+static const char* kStageNames[ST_COUNT] = {"k_tracer", "k_phase", "k_mom", "k_div_fftx", "k_fft_cols_yfwd",
+                                            "k_fft_cols_zsolve", "k_fft_cols_yinv", "k_fftx_inv",
+                                            "k_correct+k_finalize"};
+
+struct mhit_ctx {
+  mhit_params prm;
+  Geo g;
+  int dev = 0;
+  cudaStream_t st = nullptr;
+  size_t n = 0;
+  double *U[2] = {}, *V[2] = {}, *W[2] = {};
+  double *RU = nullptr, *RV = nullptr, *RW = nullptr;
+  double *PHI[2] = {}, *RPHI = nullptr;
+  void* P = nullptr;
+  void* spec = nullptr;
+  void *twx = nullptr, *twy = nullptr, *twz = nullptr;
+  double *k2x = nullptr, *k2y = nullptr, *k2z = nullptr;
+  double* tabs = nullptr;
+  double* partials = nullptr;
+  int nblk = 0;
+  DevScalars* sc = nullptr;
+  DevScalars* sc_host = nullptr;
+  double* part = nullptr;
+  int np = 0;
+  int cur = 0;
+  long long nstep = 0;
+  bool graph_built = false;
+  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  cudaEvent_t ev[2 * ST_COUNT] = {};
+};
+
+// ------------------------------------------------------------------ helpers
+static size_t tsize(const mhit_ctx* c) { return c->prm.poisson == MHIT_POISSON_FP32 ? 4 : 8; }
+
+static int check_ctx(mhit_ctx* c) {
+  if (!c) return set_error(MHIT_ERR_ARG, "null context");
+  cudaError_t e = cudaSetDevice(c->dev);
+  if (e != cudaSuccess) return set_cuda_error(e, "cudaSetDevice", __FILE__, __LINE__);
+  return MHIT_OK;
+}
+
+static std::vector<double> grid_coords(int n, double dx) {
+  // x(i) = x(i-1) + dx (multi/main.f90:210-214), extended by one entry
+  std::vector<double> x(n + 1, 0.0);
+  double acc = 0.0;
+  for (int i = 1; i <= n; ++i) {
+    acc = acc + dx;
+    x[i] = acc;
+  }
+  return x;
+}
+
+template <typename T>
+static std::vector<T> twiddles(int n) {
+  std::vector<T> t(2 * (size_t)n);
+  const long double pi = 3.141592653589793238462643383279502884L;
+  for (int m = 0; m < n; ++m) {
+    const long double a = 2.0L * pi * (long double)m / (long double)n;
+    t[2 * m] = (T)(double)cosl(a);
+    t[2 * m + 1] = (T)(double)(-sinl(a));
+  }
+  return t;
+}
+
+template <typename T>
+static int upload_vec(void** dst, const std::vector<T>& v) {
+  MHIT_CUDA_TRY(cudaMalloc(dst, v.size() * sizeof(T)));
+  MHIT_CUDA_TRY(cudaMemcpy(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return MHIT_OK;
+}
+
+static int reset_history(mhit_ctx* c) {
+  const size_t bytes = c->n * sizeof(double);
+  MHIT_CUDA_TRY(cudaMemsetAsync(c->RU, 0, bytes, c->st));
+  MHIT_CUDA_TRY(cudaMemsetAsync(c->RV, 0, bytes, c->st));
+  MHIT_CUDA_TRY(cudaMemsetAsync(c->RW, 0, bytes, c->st));
+  if (c->RPHI) MHIT_CUDA_TRY(cudaMemsetAsync(c->RPHI, 0, bytes, c->st));
+  DevScalars s;
+  memset(&s, 0, sizeof(s));
+  s.gumax = 1.0;  // multi/main.f90:442
+  *c->sc_host = s;
+  MHIT_CUDA_TRY(cudaMemcpyAsync(c->sc, c->sc_host, sizeof(DevScalars), cudaMemcpyHostToDevice, c->st));
+  MHIT_CUDA_TRY(cudaStreamSynchronize(c->st));
+  c->nstep = 0;
+  return MHIT_OK;
+}
+
+// Materialise the lazily removed mean into the stored velocity (before a partial overwrite).
+__global__ void k_apply_mean(double* u, double* v, double* w, size_t n, DevScalars* sc) {
+  const double a = sc->mean[0], b = sc->mean[1], c = sc->mean[2];
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    u[i] = u[i] - a;
+    v[i] = v[i] - b;
+    w[i] = w[i] - c;
+  }
+}
+
+__global__ void k_clear_mean(DevScalars* sc) {
+  sc->mean[0] = 0.0;
+  sc->mean[1] = 0.0;
+  sc->mean[2] = 0.0;
+}
+
+// ------------------------------------------------------------------ one step
+static int enqueue_step(mhit_ctx* c, double alpha, double beta, int cur, bool profile) {
+  const int nxt = cur ^ 1;
+  auto rec = [&](int i) -> int {
+    if (profile) MHIT_CUDA_TRY(cudaEventRecord(c->ev[i], c->st));
+    return MHIT_OK;
+  };
+  int rc;
+  const mhit_params& p = c->prm;
+  if (p.partflag && c->np > 0) {
+    TracerArgs a;
+    a.g = c->g;
+    a.part = c->part;
+    a.np = c->np;
+    a.npmax = c->np;
+    a.u = c->U[cur];
+    a.v = c->V[cur];
+    a.w = c->W[cur];
+    a.sc = c->sc;
+    a.alpha = alpha;
+    a.beta = beta;
+    a.lx = 8.0 * atan(1.0);
+    a.interp = p.interp;
+    a.yz_shift = p.yz_shift;
+    if ((rc = rec(2 * ST_TRACER))) return rc;
+    MHIT_CUDA_TRY(launch_tracer(a, c->st));
+    if ((rc = rec(2 * ST_TRACER + 1))) return rc;
+  }
+  if (p.phiflag) {
+    PhaseArgs a;
+    a.g = c->g;
+    a.phi = c->PHI[cur];
+    a.u = c->U[cur];
+    a.v = c->V[cur];
+    a.w = c->W[cur];
+    a.phin = c->PHI[nxt];
+    a.rphio = c->RPHI;
+    a.sc = c->sc;
+    a.alpha = alpha;
+    a.beta = beta;
+    if ((rc = rec(2 * ST_PHASE))) return rc;
+    MHIT_CUDA_TRY(launch_phase(a, c->st));
+    if ((rc = rec(2 * ST_PHASE + 1))) return rc;
+  }
+  {
+    MomArgs a;
+    a.g = c->g;
+    a.u = c->U[cur];
+    a.v = c->V[cur];
+    a.w = c->W[cur];
+    a.un = c->U[nxt];
+    a.vn = c->V[nxt];
+    a.wn = c->W[nxt];
+    a.ru = c->RU;
+    a.rv = c->RV;
+    a.rw = c->RW;
+    a.phi = p.phiflag ? c->PHI[nxt] : nullptr;
+    a.tabs = c->tabs;
+    a.sc = c->sc;
+    a.alpha = alpha;
+    a.beta = beta;
+    if ((rc = rec(2 * ST_MOM))) return rc;
+    MHIT_CUDA_TRY(launch_mom(a, c->st));
+    if ((rc = rec(2 * ST_MOM + 1))) return rc;
+  }
+  {
+    PoissonArgs a;
+    a.g = c->g;
+    a.fp32 = p.poisson == MHIT_POISSON_FP32;
+    a.u = c->U[nxt];
+    a.v = c->V[nxt];
+    a.w = c->W[nxt];
+    a.spec = c->spec;
+    a.p = c->P;
+    a.twx = c->twx;
+    a.twy = c->twy;
+    a.twz = c->twz;
+    a.k2x = c->k2x;
+    a.k2y = c->k2y;
+    a.k2z = c->k2z;
+    a.cdiv = p.rho * c->g.dxi / p.dt;  // (rho*dxi/dt), multi/main.f90:841
+    a.ntot = (double)c->g.nx * (double)c->g.ny * (double)c->g.nz;
+    for (int s = 0; s < PSTAGE_COUNT; ++s) {
+      if ((rc = rec(2 * (ST_XFWD + s)))) return rc;
+      MHIT_CUDA_TRY(poisson_stage(a, s, c->st));
+      if ((rc = rec(2 * (ST_XFWD + s) + 1))) return rc;
+    }
+  }
+  {
+    CorrectArgs a;
+    a.g = c->g;
+    a.u = c->U[nxt];
+    a.v = c->V[nxt];
+    a.w = c->W[nxt];
+    a.p = c->P;
+    a.fp32 = p.poisson == MHIT_POISSON_FP32;
+    a.partials = c->partials;
+    a.nblocks = c->nblk;
+    a.sc = c->sc;
+    if ((rc = rec(2 * ST_CORRECT))) return rc;
+    MHIT_CUDA_TRY(launch_correct(a, c->st));
+    if ((rc = rec(2 * ST_CORRECT + 1))) return rc;
+  }
+  return MHIT_OK;
+}
+
+static int build_graphs(mhit_ctx* c) {
+  for (int par = 0; par < 2; ++par) {
+    cudaGraph_t graph;
+    MHIT_CUDA_TRY(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+    int rc = enqueue_step(c, 1.5, 0.5, par, false);
+    cudaError_t e = cudaStreamEndCapture(c->st, &graph);
+    if (rc) return rc;
+    if (e != cudaSuccess) return set_cuda_error(e, "cudaStreamEndCapture", __FILE__, __LINE__);
+    e = cudaGraphInstantiate(&c->gexec[par], graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return set_cuda_error(e, "cudaGraphInstantiate", __FILE__, __LINE__);
+  }
+  c->graph_built = true;
+  return MHIT_OK;
+}
+
+// enqueue nsteps without the final flag check
+static int enqueue_steps(mhit_ctx* c, int nsteps) {
+  for (int s = 0; s < nsteps; ++s) {
+    int rc;
+    if (c->nstep == 0) {
+      rc = enqueue_step(c, 1.0, 0.0, c->cur, false);  // Euler first step, multi/main.f90:440-441
+    } else if (c->prm.use_graph) {
+      if (!c->graph_built && (rc = build_graphs(c))) return rc;
+      MHIT_CUDA_TRY(cudaGraphLaunch(c->gexec[c->cur], c->st));
+      rc = MHIT_OK;
+    } else {
+      rc = enqueue_step(c, 1.5, 0.5, c->cur, false);  // AB2, multi/main.f90:801-802
+    }
+    if (rc) return rc;
+    c->cur ^= 1;
+    c->nstep++;
+  }
+  return MHIT_OK;
+}
+
+static int fetch_scalars(mhit_ctx* c) {
+  MHIT_CUDA_TRY(cudaMemcpyAsync(c->sc_host, c->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, c->st));
+  MHIT_CUDA_TRY(cudaStreamSynchronize(c->st));
+  return MHIT_OK;
+}
+
+// ------------------------------------------------------------------ C ABI
+extern "C" {
+
+int mhit_abi_version(void) { return MHIT_ABI_VERSION; }
+
+const char* mhit_last_error(void) { return g_err.c_str(); }
+
+int mhit_params_default(mhit_params* p) {
+  if (!p) return set_error(MHIT_ERR_ARG, "null params");
+  memset(p, 0, sizeof(*p));
+  p->nx = p->ny = p->nz = 64;
+  // multi/input.inp:7-16
+  p->dt = 0.0002;
+  p->mu = 0.006;
+  p->rho = 1.0;
+  p->f1 = p->f2 = p->f3 = 1.0;
+  p->k0 = 2.0;
+  p->radius = 0.5;
+  p->sigma = 1.0;
+  p->epsr = 1.0;
+  p->npart = 0;
+  p->poisson = MHIT_POISSON_FP64;
+  p->laplacian = MHIT_LAP_EXACT;
+  p->interp = MHIT_INTERP_LINEAR1D;
+  p->yz_shift = 1;
+  p->use_graph = 1;
+  p->device = 0;
+  return MHIT_OK;
+}
+
+static int parse_num(FILE* f, double* out, int lineno, const char* path) {
+  char line[512];
+  if (!fgets(line, sizeof(line), f)) {
+    char b[600];
+    snprintf(b, sizeof(b), "%s: missing line %d", path, lineno);
+    return set_error(MHIT_ERR_IO, b);
+  }
+  // first token; Fortran d/D exponent -> e
+  char tok[128];
+  if (sscanf(line, "%127s", tok) != 1) {
+    char b[600];
+    snprintf(b, sizeof(b), "%s: empty line %d", path, lineno);
+    return set_error(MHIT_ERR_IO, b);
+  }
+  for (char* q = tok; *q; ++q)
+    if (*q == 'd' || *q == 'D') *q = 'e';
+  char* end = nullptr;
+  *out = strtod(tok, &end);
+  if (end == tok) {
+    char b[600];
+    snprintf(b, sizeof(b), "%s: line %d is not a number: %s", path, lineno, tok);
+    return set_error(MHIT_ERR_IO, b);
+  }
+  return MHIT_OK;
+}
+
+int mhit_read_input(const char* path, mhit_params* p, mhit_run* run) {
+  if (!path || !p) return set_error(MHIT_ERR_ARG, "null argument");
+  FILE* f = fopen(path, "r");
+  if (!f) return set_error(MHIT_ERR_IO, std::string("cannot open ") + path);
+  double v[18];
+  for (int i = 0; i < 18; ++i) {
+    int rc = parse_num(f, &v[i], i + 1, path);
+    if (rc) {
+      fclose(f);
+      return rc;
+    }
+  }
+  fclose(f);
+  // multi/readinput.f90:14-35, in file order
+  if (run) {
+    run->restart = (int)v[0];
+    run->tstart = (int)v[1];
+    run->tfin = (int)v[2];
+    run->dump = (int)v[3];
+    run->inflow = (int)v[4];
+    run->inphi = (int)v[5];
+    run->inpart = (int)v[17];
+  }
+  p->dt = v[6];
+  p->mu = v[7];
+  p->rho = v[8];
+  p->f1 = v[9];
+  p->f2 = v[10];
+  p->f3 = v[11];
+  p->k0 = v[12];
+  p->radius = v[13];
+  p->sigma = v[14];
+  p->epsr = v[15];
+  p->npart = (int)v[16];
+  return MHIT_OK;
+}
+
+void mhit_destroy(mhit_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->dev);
+  if (c->st) cudaStreamSynchronize(c->st);
+  for (int i = 0; i < 2; ++i) {
+    if (c->gexec[i]) cudaGraphExecDestroy(c->gexec[i]);
+    cudaFree(c->U[i]);
+    cudaFree(c->V[i]);
+    cudaFree(c->W[i]);
+    cudaFree(c->PHI[i]);
+  }
+  cudaFree(c->RU);
+  cudaFree(c->RV);
+  cudaFree(c->RW);
+  cudaFree(c->RPHI);
+  cudaFree(c->P);
+  cudaFree(c->spec);
+  cudaFree(c->twx);
+  cudaFree(c->twy);
+  cudaFree(c->twz);
+  cudaFree(c->k2x);
+  cudaFree(c->k2y);
+  cudaFree(c->k2z);
+  cudaFree(c->tabs);
+  cudaFree(c->partials);
+  cudaFree(c->sc);
+  cudaFree(c->part);
+  if (c->sc_host) cudaFreeHost(c->sc_host);
+  for (int i = 0; i < 2 * ST_COUNT; ++i)
+    if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+  if (c->st) cudaStreamDestroy(c->st);
+  delete c;
+}
+
+static int init_impl(const mhit_params* p, mhit_ctx* c) {
+  c->prm = *p;
+  c->dev = p->device;
+  MHIT_CUDA_TRY(cudaSetDevice(c->dev));
+  MHIT_CUDA_TRY(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+  for (int i = 0; i < 2 * ST_COUNT; ++i) MHIT_CUDA_TRY(cudaEventCreate(&c->ev[i]));
+  Geo& g = c->g;
+  g.nx = p->nx;
+  g.ny = p->ny;
+  g.nz = p->nz;
+  g.nkx = p->nx / 2 + 1;
+  g.pitch = (g.nkx + 15) / 16 * 16;
+  // multi/readinput.f90:114-124
+  const double twopi = 8.0 * atan(1.0);
+  const double lx = twopi;
+  g.dx = lx / p->nx;
+  g.dxi = 1.0 / g.dx;
+  g.ddxi = 1.0 / g.dx / g.dx;
+  g.rhoi = 1.0 / p->rho;
+  g.eps = p->epsr * g.dx;
+  g.epsi = 1.0 / g.eps;
+  g.dt = p->dt;
+  g.mu = p->mu;
+  g.rho = p->rho;
+  g.sigma = p->sigma;
+  g.f1 = p->f1;
+  g.f2 = p->f2;
+  g.f3 = p->f3;
+  const size_t n = (size_t)g.nx * g.ny * g.nz;
+  c->n = n;
+  const size_t fb = n * sizeof(double);
+  for (int i = 0; i < 2; ++i) {
+    MHIT_CUDA_TRY(cudaMalloc(&c->U[i], fb));
+    MHIT_CUDA_TRY(cudaMalloc(&c->V[i], fb));
+    MHIT_CUDA_TRY(cudaMalloc(&c->W[i], fb));
+    MHIT_CUDA_TRY(cudaMemset(c->U[i], 0, fb));
+    MHIT_CUDA_TRY(cudaMemset(c->V[i], 0, fb));
+    MHIT_CUDA_TRY(cudaMemset(c->W[i], 0, fb));
+    if (p->phiflag) {
+      MHIT_CUDA_TRY(cudaMalloc(&c->PHI[i], fb));
+      MHIT_CUDA_TRY(cudaMemset(c->PHI[i], 0, fb));
+    }
+  }
+  MHIT_CUDA_TRY(cudaMalloc(&c->RU, fb));
+  MHIT_CUDA_TRY(cudaMalloc(&c->RV, fb));
+  MHIT_CUDA_TRY(cudaMalloc(&c->RW, fb));
+  if (p->phiflag) MHIT_CUDA_TRY(cudaMalloc(&c->RPHI, fb));
+  const size_t ts = tsize(c);
+  MHIT_CUDA_TRY(cudaMalloc(&c->P, n * ts));
+  MHIT_CUDA_TRY(cudaMemset(c->P, 0, n * ts));
+  MHIT_CUDA_TRY(cudaMalloc(&c->spec, (size_t)g.pitch * g.ny * g.nz * 2 * ts));
+  MHIT_CUDA_TRY(cudaMemset(c->spec, 0, (size_t)g.pitch * g.ny * g.nz * 2 * ts));
+  int rc;
+  if (ts == 4) {
+    if ((rc = upload_vec(&c->twx, twiddles<float>(g.nx)))) return rc;
+    if ((rc = upload_vec(&c->twy, twiddles<float>(g.ny)))) return rc;
+    if ((rc = upload_vec(&c->twz, twiddles<float>(g.nz)))) return rc;
+  } else {
+    if ((rc = upload_vec(&c->twx, twiddles<double>(g.nx)))) return rc;
+    if ((rc = upload_vec(&c->twy, twiddles<double>(g.ny)))) return rc;
+    if ((rc = upload_vec(&c->twz, twiddles<double>(g.nz)))) return rc;
+  }
+  // k^2 per axis (multi/main.f90:234-240, 889), or the modified wavenumber
+  auto k2tab = [&](int nn, int len) {
+    std::vector<double> t(len);
+    for (int i = 0; i < len; ++i) {
+      const double kk = (i < nn / 2) ? (double)i : (double)(i - nn);
+      t[i] = p->laplacian == MHIT_LAP_MODIFIED ? (2.0 - 2.0 * cos(kk * g.dx)) * g.ddxi : kk * kk;
+    }
+    return t;
+  };
+  if ((rc = upload_vec((void**)&c->k2x, k2tab(g.nx, g.nkx)))) return rc;
+  if ((rc = upload_vec((void**)&c->k2y, k2tab(g.ny, g.ny)))) return rc;
+  if ((rc = upload_vec((void**)&c->k2z, k2tab(g.nz, g.nz)))) return rc;
+  // forcing tables (multi/main.f90:244-250; y/z read one entry on, see header)
+  {
+    std::vector<double> t;
+    const int ns[3] = {g.nx, g.ny, g.nz};
+    std::vector<double> sv[3], cv[3];
+    for (int ax = 0; ax < 3; ++ax) {
+      const int nn = ns[ax];
+      std::vector<double> xc = grid_coords(nn, g.dx);
+      const int off = ax == 0 ? 0 : p->yz_shift;
+      for (int i = 0; i < nn; ++i) {
+        t.push_back(sin(p->k0 * xc[i + off] + g.dx / 2));
+      }
+      for (int i = 0; i < nn; ++i) {
+        t.push_back(cos(p->k0 * xc[i + off] + g.dx / 2));
+      }
+    }
+    if ((rc = upload_vec((void**)&c->tabs, t))) return rc;
+  }
+  c->nblk = correct_blocks(g);
+  MHIT_CUDA_TRY(cudaMalloc(&c->partials, (size_t)c->nblk * 6 * sizeof(double)));
+  MHIT_CUDA_TRY(cudaMalloc(&c->sc, sizeof(DevScalars)));
+  MHIT_CUDA_TRY(cudaMallocHost(&c->sc_host, sizeof(DevScalars)));
+  return reset_history(c);
+}
+
+int mhit_init(const mhit_params* p, mhit_ctx** out) {
+  if (!p || !out) return set_error(MHIT_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (!poisson_size_supported(p->nx, true) || !poisson_size_supported(p->ny, false) ||
+      !poisson_size_supported(p->nz, false) || p->nx < 16) {
+    char b[256];
+    snprintf(b, sizeof(b), "unsupported grid %dx%dx%d (each of 16,32,64,128,192,256,512,1024; nx even)", p->nx, p->ny,
+             p->nz);
+    return set_error(MHIT_ERR_ARG, b);
+  }
+  if (p->nx != 2 * (p->nx / 2) || !(p->dt > 0) || !(p->rho > 0) || !(p->epsr > 0))
+    return set_error(MHIT_ERR_ARG, "dt, rho and epsr must be positive");
+  if (p->poisson != MHIT_POISSON_FP64 && p->poisson != MHIT_POISSON_FP32)
+    return set_error(MHIT_ERR_ARG, "poisson must be MHIT_POISSON_FP64 or MHIT_POISSON_FP32");
+  if (p->laplacian != MHIT_LAP_EXACT && p->laplacian != MHIT_LAP_MODIFIED)
+    return set_error(MHIT_ERR_ARG, "laplacian must be MHIT_LAP_EXACT or MHIT_LAP_MODIFIED");
+  if (p->interp != MHIT_INTERP_LINEAR1D && p->interp != MHIT_INTERP_TRILINEAR)
+    return set_error(MHIT_ERR_ARG, "interp must be MHIT_INTERP_LINEAR1D or MHIT_INTERP_TRILINEAR");
+  if (p->yz_shift != 0 && p->yz_shift != 1) return set_error(MHIT_ERR_ARG, "yz_shift must be 0 or 1");
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess) return set_cuda_error(e, "cudaGetDeviceCount", __FILE__, __LINE__);
+  if (p->device < 0 || p->device >= ndev) return set_error(MHIT_ERR_ARG, "device ordinal out of range");
+  mhit_ctx* c = new mhit_ctx();
+  int rc = init_impl(p, c);
+  if (rc) {
+    std::string keep = g_err;
+    mhit_destroy(c);
+    g_err = keep;
+    return rc;
+  }
+  *out = c;
+  return MHIT_OK;
+}
+
+int mhit_upload_fields(mhit_ctx* c, const double* u, const double* v, const double* w, const double* phi) {
+  int rc;
+  if ((rc = check_ctx(c))) return rc;
+  if (!u || !v || !w) return set_error(MHIT_ERR_ARG, "u, v and w are required");
+  if (c->prm.phiflag && !phi) return set_error(MHIT_ERR_ARG, "phi is required when phiflag=1");
+  const size_t fb = c->n * sizeof(double);
+  c->cur = 0;
+  MHIT_CUDA_TRY(cudaMemcpyAsync(c->U[0], u, fb, cudaMemcpyHostToDevice, c->st));
+  MHIT_CUDA_TRY(cudaMemcpyAsync(c->V[0], v, fb, cudaMemcpyHostToDevice, c->st));
+  MHIT_CUDA_TRY(cudaMemcpyAsync(c->W[0], w, fb, cudaMemcpyHostToDevice, c->st));
+  if (c->prm.phiflag) MHIT_CUDA_TRY(cudaMemcpyAsync(c->PHI[0], phi, fb, cudaMemcpyHostToDevice, c->st));
+  return reset_history(c);
+}
+
+int mhit_upload_particles(mhit_ctx* c, const double* part, int npart) {
+  int rc;
+  if ((rc = check_ctx(c))) return rc;
+  if (!c->prm.partflag) return set_error(MHIT_ERR_STATE, "context was created with partflag=0");
+  if (npart < 0 || (npart > 0 && !part)) return set_error(MHIT_ERR_ARG, "bad particle table");
+  if (c->part) {
+    MHIT_CUDA_TRY(cudaStreamSynchronize(c->st));
+    cudaFree(c->part);
+    c->part = nullptr;
+  }
+  c->np = npart;
+  if (npart == 0) return MHIT_OK;
+  const size_t bytes = (size_t)npart * 12 * sizeof(double);
+  MHIT_CUDA_TRY(cudaMalloc(&c->part, bytes));
+  MHIT_CUDA_TRY(cudaMemcpyAsync(c->part, part, bytes, cudaMemcpyHostToDevice, c->st));
+  MHIT_CUDA_TRY(cudaStreamSynchronize(c->st));
+  // the tracer kernel's pointer is baked into captured graphs
+  for (int i = 0; i < 2; ++i)
+    if (c->gexec[i]) {
+      cudaGraphExecDestroy(c->gexec[i]);
+      c->gexec[i] = nullptr;
+    }
+  c->graph_built = false;
+  return MHIT_OK;
+}
+
+int mhit_download_particles(mhit_ctx* c, double* part, int npart) {
+  int rc;
+  if ((rc = check_ctx(c))) return rc;
+  if (npart != c->np) return set_error(MHIT_ERR_ARG, "npart does not match the uploaded table");
+  if (npart == 0) return MHIT_OK;
+  if (!part) return set_error(MHIT_ERR_ARG, "null particle buffer");
+  MHIT_CUDA_TRY(cudaMemcpyAsync(part, c->part, (size_t)npart * 12 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  MHIT_CUDA_TRY(cudaStreamSynchronize(c->st));
+  return MHIT_OK;
+}
+
+int mhit_step(mhit_ctx* c, int nsteps) {
+  int rc;
+  if ((rc = check_ctx(c))) return rc;
+  if (nsteps < 0) return set_error(MHIT_ERR_ARG, "nsteps < 0");
+  if ((rc = enqueue_steps(c, nsteps))) return rc;
+  if ((rc = fetch_scalars(c))) return rc;
+  if (c->sc_host->flag & 1) return set_error(MHIT_ERR_NAN, "NaN in the velocity field");
+  if (c->sc_host->flag & 2) {
+    char b[128];
+    snprintf(b, sizeof(b), "CFL %.6g > 7 (multi/main.f90:1006 stops here)", c->sc_host->cfl);
+    return set_error(MHIT_ERR_CFL, b);
+  }
+  return MHIT_OK;
+}
+
+int mhit_time_steps(mhit_ctx* c, int nsteps, double* ms) {
+  int rc;
+  if ((rc = check_ctx(c))) return rc;
+  if (!ms || nsteps < 0) return set_error(MHIT_ERR_ARG, "bad argument");
+  MHIT_CUDA_TRY(cudaEventRecord(c->ev[0], c->st));
+  if ((rc = enqueue_steps(c, nsteps))) return rc;
+  MHIT_CUDA_TRY(cudaEventRecord(c->ev[1], c->st));
+  MHIT_CUDA_TRY(cudaEventSynchronize(c->ev[1]));
+  float f = 0.f;
+  MHIT_CUDA_TRY(cudaEventElapsedTime(&f, c->ev[0], c->ev[1]));
+  *ms = f;
+  return MHIT_OK;
+}
+
+int mhit_profile_step(mhit_ctx* c, double* ms, const char** names, int* nstages) {
+  int rc;
+  if ((rc = check_ctx(c))) return rc;
+  if (!ms || !nstages || *nstages < ST_COUNT) return set_error(MHIT_ERR_ARG, "need room for all stages");
+  const bool first = c->nstep == 0;
+  MHIT_CUDA_TRY(cudaStreamSynchronize(c->st));
+  // mark stages that do not run
+  for (int i = 0; i < ST_COUNT; ++i) ms[i] = -1.0;
+  if ((rc = enqueue_step(c, first ? 1.0 : 1.5, first ? 0.0 : 0.5, c->cur, true))) return rc;
+  MHIT_CUDA_TRY(cudaStreamSynchronize(c->st));
+  for (int i = 0; i < ST_COUNT; ++i) {
+    const bool ran = !((i == ST_TRACER && !(c->prm.partflag && c->np > 0)) || (i == ST_PHASE && !c->prm.phiflag));
+    if (ran) {
+      float f = 0.f;
+      MHIT_CUDA_TRY(cudaEventElapsedTime(&f, c->ev[2 * i], c->ev[2 * i + 1]));
+      ms[i] = f;
+    }
+    if (names) names[i] = kStageNames[i];
+  }
+  *nstages = ST_COUNT;
+  c->cur ^= 1;
+  c->nstep++;
+  return MHIT_OK;
+}
+
+int mhit_download_fields(mhit_ctx* c, double* u, double* v, double* w, double* p, double* phi) {
+  int rc;
+  if ((rc = check_ctx(c))) return rc;
+  if ((rc = fetch_scalars(c))) return rc;
+  const size_t n = c->n, fb = n * sizeof(double);
+  double* outs[3] = {u, v, w};
+  double* srcs[3] = {c->U[c->cur], c->V[c->cur], c->W[c->cur]};
+  for (int q = 0; q < 3; ++q) {
+    if (!outs[q]) continue;
+    MHIT_CUDA_TRY(cudaMemcpyAsync(outs[q], srcs[q], fb, cudaMemcpyDeviceToHost, c->st));
+  }
+  if (phi) {
+    if (!c->prm.phiflag) return set_error(MHIT_ERR_STATE, "context was created with phiflag=0");
+    MHIT_CUDA_TRY(cudaMemcpyAsync(phi, c->PHI[c->cur], fb, cudaMemcpyDeviceToHost, c->st));
+  }
+  std::vector<float> pf;
+  if (p) {
+    if (tsize(c) == 4) {
+      pf.resize(n);
+      MHIT_CUDA_TRY(cudaMemcpyAsync(pf.data(), c->P, n * 4, cudaMemcpyDeviceToHost, c->st));
+    } else {
+      MHIT_CUDA_TRY(cudaMemcpyAsync(p, c->P, fb, cudaMemcpyDeviceToHost, c->st));
+    }
+  }
+  MHIT_CUDA_TRY(cudaStreamSynchronize(c->st));
+  // lazily removed mean (multi/main.f90:977-981)
+  for (int q = 0; q < 3; ++q) {
+    if (!outs[q]) continue;
+    const double m = c->sc_host->mean[q];
+    if (m != 0.0)
+      for (size_t i = 0; i < n; ++i) outs[q][i] = outs[q][i] - m;
+  }
+  if (p && tsize(c) == 4)
+    for (size_t i = 0; i < n; ++i) p[i] = (double)pf[i];
+  return MHIT_OK;
+}
+
+int mhit_diagnostics(mhit_ctx* c, mhit_diag* d) {
+  int rc;
+  if ((rc = check_ctx(c))) return rc;
+  if (!d) return set_error(MHIT_ERR_ARG, "null diag");
+  // the partials buffer of the projection is reused (stream ordered)
+  DiagArgs a;
+  a.g = c->g;
+  a.u = c->U[c->cur];
+  a.v = c->V[c->cur];
+  a.w = c->W[c->cur];
+  a.partials = c->partials;
+  a.nblocks = c->nblk;
+  a.sc = c->sc;
+  a.nu = c->prm.mu / c->prm.rho;
+  a.dxd = c->g.dx;
+  MHIT_CUDA_TRY(launch_diag(a, c->st));
+  if ((rc = fetch_scalars(c))) return rc;
+  const DevScalars& s = *c->sc_host;
+  d->nstep = c->nstep;
+  d->gumax = s.gumax;
+  d->cfl = s.cfl;
+  for (int q = 0; q < 3; ++q) d->mean[q] = s.mean[q];
+  d->maxdiv = s.diag[0];
+  d->ke = s.diag[1];
+  d->dissipation = s.diag[2];
+  d->flags = s.flag;
+  return MHIT_OK;
+}
+
+static const char* kFieldNames[6] = {"", "u", "v", "w", "p", "phi"};
+
+int mhit_write_field(mhit_ctx* c, const char* dir, int t, int fieldn) {
+  int rc;
+  if ((rc = check_ctx(c))) return rc;
+  if (!dir || fieldn < 1 || fieldn > 5) return set_error(MHIT_ERR_ARG, "fieldn must be 1..5");
+  if (fieldn == 5 && !c->prm.phiflag) return set_error(MHIT_ERR_STATE, "context was created with phiflag=0");
+  std::vector<double> buf(c->n);
+  double* ptrs[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  ptrs[fieldn] = buf.data();
+  if ((rc = mhit_download_fields(c, ptrs[1], ptrs[2], ptrs[3], ptrs[4], ptrs[5]))) return rc;
+  char path[4096];
+  // './output/u_',t,'.dat' with i8.8 (multi/readwrite.f90:41)
+  snprintf(path, sizeof(path), "%s/%s_%08d.dat", dir, kFieldNames[fieldn], t);
+  FILE* f = fopen(path, "wb");
+  if (!f) return set_error(MHIT_ERR_IO, std::string("cannot create ") + path);
+  const size_t wr = fwrite(buf.data(), sizeof(double), c->n, f);
+  const int cl = fclose(f);
+  if (wr != c->n || cl != 0) return set_error(MHIT_ERR_IO, std::string("short write to ") + path);
+  return MHIT_OK;
+}
+
+int mhit_read_field(mhit_ctx* c, const char* path, int fieldn) {
+  int rc;
+  if ((rc = check_ctx(c))) return rc;
+  if (!path || fieldn < 1 || fieldn > 5) return set_error(MHIT_ERR_ARG, "fieldn must be 1..5");
+  if (fieldn == 5 && !c->prm.phiflag) return set_error(MHIT_ERR_STATE, "context was created with phiflag=0");
+  std::vector<double> buf(c->n);
+  FILE* f = fopen(path, "rb");
+  if (!f) return set_error(MHIT_ERR_IO, std::string("cannot open ") + path);
+  const size_t rd = fread(buf.data(), sizeof(double), c->n, f);
+  fclose(f);
+  if (rd != c->n) return set_error(MHIT_ERR_IO, std::string("short read from ") + path);
+  const size_t fb = c->n * sizeof(double);
+  // make the stored velocity explicit before replacing one component
+  k_apply_mean<<<148 * 4, 256, 0, c->st>>>(c->U[c->cur], c->V[c->cur], c->W[c->cur], c->n, c->sc);
+  MHIT_CUDA_TRY(cudaGetLastError());
+  k_clear_mean<<<1, 1, 0, c->st>>>(c->sc);
+  MHIT_CUDA_TRY(cudaGetLastError());
+  if (fieldn <= 3) {
+    double* dst = fieldn == 1 ? c->U[c->cur] : (fieldn == 2 ? c->V[c->cur] : c->W[c->cur]);
+    MHIT_CUDA_TRY(cudaMemcpyAsync(dst, buf.data(), fb, cudaMemcpyHostToDevice, c->st));
+  } else if (fieldn == 5) {
+    MHIT_CUDA_TRY(cudaMemcpyAsync(c->PHI[c->cur], buf.data(), fb, cudaMemcpyHostToDevice, c->st));
+  } else {
+    if (tsize(c) == 4) {
+      std::vector<float> pf(c->n);
+      for (size_t i = 0; i < c->n; ++i) pf[i] = (float)buf[i];
+      MHIT_CUDA_TRY(cudaMemcpyAsync(c->P, pf.data(), c->n * 4, cudaMemcpyHostToDevice, c->st));
+      MHIT_CUDA_TRY(cudaStreamSynchronize(c->st));
+    } else {
+      MHIT_CUDA_TRY(cudaMemcpyAsync(c->P, buf.data(), fb, cudaMemcpyHostToDevice, c->st));
+    }
+  }
+  MHIT_CUDA_TRY(cudaStreamSynchronize(c->st));
+  // a field read happens at setup: the next step is an Euler step with empty history
+  // (multi/main.f90:440-441; rhs_o is not part of the files)
+  return reset_history(c);
+}
+
+}  // extern "C"

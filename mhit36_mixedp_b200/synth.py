@@ -1,0 +1,118 @@
+"""Seeded synthetic initial conditions (numpy, host side).
+
+The reference reads such fields through its ``inflow=1`` / ``inphi=1`` file path
+(multi/main.f90:338-343, 383-386) or builds Taylor-Green / one centred drop
+(multi/main.f90:324-337, 370-382).  The generators here produce the inputs of the benchmark
+configurations with explicit seeds (``numpy.random.default_rng``):
+
+* ``solenoidal_velocity``: random Fourier modes 0 < |k| <= kmax with complex Gaussian
+  amplitudes, Leray-projected (k . c = 0), sampled at the staggered face positions of the
+  reference (u at x - dx/2 as in multi/main.f90:331, v at y - dx/2, w at z - dx/2) and scaled
+  to unit rms per component.
+* ``drops_phi``: phi = 0.5 (1 - tanh((r - R)/(2 eps))) with r the minimum-image distance to the
+  nearest of ``ndrops`` uniformly placed centres (the max over spheres of the single-drop
+  profile of multi/main.f90:377-378; distances are capped at R + 40 eps, where phi < 1e-17).
+* ``uniform_particles``: the tracer table of multi/particles.f90:46-72 with seeded positions.
+
+Grid coordinates use the reference labelling: x = i dx, y = (j + s) dx, z = (k + s) dx with
+s = yz_shift (1 for the reference, see multi/main.f90:327-331).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+LX = 8.0 * math.atan(1.0)
+
+
+def _coords(n, s):
+    dx = LX / n
+    return (np.arange(n) + s) * dx
+
+
+def solenoidal_velocity(nx, seed, kmax=4, rms=1.0, yz_shift=1, ny=None, nz=None):
+    ny = ny or nx
+    nz = nz or nx
+    rng = np.random.default_rng(seed)
+    ks = np.arange(-kmax, kmax + 1)
+    KZ, KY, KX = np.meshgrid(ks, ks, ks, indexing="ij")
+    k2 = KX ** 2 + KY ** 2 + KZ ** 2
+    mask = (k2 > 0) & (k2 <= kmax * kmax)
+    c = (rng.standard_normal((3,) + KX.shape) + 1j * rng.standard_normal((3,) + KX.shape)) * mask
+    kv = np.stack([KX, KY, KZ]).astype(np.float64)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        kdotc = (kv * c).sum(axis=0) / np.where(k2 > 0, k2, 1)
+    c = c - kv * kdotc[None]
+    c = c * mask
+    dx = LX / nx
+    x = _coords(nx, 0)
+    y = _coords(ny, yz_shift)
+    z = _coords(nz, yz_shift)
+    out = []
+    for comp in range(3):
+        xs = x - dx / 2 if comp == 0 else x
+        ys = y - dx / 2 if comp == 1 else y
+        zs = z - dx / 2 if comp == 2 else z
+        ex = np.exp(1j * np.outer(xs, ks))   # (nx, K)
+        ey = np.exp(1j * np.outer(ys, ks))   # (ny, K)
+        ez = np.exp(1j * np.outer(zs, ks))   # (nz, K)
+        a = c[comp] @ ex.T                    # (Kz, Ky, nx)
+        b = np.einsum("jY,ZYi->Zji", ey, a)   # (Kz, ny, nx)
+        b = b.reshape(len(ks), ny * nx)
+        f = np.empty((nz, ny * nx))
+        for z0 in range(0, nz, 64):
+            z1 = min(nz, z0 + 64)
+            f[z0:z1] = ez[z0:z1].real @ b.real - ez[z0:z1].imag @ b.imag
+        f = f.reshape(nz, ny, nx)
+        f *= rms / math.sqrt(float(np.mean(f * f)))
+        out.append(f)
+    return tuple(out)
+
+
+def drop_centres(ndrops, seed):
+    rng = np.random.default_rng(seed)
+    return rng.uniform(0.0, LX, size=(ndrops, 3))
+
+
+def drops_phi(nx, centres, radius, eps, yz_shift=1):
+    n = nx
+    dx = LX / n
+    cap = radius + 40.0 * eps
+    x = _coords(n, 0)
+    y = _coords(n, yz_shift)
+    z = _coords(n, yz_shift)
+    rmin = np.full((n, n, n), cap)
+    h = int(math.ceil(cap / dx)) + 1
+    for cx, cy, cz in centres:
+        ix = int(round(cx / dx))
+        iy = int(round(cy / dx - yz_shift))
+        iz = int(round(cz / dx - yz_shift))
+        ii = np.arange(ix - h, ix + h + 1) % n
+        jj = np.arange(iy - h, iy + h + 1) % n
+        kk = np.arange(iz - h, iz + h + 1) % n
+        if len(np.unique(ii)) < len(ii):
+            ii, jj, kk = np.arange(n), np.arange(n), np.arange(n)
+        ddx = x[ii] - cx
+        ddy = y[jj] - cy
+        ddz = z[kk] - cz
+        ddx -= LX * np.round(ddx / LX)
+        ddy -= LX * np.round(ddy / LX)
+        ddz -= LX * np.round(ddz / LX)
+        r = np.sqrt(ddz[:, None, None] ** 2 + ddy[None, :, None] ** 2 + ddx[None, None, :] ** 2)
+        sub = rmin[np.ix_(kk, jj, ii)]
+        rmin[np.ix_(kk, jj, ii)] = np.minimum(sub, r)
+    return 0.5 * (1.0 - np.tanh((rmin - radius) / 2.0 / eps))
+
+
+def uniform_particles(npart, seed):
+    rng = np.random.default_rng(seed)
+    part = np.zeros((npart, 12), dtype=np.float64, order="F")
+    part[:, 0] = np.arange(1, npart + 1)
+    part[:, 1:4] = rng.uniform(0.0, LX, size=(npart, 3))
+    return part
+
+
+def sigma_from_weber(rho, u_rms, radius, weber):
+    """sigma = rho u_rms^2 (2R) / We (the reference has no Weber number; this is the choice)."""
+    return rho * u_rms * u_rms * (2.0 * radius) / weber
