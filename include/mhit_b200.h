@@ -143,6 +143,42 @@ int mhit_read_field(mhit_ctx* ctx, const char* path, int fieldn);
 int mhit_time_steps(mhit_ctx* ctx, int nsteps, double* ms);
 int mhit_profile_step(mhit_ctx* ctx, double* ms, const char** names, int* nstages);
 
+/* Test hooks (no reference counterpart): run one stage of the step pipeline on the current
+ * buffers, read an internal buffer widened to float64, and commit the staged step.  They let
+ * a test compare each kernel with the matching block of multi/main.f90.  Stage order:
+ * tracer (:477-508), phase (:522-636), momentum (:658-816), then the Poisson stages x-fwd,
+ * y-fwd, z-solve, y-inv, x-inv (:833-923) and the projection (:942-1007).  A stage of a
+ * disabled feature is a no-op.  Buffers: u,v,w of the current step (stored, before the lazy
+ * mean removal), u*,v*,w* / phi^{n+1} of the step being built, the pressure, rhs_o, rhsphi_o,
+ * and the spectrum (interleaved re,im with a row pitch, see mhit_debug_buffer_len). */
+#define MHIT_STAGE_TRACER 0
+#define MHIT_STAGE_PHASE 1
+#define MHIT_STAGE_MOMENTUM 2
+#define MHIT_STAGE_XFWD 3
+#define MHIT_STAGE_YFWD 4
+#define MHIT_STAGE_ZSOLVE 5
+#define MHIT_STAGE_YINV 6
+#define MHIT_STAGE_XINV 7
+#define MHIT_STAGE_CORRECT 8
+#define MHIT_BUF_U 0
+#define MHIT_BUF_V 1
+#define MHIT_BUF_W 2
+#define MHIT_BUF_UN 3
+#define MHIT_BUF_VN 4
+#define MHIT_BUF_WN 5
+#define MHIT_BUF_P 6
+#define MHIT_BUF_PHI 7
+#define MHIT_BUF_PHIN 8
+#define MHIT_BUF_RU 9
+#define MHIT_BUF_RV 10
+#define MHIT_BUF_RW 11
+#define MHIT_BUF_RPHI 12
+#define MHIT_BUF_SPEC 13
+int mhit_debug_run_stage(mhit_ctx* ctx, int stage);
+int mhit_debug_commit_step(mhit_ctx* ctx);
+long long mhit_debug_buffer_len(mhit_ctx* ctx, int which);
+int mhit_debug_get_buffer(mhit_ctx* ctx, int which, double* out);
+
 #ifdef __cplusplus
 }
 #endif

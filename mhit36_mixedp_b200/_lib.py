@@ -70,7 +70,14 @@ SIGNATURES = {
     "mhit_read_field": (_c.c_int, [_c.c_void_p, _c.c_char_p, _c.c_int]),
     "mhit_time_steps": (_c.c_int, [_c.c_void_p, _c.c_int, _dp]),
     "mhit_profile_step": (_c.c_int, [_c.c_void_p, _dp, _P(_c.c_char_p), _P(_c.c_int)]),
+    "mhit_debug_run_stage": (_c.c_int, [_c.c_void_p, _c.c_int]),
+    "mhit_debug_commit_step": (_c.c_int, [_c.c_void_p]),
+    "mhit_debug_buffer_len": (_c.c_longlong, [_c.c_void_p, _c.c_int]),
+    "mhit_debug_get_buffer": (_c.c_int, [_c.c_void_p, _c.c_int, _dp]),
 }
+
+STAGES = ["tracer", "phase", "momentum", "xfwd", "yfwd", "zsolve", "yinv", "xinv", "correct"]
+BUFFERS = ["u", "v", "w", "un", "vn", "wn", "p", "phi", "phin", "ru", "rv", "rw", "rphi", "spec"]
 
 _lib = None
 

@@ -237,6 +237,27 @@ class Solver:
         _check(self._lib.mhit_time_steps(self._ctx, int(nsteps), ctypes.byref(ms)))
         return ms.value
 
+    # -------------------------------------------------------------- test hooks
+    def run_stage(self, stage: str):
+        """Run one stage of the step being built (see mhit_debug_run_stage)."""
+        _check(self._lib.mhit_debug_run_stage(self._ctx, _lib.STAGES.index(stage)))
+
+    def commit_step(self):
+        _check(self._lib.mhit_debug_commit_step(self._ctx))
+
+    def buffer(self, name: str) -> np.ndarray:
+        """An internal device buffer widened to float64 (fields in (nz, ny, nx) shape)."""
+        which = _lib.BUFFERS.index(name)
+        n = self._lib.mhit_debug_buffer_len(self._ctx, which)
+        out = np.empty(int(n), dtype=np.float64)
+        _check(self._lib.mhit_debug_get_buffer(self._ctx, which, _dptr(out)))
+        if name == "spec":
+            p = self.params
+            pitch = n // (2 * p.ny * p.nz)
+            c = out.reshape(p.nz, p.ny, pitch, 2)
+            return (c[..., 0] + 1j * c[..., 1])[:, :, : p.nx // 2 + 1]
+        return out.reshape(self.params.shape)
+
     def profile_step(self) -> dict:
         cap = 16
         ms = (ctypes.c_double * cap)()

@@ -94,13 +94,13 @@ k_div_fftx(const double* __restrict__ u, const double* __restrict__ v, const dou
         const Cx<T> a = scale(zk + conj(zm), h);
         const Cx<T> d = zk - conj(zm);
         const Cx<T> t = cmul(twx[kk], d);  // W^k d
-        s[sw<B>(kk, b)] = cx<T>(a.x - h * t.y, a.y + h * t.x);  // a - i/2 t
+        s[sw<B>(kk, b)] = cx<T>(a.x + h * t.y, a.y - h * t.x);  // a - i/2 t
       }
       if (kk != M - kk) {
         const Cx<T> a = scale(zm + conj(zk), h);
         const Cx<T> d = zm - conj(zk);
         const Cx<T> t = cmul(twx[M - kk], d);
-        s[sw<B>(M - kk, b)] = cx<T>(a.x - h * t.y, a.y + h * t.x);
+        s[sw<B>(M - kk, b)] = cx<T>(a.x + h * t.y, a.y - h * t.x);
       }
     }
   }

@@ -149,107 +149,120 @@ __global__ void k_clear_mean(DevScalars* sc) {
 }
 
 // ------------------------------------------------------------------ one step
-static int enqueue_step(mhit_ctx* c, double alpha, double beta, int cur, bool profile) {
+static bool stage_runs(const mhit_ctx* c, int stage) {
+  if (stage == ST_TRACER) return c->prm.partflag && c->np > 0;
+  if (stage == ST_PHASE) return c->prm.phiflag != 0;
+  return true;
+}
+
+// Launch one stage of the step that reads buffer set `cur` and writes set `cur ^ 1`.
+static int enqueue_stage(mhit_ctx* c, int stage, double alpha, double beta, int cur) {
   const int nxt = cur ^ 1;
-  auto rec = [&](int i) -> int {
-    if (profile) MHIT_CUDA_TRY(cudaEventRecord(c->ev[i], c->st));
-    return MHIT_OK;
-  };
-  int rc;
   const mhit_params& p = c->prm;
-  if (p.partflag && c->np > 0) {
-    TracerArgs a;
-    a.g = c->g;
-    a.part = c->part;
-    a.np = c->np;
-    a.npmax = c->np;
-    a.u = c->U[cur];
-    a.v = c->V[cur];
-    a.w = c->W[cur];
-    a.sc = c->sc;
-    a.alpha = alpha;
-    a.beta = beta;
-    a.lx = 8.0 * atan(1.0);
-    a.interp = p.interp;
-    a.yz_shift = p.yz_shift;
-    if ((rc = rec(2 * ST_TRACER))) return rc;
-    MHIT_CUDA_TRY(launch_tracer(a, c->st));
-    if ((rc = rec(2 * ST_TRACER + 1))) return rc;
-  }
-  if (p.phiflag) {
-    PhaseArgs a;
-    a.g = c->g;
-    a.phi = c->PHI[cur];
-    a.u = c->U[cur];
-    a.v = c->V[cur];
-    a.w = c->W[cur];
-    a.phin = c->PHI[nxt];
-    a.rphio = c->RPHI;
-    a.sc = c->sc;
-    a.alpha = alpha;
-    a.beta = beta;
-    if ((rc = rec(2 * ST_PHASE))) return rc;
-    MHIT_CUDA_TRY(launch_phase(a, c->st));
-    if ((rc = rec(2 * ST_PHASE + 1))) return rc;
-  }
-  {
-    MomArgs a;
-    a.g = c->g;
-    a.u = c->U[cur];
-    a.v = c->V[cur];
-    a.w = c->W[cur];
-    a.un = c->U[nxt];
-    a.vn = c->V[nxt];
-    a.wn = c->W[nxt];
-    a.ru = c->RU;
-    a.rv = c->RV;
-    a.rw = c->RW;
-    a.phi = p.phiflag ? c->PHI[nxt] : nullptr;
-    a.tabs = c->tabs;
-    a.sc = c->sc;
-    a.alpha = alpha;
-    a.beta = beta;
-    if ((rc = rec(2 * ST_MOM))) return rc;
-    MHIT_CUDA_TRY(launch_mom(a, c->st));
-    if ((rc = rec(2 * ST_MOM + 1))) return rc;
-  }
-  {
-    PoissonArgs a;
-    a.g = c->g;
-    a.fp32 = p.poisson == MHIT_POISSON_FP32;
-    a.u = c->U[nxt];
-    a.v = c->V[nxt];
-    a.w = c->W[nxt];
-    a.spec = c->spec;
-    a.p = c->P;
-    a.twx = c->twx;
-    a.twy = c->twy;
-    a.twz = c->twz;
-    a.k2x = c->k2x;
-    a.k2y = c->k2y;
-    a.k2z = c->k2z;
-    a.cdiv = p.rho * c->g.dxi / p.dt;  // (rho*dxi/dt), multi/main.f90:841
-    a.ntot = (double)c->g.nx * (double)c->g.ny * (double)c->g.nz;
-    for (int s = 0; s < PSTAGE_COUNT; ++s) {
-      if ((rc = rec(2 * (ST_XFWD + s)))) return rc;
-      MHIT_CUDA_TRY(poisson_stage(a, s, c->st));
-      if ((rc = rec(2 * (ST_XFWD + s) + 1))) return rc;
+  if (!stage_runs(c, stage)) return MHIT_OK;
+  switch (stage) {
+    case ST_TRACER: {
+      TracerArgs a;
+      a.g = c->g;
+      a.part = c->part;
+      a.np = c->np;
+      a.npmax = c->np;
+      a.u = c->U[cur];
+      a.v = c->V[cur];
+      a.w = c->W[cur];
+      a.sc = c->sc;
+      a.alpha = alpha;
+      a.beta = beta;
+      a.lx = 8.0 * atan(1.0);
+      a.interp = p.interp;
+      a.yz_shift = p.yz_shift;
+      MHIT_CUDA_TRY(launch_tracer(a, c->st));
+      return MHIT_OK;
+    }
+    case ST_PHASE: {
+      PhaseArgs a;
+      a.g = c->g;
+      a.phi = c->PHI[cur];
+      a.u = c->U[cur];
+      a.v = c->V[cur];
+      a.w = c->W[cur];
+      a.phin = c->PHI[nxt];
+      a.rphio = c->RPHI;
+      a.sc = c->sc;
+      a.alpha = alpha;
+      a.beta = beta;
+      MHIT_CUDA_TRY(launch_phase(a, c->st));
+      return MHIT_OK;
+    }
+    case ST_MOM: {
+      MomArgs a;
+      a.g = c->g;
+      a.u = c->U[cur];
+      a.v = c->V[cur];
+      a.w = c->W[cur];
+      a.un = c->U[nxt];
+      a.vn = c->V[nxt];
+      a.wn = c->W[nxt];
+      a.ru = c->RU;
+      a.rv = c->RV;
+      a.rw = c->RW;
+      a.phi = p.phiflag ? c->PHI[nxt] : nullptr;
+      a.tabs = c->tabs;
+      a.sc = c->sc;
+      a.alpha = alpha;
+      a.beta = beta;
+      MHIT_CUDA_TRY(launch_mom(a, c->st));
+      return MHIT_OK;
+    }
+    case ST_XFWD:
+    case ST_YFWD:
+    case ST_ZSOLVE:
+    case ST_YINV:
+    case ST_XINV: {
+      PoissonArgs a;
+      a.g = c->g;
+      a.fp32 = p.poisson == MHIT_POISSON_FP32;
+      a.u = c->U[nxt];
+      a.v = c->V[nxt];
+      a.w = c->W[nxt];
+      a.spec = c->spec;
+      a.p = c->P;
+      a.twx = c->twx;
+      a.twy = c->twy;
+      a.twz = c->twz;
+      a.k2x = c->k2x;
+      a.k2y = c->k2y;
+      a.k2z = c->k2z;
+      a.cdiv = p.rho * c->g.dxi / p.dt;  // (rho*dxi/dt), multi/main.f90:841
+      a.ntot = (double)c->g.nx * (double)c->g.ny * (double)c->g.nz;
+      MHIT_CUDA_TRY(poisson_stage(a, stage - ST_XFWD, c->st));
+      return MHIT_OK;
+    }
+    case ST_CORRECT: {
+      CorrectArgs a;
+      a.g = c->g;
+      a.u = c->U[nxt];
+      a.v = c->V[nxt];
+      a.w = c->W[nxt];
+      a.p = c->P;
+      a.fp32 = p.poisson == MHIT_POISSON_FP32;
+      a.partials = c->partials;
+      a.nblocks = c->nblk;
+      a.sc = c->sc;
+      MHIT_CUDA_TRY(launch_correct(a, c->st));
+      return MHIT_OK;
     }
   }
-  {
-    CorrectArgs a;
-    a.g = c->g;
-    a.u = c->U[nxt];
-    a.v = c->V[nxt];
-    a.w = c->W[nxt];
-    a.p = c->P;
-    a.fp32 = p.poisson == MHIT_POISSON_FP32;
-    a.partials = c->partials;
-    a.nblocks = c->nblk;
-    a.sc = c->sc;
-    if ((rc = rec(2 * ST_CORRECT))) return rc;
-    MHIT_CUDA_TRY(launch_correct(a, c->st));
-    if ((rc = rec(2 * ST_CORRECT + 1))) return rc;
+  return set_error(MHIT_ERR_ARG, "unknown stage");
+}
+
+static int enqueue_step(mhit_ctx* c, double alpha, double beta, int cur, bool profile) {
+  for (int s = 0; s < ST_COUNT; ++s) {
+    const bool ran = stage_runs(c, s);
+    if (profile && ran) MHIT_CUDA_TRY(cudaEventRecord(c->ev[2 * s], c->st));
+    int rc = enqueue_stage(c, s, alpha, beta, cur);
+    if (rc) return rc;
+    if (profile && ran) MHIT_CUDA_TRY(cudaEventRecord(c->ev[2 * s + 1], c->st));
   }
   return MHIT_OK;
 }
@@ -648,8 +661,7 @@ int mhit_profile_step(mhit_ctx* c, double* ms, const char** names, int* nstages)
   if ((rc = enqueue_step(c, first ? 1.0 : 1.5, first ? 0.0 : 0.5, c->cur, true))) return rc;
   MHIT_CUDA_TRY(cudaStreamSynchronize(c->st));
   for (int i = 0; i < ST_COUNT; ++i) {
-    const bool ran = !((i == ST_TRACER && !(c->prm.partflag && c->np > 0)) || (i == ST_PHASE && !c->prm.phiflag));
-    if (ran) {
+    if (stage_runs(c, i)) {
       float f = 0.f;
       MHIT_CUDA_TRY(cudaEventElapsedTime(&f, c->ev[2 * i], c->ev[2 * i + 1]));
       ms[i] = f;
@@ -786,6 +798,70 @@ int mhit_read_field(mhit_ctx* c, const char* path, int fieldn) {
   // a field read happens at setup: the next step is an Euler step with empty history
   // (multi/main.f90:440-441; rhs_o is not part of the files)
   return reset_history(c);
+}
+
+// ------------------------------------------------------------------ test hooks
+int mhit_debug_run_stage(mhit_ctx* c, int stage) {
+  int rc;
+  if ((rc = check_ctx(c))) return rc;
+  if (stage < 0 || stage >= ST_COUNT) return set_error(MHIT_ERR_ARG, "stage out of range");
+  const bool first = c->nstep == 0;
+  if ((rc = enqueue_stage(c, stage, first ? 1.0 : 1.5, first ? 0.0 : 0.5, c->cur))) return rc;
+  MHIT_CUDA_TRY(cudaStreamSynchronize(c->st));
+  return MHIT_OK;
+}
+
+int mhit_debug_commit_step(mhit_ctx* c) {
+  int rc;
+  if ((rc = check_ctx(c))) return rc;
+  c->cur ^= 1;
+  c->nstep++;
+  return MHIT_OK;
+}
+
+long long mhit_debug_buffer_len(mhit_ctx* c, int which) {
+  if (!c) return -1;
+  if (which == MHIT_BUF_SPEC) return (long long)c->g.pitch * c->g.ny * c->g.nz * 2;
+  if (which >= 0 && which < MHIT_BUF_SPEC) return (long long)c->n;
+  return -1;
+}
+
+int mhit_debug_get_buffer(mhit_ctx* c, int which, double* out) {
+  int rc;
+  if ((rc = check_ctx(c))) return rc;
+  if (!out) return set_error(MHIT_ERR_ARG, "null buffer");
+  const int cur = c->cur, nxt = cur ^ 1;
+  const void* src = nullptr;
+  bool typed = false;  // buffer in the Poisson precision
+  size_t len = c->n;
+  switch (which) {
+    case MHIT_BUF_U: src = c->U[cur]; break;
+    case MHIT_BUF_V: src = c->V[cur]; break;
+    case MHIT_BUF_W: src = c->W[cur]; break;
+    case MHIT_BUF_UN: src = c->U[nxt]; break;
+    case MHIT_BUF_VN: src = c->V[nxt]; break;
+    case MHIT_BUF_WN: src = c->W[nxt]; break;
+    case MHIT_BUF_P: src = c->P; typed = true; break;
+    case MHIT_BUF_PHI: src = c->PHI[cur]; break;
+    case MHIT_BUF_PHIN: src = c->PHI[nxt]; break;
+    case MHIT_BUF_RU: src = c->RU; break;
+    case MHIT_BUF_RV: src = c->RV; break;
+    case MHIT_BUF_RW: src = c->RW; break;
+    case MHIT_BUF_RPHI: src = c->RPHI; break;
+    case MHIT_BUF_SPEC: src = c->spec; typed = true; len = (size_t)c->g.pitch * c->g.ny * c->g.nz * 2; break;
+    default: return set_error(MHIT_ERR_ARG, "unknown buffer");
+  }
+  if (!src) return set_error(MHIT_ERR_STATE, "buffer not allocated on this context");
+  if (typed && tsize(c) == 4) {
+    std::vector<float> f(len);
+    MHIT_CUDA_TRY(cudaMemcpyAsync(f.data(), src, len * 4, cudaMemcpyDeviceToHost, c->st));
+    MHIT_CUDA_TRY(cudaStreamSynchronize(c->st));
+    for (size_t i = 0; i < len; ++i) out[i] = f[i];
+  } else {
+    MHIT_CUDA_TRY(cudaMemcpyAsync(out, src, len * 8, cudaMemcpyDeviceToHost, c->st));
+    MHIT_CUDA_TRY(cudaStreamSynchronize(c->st));
+  }
+  return MHIT_OK;
 }
 
 }  // extern "C"
