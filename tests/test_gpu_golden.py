@@ -1,0 +1,66 @@
+"""GPU path against the committed golden fixtures: the oracle's 16^3 outputs and the
+reference's own published Taylor-Green Re=1600 dissipation curve (val/cudec_128_d2z.txt)."""
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+from mhit36_mixedp_b200 import Params, Solver
+from oracle import mhit_oracle as orc
+from tests.golden.make_golden import CASES, NSTEPS, case_inputs
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_gpu_matches_fixture(gpu, name):
+    prm, u, v, w, phi, part = case_inputs(name)
+    gold = np.load(os.path.join(GOLD, "oracle_16.npz"))
+    with Solver(Params(**prm)) as s:
+        s.upload(u, v, w, phi)
+        if part is not None:
+            s.upload_particles(part)
+        s.step(NSTEPS)
+        out = s.download()
+        gp = s.download_particles() if part is not None else None
+    tol = 1e-5 if prm.get("poisson") == "fp32" else 1e-12
+    for f in ("u", "v", "w"):
+        ref = gold[f"{name}/{f}"]
+        e = np.max(np.abs(out[f] - ref)) / np.max(np.abs(ref))
+        assert e < tol, (f, e)
+    if phi is not None:
+        ref = gold[f"{name}/phi"]
+        assert np.max(np.abs(out["phi"] - ref)) / np.max(np.abs(ref)) < tol
+    if gp is not None:
+        assert np.max(np.abs(gp[:, 1:7] - gold[f"{name}/part"][:, 1:7])) < 1e-12
+
+
+def test_taylor_green_reference_curve(gpu):
+    """128^3 Taylor-Green (nu=6.25e-4, dt=2e-4, no forcing), FP64: the dissipation after each
+    1000 steps against the reference's published curve, computed with its post-processor's
+    dx = 2*float32(pi)/(nx-1)."""
+    with open(os.path.join(GOLD, "tg128_d2z.json")) as f:
+        g = json.load(f)
+    n = 128
+    p = orc.Params(nx=n, mu=g["nu"], f1=0.0, f2=0.0, f3=0.0, dt=g["dt"])
+    u, v, w = orc.taylor_green(p)
+    dxp = 2.0 * float(np.float32(math.pi)) / (n - 1)
+    errs = []
+    with Solver(Params(nx=n, dt=g["dt"], mu=g["nu"], rho=1.0, f1=0.0, f2=0.0, f3=0.0)) as s:
+        s.upload(u, v, w)
+        last = 0
+        for t, ref in g["t_eps"]:
+            k = int(round(t / g["dt"]))
+            if k > last:
+                s.step(k - last)
+                last = k
+            out = s.download(("u", "v", "w"))
+            eps = orc.dissipation(out["u"], out["v"], out["w"], g["nu"], dxp)
+            errs.append((t, eps / ref - 1))
+    print("Taylor-Green 128^3 vs val/cudec_128_d2z.txt:", ["%.1f:%.1e" % e for e in errs])
+    for t, e in errs:
+        bound = 1e-11 if t <= 1.0 else 1e-6
+        assert abs(e) < bound, (t, e)

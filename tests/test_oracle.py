@@ -1,0 +1,129 @@
+"""CPU tests of the oracle: pinned against the reference's own published Taylor-Green curve,
+checked against the committed 16^3 fixtures, and cross-checked between the NumPy and the
+C/OpenMP restatements."""
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+from oracle import mhit_oracle as orc
+from tests.golden.make_golden import CASES, NSTEPS, case_inputs
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def tg_curve():
+    with open(os.path.join(GOLD, "tg128_d2z.json")) as f:
+        return json.load(f)
+
+
+def postproc_dx(n):
+    # post/compute_diss: dx = lx/(nx-1), lx = 2*pi with pi a default-REAL literal
+    return 2.0 * float(np.float32(math.pi)) / (n - 1)
+
+
+def test_tg_initial_dissipation_matches_reference():
+    g = tg_curve()
+    p = orc.Params(nx=128, mu=g["nu"], f1=0.0, f2=0.0, f3=0.0, dt=g["dt"])
+    u, v, w = orc.taylor_green(p)
+    eps0 = orc.dissipation(u, v, w, g["nu"], postproc_dx(128))
+    t0, ref0 = g["t_eps"][0]
+    assert t0 == 0.0
+    assert abs(eps0 / ref0 - 1) < 1e-12
+
+
+def test_tg_1000_steps_matches_reference_curve():
+    """C/OpenMP oracle, 128^3 Taylor-Green, 1000 AB2 steps (t = 0.2) vs val/cudec_128_d2z.txt."""
+    from oracle.coracle import COracle
+    g = tg_curve()
+    p = orc.Params(nx=128, mu=g["nu"], f1=0.0, f2=0.0, f3=0.0, dt=g["dt"])
+    u, v, w = orc.taylor_green(p)
+    c = COracle(nx=128, dt=g["dt"], mu=g["nu"], rho=1.0, f1=0.0, f2=0.0, f3=0.0, k0=2.0)
+    c.set_fields(u, v, w)
+    c.step(1000)
+    f = c.fields()
+    eps = orc.dissipation(f["u"], f["v"], f["w"], g["nu"], postproc_dx(128))
+    t, ref = g["t_eps"][1]
+    assert abs(t - 0.2) < 1e-12
+    assert abs(eps / ref - 1) < 1e-11, eps / ref - 1
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_oracle_reproduces_fixtures(name):
+    prm, u, v, w, phi, part = case_inputs(name)
+    op = orc.Params(**prm)
+    st = orc.new_state(op, u, v, w, phi=phi, part=part)
+    orc.run(op, st, NSTEPS)
+    gold = np.load(os.path.join(GOLD, "oracle_16.npz"))
+    for f in ("u", "v", "w", "p"):
+        np.testing.assert_allclose(getattr(st, f), gold[f"{name}/{f}"], rtol=0, atol=1e-14)
+    if phi is not None:
+        np.testing.assert_allclose(st.phi, gold[f"{name}/phi"], rtol=0, atol=1e-14)
+    if part is not None:
+        np.testing.assert_allclose(st.part, gold[f"{name}/part"], rtol=0, atol=1e-13)
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_c_oracle_matches_numpy_oracle(name):
+    from oracle.coracle import COracle
+    prm, u, v, w, phi, part = case_inputs(name)
+    c = COracle(**prm)
+    c.set_fields(u, v, w, phi)
+    if part is not None:
+        c.set_particles(part)
+    c.step(NSTEPS)
+    f = c.fields()
+    gold = np.load(os.path.join(GOLD, "oracle_16.npz"))
+    for k in ("u", "v", "w"):
+        ref = gold[f"{name}/{k}"]
+        assert np.max(np.abs(f[k] - ref)) / np.max(np.abs(ref)) < 1e-13
+    if part is not None:
+        assert np.max(np.abs(c.particles()[:, 1:7] - gold[f"{name}/part"][:, 1:7])) < 1e-13
+
+
+def test_modified_laplacian_projects_to_zero_divergence():
+    prm, u, v, w, _, _ = case_inputs("ns_fp64")
+    op = orc.Params(laplacian="modified", **prm)
+    st = orc.new_state(op, u, v, w)
+    orc.step(op, st)
+    div = orc.divergence(op, st.u, st.v, st.w)
+    assert np.max(np.abs(div)) < 1e-11
+    # the reference's exact-k^2 divide leaves an O(dx^2) divergence
+    op2 = orc.Params(**prm)
+    st2 = orc.new_state(op2, u, v, w)
+    orc.step(op2, st2)
+    assert np.max(np.abs(orc.divergence(op2, st2.u, st2.v, st2.w))) > 1e-6
+
+
+def test_fp32_poisson_close_to_fp64():
+    prm, u, v, w, _, _ = case_inputs("ns_fp64")
+    a = orc.new_state(orc.Params(**prm), u, v, w)
+    b = orc.new_state(orc.Params(poisson="fp32", **prm), u, v, w)
+    orc.run(orc.Params(**prm), a, 5)
+    orc.run(orc.Params(poisson="fp32", **prm), b, 5)
+    assert np.max(np.abs(a.u - b.u)) / np.max(np.abs(a.u)) < 1e-5
+    assert np.max(np.abs(a.u - b.u)) > 0
+
+
+def test_forcing_tables_reference_labelling():
+    """y/z tables read mysin(jg) with jg one entry on from x (multi/main.f90:709-714)."""
+    p = orc.Params(nx=16, k0=2.0)
+    sx, cx, sy, cy, sz, cz = orc.forcing_tables(p)
+    np.testing.assert_array_equal(sy[:-1], sx[1:])
+    np.testing.assert_array_equal(cz[:-1], cx[1:])
+    # the entry one past the table is the periodic continuation for integer k0
+    assert abs(sy[-1] - sx[0]) < 1e-14
+    p0 = orc.Params(nx=16, k0=2.0, yz_shift=0)
+    t0 = orc.forcing_tables(p0)
+    np.testing.assert_array_equal(t0[2], t0[0])
+
+
+def test_mean_removed_and_gumax_signed():
+    prm, u, v, w, _, _ = case_inputs("ns_fp64")
+    op = orc.Params(**prm)
+    st = orc.new_state(op, u + 0.3, v, w)
+    orc.step(op, st)
+    assert abs(st.u.mean()) < 1e-15 and abs(st.v.mean()) < 1e-15
+    assert st.gumax == max(st.u.max(), st.v.max(), st.w.max())
