@@ -62,5 +62,4 @@ def test_taylor_green_reference_curve(gpu):
             errs.append((t, eps / ref - 1))
     print("Taylor-Green 128^3 vs val/cudec_128_d2z.txt:", ["%.1f:%.1e" % e for e in errs])
     for t, e in errs:
-        bound = 1e-11 if t <= 1.0 else 1e-6
-        assert abs(e) < bound, (t, e)
+        assert abs(e) < 1e-11, (t, e)
