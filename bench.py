@@ -3,7 +3,8 @@
 
 Workload (the headline metric's configuration): 512^3 periodic box, NS + ACDI phase field,
 64 drops of radius 0.3 (eps = dx) at seeded uniform centres (seed 1), seeded solenoidal
-velocity (seed 2, unit rms), nu = 0.003, rho = 1, sigma from We = 1, dt = 5e-4, ABC forcing
+velocity (seed 2, unit rms), nu = 0.003, rho = 1, sigma from We = 1, dt = 2e-4 (the reference's
+input.inp value; 5e-4 exceeds the explicit ACDI diffusion limit dx/(6 gamma) at 512^3), ABC forcing
 f = 1 at k0 = 2.  ``value`` is the mixed-precision step (FP32 Poisson, FP64 state); the FP64
 step is measured on the same inputs and reported beside it with both steps' max divergence.
 Fields are 1.07 GB each, larger than L2, so no flush is needed between steps.
@@ -123,7 +124,7 @@ def workload(n, seed_drops=1, seed_vel=2):
     u, v, w = synth.solenoidal_velocity(n, seed_vel)
     phi = synth.drops_phi(n, synth.drop_centres(64, seed_drops), radius, eps)
     sigma = synth.sigma_from_weber(rho, 1.0, radius, we)
-    prm = dict(nx=n, dt=5e-4, mu=0.003, rho=rho, f1=1.0, f2=1.0, f3=1.0, k0=2.0, radius=radius, sigma=sigma,
+    prm = dict(nx=n, dt=2e-4, mu=0.003, rho=rho, f1=1.0, f2=1.0, f3=1.0, k0=2.0, radius=radius, sigma=sigma,
                epsr=1.0, phiflag=1, partflag=0)
     return prm, u, v, w, phi
 
@@ -285,7 +286,7 @@ def main():
             "metric": METRIC, "value": ms32, "unit": "ms/timestep", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms32, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic",
-            "config": {"workload": f"NS+ACDI {n}^3, 64 drops R=0.3 eps=dx, We=1, nu=0.003, dt=5e-4, "
+            "config": {"workload": f"NS+ACDI {n}^3, 64 drops R=0.3 eps=dx, We=1, nu=0.003, dt=2e-4, "
                                    f"seeds drops=1 vel=2; value: FP32 Poisson (mixed)",
                        "parallelism": "replicas" if world > 1 else "single", "l2": "inputs larger than L2"},
             "fp64_ms_per_step": ms64, "mixed_speedup_vs_fp64": ms64 / ms32,

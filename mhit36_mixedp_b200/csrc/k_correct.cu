@@ -191,25 +191,46 @@ __global__ void __launch_bounds__(CNT) k_diag(DiagArgs a) {
   }
 }
 
-__global__ void k_diag_finalize(const double* __restrict__ partials, int nblocks, Geo g, double nu, DevScalars* sc) {
-  if (threadIdx.x != 0) return;
-  double mdiv = 0.0, ke = 0.0, ss = 0.0;
-  for (int b = 0; b < nblocks; ++b) {
-    mdiv = fmax(mdiv, partials[(size_t)b * 4 + 0]);
-    ke += partials[(size_t)b * 4 + 1];
-    ss += partials[(size_t)b * 4 + 2];
+__global__ void __launch_bounds__(1024) k_diag_finalize(const double* __restrict__ partials, int nblocks, Geo g,
+                                                        double nu, DevScalars* sc) {
+  __shared__ double red[3][32];
+  double vals[3] = {0.0, 0.0, 0.0};
+  for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
+    vals[0] = fmax(vals[0], partials[(size_t)b * 4 + 0]);
+    vals[1] += partials[(size_t)b * 4 + 1];
+    vals[2] += partials[(size_t)b * 4 + 2];
   }
-  const double n = (double)g.nx * g.ny * g.nz;
-  sc->diag[0] = mdiv;
-  sc->diag[1] = 0.5 * ke / n;
-  sc->diag[2] = 2.0 * nu * ss / n;
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    double x = vals[q];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double y = __shfl_down_sync(0xffffffffu, x, o);
+      x = q == 0 ? fmax(x, y) : x + y;
+    }
+    if ((threadIdx.x & 31) == 0) red[q][threadIdx.x >> 5] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int nw = (blockDim.x + 31) / 32;
+    double r[3];
+    for (int q = 0; q < 3; ++q) {
+      double x = red[q][0];
+      for (int wv = 1; wv < nw; ++wv) x = q == 0 ? fmax(x, red[q][wv]) : x + red[q][wv];
+      r[q] = x;
+    }
+    const double n = (double)g.nx * g.ny * g.nz;
+    sc->diag[0] = r[0];
+    sc->diag[1] = 0.5 * r[1] / n;
+    sc->diag[2] = 2.0 * nu * r[2] / n;
+  }
 }
 
 cudaError_t launch_diag(const DiagArgs& a, cudaStream_t st) {
   k_diag<<<a.nblocks, CNT, 0, st>>>(a);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  k_diag_finalize<<<1, 32, 0, st>>>(a.partials, a.nblocks, a.g, a.nu, a.sc);
+  k_diag_finalize<<<1, 1024, 0, st>>>(a.partials, a.nblocks, a.g, a.nu, a.sc);
   return cudaGetLastError();
 }
 
