@@ -2,136 +2,267 @@
 //
 // Per cell: conservative advection (h11..h33, :672-694), viscous Laplacian (:696-707), ABC
 // forcing from the per-axis sin/cos tables (:712-714), and with the phase field the
-// chemical-potential surface-tension force recomputed on chip at the cell and at its -x,-y,-z
-// neighbours (:734-739) and averaged to the faces (:768-770) -- the reference's fxst/fyst/fzst
-// arrays and their 6 halo exchanges (:746-757) are never stored.  Then the AB2 update
-// u* = u + dt (alpha rhs - beta rhs_o), rhs_o = rhs (:771-776 / :787-792).
+// chemical-potential surface-tension force (:734-739) averaged to the faces (:768-770) -- the
+// reference's fxst/fyst/fzst arrays and their 6 halo exchanges (:746-757) are never stored.
+// Then the AB2 update u* = u + dt (alpha rhs - beta rhs_o), rhs_o = rhs (:771-776 / :787-792).
+//
+// Blocking: a block owns a MTX x MTY column of cells and marches up a chunk of z planes.
+// Rings of z planes live in shared memory, filled with cp.async one plane ahead of use:
+//   u, v, w   planes k-1..k+2 (slot k+2 in flight), x/y halo 1
+//   phi^{n+1} planes k-2..k+2, x halo [-2,+1], y halo [-2,+1]
+//   chempot   planes k-1, k over x [-1, MTX-1], y [-1, MTY-1]
+// so every input byte crosses HBM once (plus the x/y halo re-read from L2) and the chemical
+// potential is evaluated once per cell.
 //
 // The velocity read here is the stored one minus the running mean of the previous
 // projection (DevScalars::mean); subtracting on read is exactly the reference's
 // u = u - gumean (:977-981) done lazily.
+#include <cuda_pipeline.h>
+
 #include "common.cuh"
 #include "kernels.h"
 
 namespace mhit {
 
-__device__ __forceinline__ double chempot_at(const double* __restrict__ phi, int i, int j, int k, const Geo& g) {
-  const int nx = g.nx, ny = g.ny, nz = g.nz;
-  const int ip = wrapp(i, nx), im = wrapm(i, nx), jp = wrapp(j, ny), jm = wrapm(j, ny);
-  const int kp = wrapp(k, nz), km = wrapm(k, nz);
-  const double c = __ldg(phi + lin(i, j, k, nx, ny));
-  const double s = __ldg(phi + lin(ip, j, k, nx, ny)) + __ldg(phi + lin(im, j, k, nx, ny)) +
-                   __ldg(phi + lin(i, jp, k, nx, ny)) + __ldg(phi + lin(i, jm, k, nx, ny)) +
-                   __ldg(phi + lin(i, j, kp, nx, ny)) + __ldg(phi + lin(i, j, km, nx, ny));
-  // multi/main.f90:735
-  return c * (1.0 - c) * (1.0 - 2.0 * c) * g.epsi - g.eps * (s - 6.0 * c) * g.ddxi;
+constexpr int MTX = 32, MTY = 8, MNT = MTX * MTY;
+constexpr int MZC = 32;                       // z planes per block
+constexpr int UPX = MTX + 2, UPY = MTY + 2;   // u/v/w plane (halo 1)
+constexpr int UPL = UPX * UPY;
+constexpr int PPX = MTX + 3, PPY = MTY + 3;   // phi plane: x,y in [-2, T+1)
+constexpr int PPL = PPX * PPY;
+constexpr int CPX = MTX + 1, CPY = MTY + 1;   // chempot plane: x,y in [-1, T)
+constexpr int CPL = CPX * CPY;
+constexpr int UCP = (UPL + MNT - 1) / MNT;    // copies per thread per u/v/w plane
+constexpr int PCP = (PPL + MNT - 1) / MNT;
+
+template <bool PHI> struct MomSmem;
+template <> struct MomSmem<false> {
+  double u[4][UPL], v[4][UPL], w[4][UPL];
+};
+template <> struct MomSmem<true> {
+  double u[4][UPL], v[4][UPL], w[4][UPL];
+  double phi[5][PPL];
+  double cp[2][CPL];
+};
+
+__device__ __forceinline__ int wrap_small(int x, int n) {
+  // x in [-n, 2n)
+  return x < 0 ? x + n : (x >= n ? x - n : x);
 }
 
 template <bool PHI>
-__global__ void __launch_bounds__(256) k_mom(MomArgs a) {
+__global__ void __launch_bounds__(MNT, 3) k_mom(MomArgs a) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  MomSmem<PHI>& S = *reinterpret_cast<MomSmem<PHI>*>(smraw);
   const Geo& g = a.g;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z * blockDim.z + threadIdx.z;
-  if (i >= nx || j >= ny || k >= nz) return;
-  const int ip = wrapp(i, nx), im = wrapm(i, nx), jp = wrapp(j, ny), jm = wrapm(j, ny);
-  const int kp = wrapp(k, nz), km = wrapm(k, nz);
-  const double mu_ = a.sc->mean[0], mv_ = a.sc->mean[1], mw_ = a.sc->mean[2];
-  const double* __restrict__ U = a.u;
-  const double* __restrict__ V = a.v;
-  const double* __restrict__ W = a.w;
-#define LU(ii, jj, kk) (__ldg(U + lin(ii, jj, kk, nx, ny)) - mu_)
-#define LV(ii, jj, kk) (__ldg(V + lin(ii, jj, kk, nx, ny)) - mv_)
-#define LW(ii, jj, kk) (__ldg(W + lin(ii, jj, kk, nx, ny)) - mw_)
-  const double u0 = LU(i, j, k), v0 = LV(i, j, k), w0 = LW(i, j, k);
-  const double uxp = LU(ip, j, k), uxm = LU(im, j, k), uyp = LU(i, jp, k), uym = LU(i, jm, k);
-  const double uzp = LU(i, j, kp), uzm = LU(i, j, km);
-  const double vxp = LV(ip, j, k), vxm = LV(im, j, k), vyp = LV(i, jp, k), vym = LV(i, jm, k);
-  const double vzp = LV(i, j, kp), vzm = LV(i, j, km);
-  const double wxp = LW(ip, j, k), wxm = LW(im, j, k), wyp = LW(i, jp, k), wym = LW(i, jm, k);
-  const double wzp = LW(i, j, kp), wzm = LW(i, j, km);
-  const double v_imjp = LV(im, jp, k), w_imkp = LW(im, j, kp), u_ipjm = LU(ip, jm, k);
-  const double w_jmkp = LW(i, jm, kp), u_ipkm = LU(ip, j, km), v_jpkm = LV(i, jp, km);
-#undef LU
-#undef LV
-#undef LW
-  const double dxi = g.dxi, ddxi = g.ddxi, rhoi = g.rhoi, mu = g.mu;
-  // multi/main.f90:672-680
-  double h11 = (uxp + u0) * (uxp + u0) - (u0 + uxm) * (u0 + uxm);
-  double h12 = (uyp + u0) * (vyp + v_imjp) - (u0 + uym) * (v0 + vxm);
-  double h13 = (uzp + u0) * (wzp + w_imkp) - (u0 + uzm) * (w0 + wxm);
-  double h21 = (uxp + u_ipjm) * (vxp + v0) - (u0 + uym) * (v0 + vxm);
-  double h22 = (vyp + v0) * (vyp + v0) - (v0 + vym) * (v0 + vym);
-  double h23 = (wzp + w_jmkp) * (vzp + v0) - (w0 + wym) * (v0 + vzm);
-  double h31 = (wxp + w0) * (uxp + u_ipkm) - (w0 + wxm) * (u0 + uzm);
-  double h32 = (vyp + v_jpkm) * (wyp + w0) - (v0 + vzm) * (w0 + wym);
-  double h33 = (wzp + w0) * (wzp + w0) - (w0 + wzm) * (w0 + wzm);
-  // :682-694
-  double ru = -(h11 * 0.25 * dxi + h12 * 0.25 * dxi + h13 * 0.25 * dxi);
-  double rv = -(h21 * 0.25 * dxi + h22 * 0.25 * dxi + h23 * 0.25 * dxi);
-  double rw = -(h31 * 0.25 * dxi + h32 * 0.25 * dxi + h33 * 0.25 * dxi);
-  // :696-707
-  h11 = mu * (uxp - 2.0 * u0 + uxm) * ddxi;
-  h12 = mu * (uyp - 2.0 * u0 + uym) * ddxi;
-  h13 = mu * (uzp - 2.0 * u0 + uzm) * ddxi;
-  h21 = mu * (vxp - 2.0 * v0 + vxm) * ddxi;
-  h22 = mu * (vyp - 2.0 * v0 + vym) * ddxi;
-  h23 = mu * (vzp - 2.0 * v0 + vzm) * ddxi;
-  h31 = mu * (wxp - 2.0 * w0 + wxm) * ddxi;
-  h32 = mu * (wyp - 2.0 * w0 + wym) * ddxi;
-  h33 = mu * (wzp - 2.0 * w0 + wzm) * ddxi;
-  ru = ru + (h11 + h12 + h13) * rhoi;
-  rv = rv + (h21 + h22 + h23) * rhoi;
-  rw = rw + (h31 + h32 + h33) * rhoi;
-  // :712-714, tables: sx cx | sy cy | sz cz
-  const double* t = a.tabs;
-  const double sxi = __ldg(t + i), cxi = __ldg(t + nx + i);
-  const double syj = __ldg(t + 2 * nx + j), cyj = __ldg(t + 2 * nx + ny + j);
-  const double szk = __ldg(t + 2 * nx + 2 * ny + k), czk = __ldg(t + 2 * nx + 2 * ny + nz + k);
-  ru = ru + g.f3 * szk + g.f2 * cyj;
-  rv = rv + g.f1 * sxi + g.f3 * czk;
-  rw = rw + g.f2 * syj + g.f1 * cxi;
-  if constexpr (PHI) {
-    // :734-739 at the cell and its -x/-y/-z neighbours, :768-770 face average
-    const double* __restrict__ P = a.phi;
-    const double s6 = 6.0 * g.sigma;
-    const double c0 = chempot_at(P, i, j, k, g);
-    const double p_xp = __ldg(P + lin(ip, j, k, nx, ny)), p_xm = __ldg(P + lin(im, j, k, nx, ny));
-    const double p_yp = __ldg(P + lin(i, jp, k, nx, ny)), p_ym = __ldg(P + lin(i, jm, k, nx, ny));
-    const double p_zp = __ldg(P + lin(i, j, kp, nx, ny)), p_zm = __ldg(P + lin(i, j, km, nx, ny));
-    const double p_c = __ldg(P + lin(i, j, k, nx, ny));
-    const int imm = wrapm(im, nx), jmm = wrapm(jm, ny), kmm = wrapm(km, nz);
-    const double fx0 = s6 * c0 * 0.5 * (p_xp - p_xm) * dxi;
-    const double fy0 = s6 * c0 * 0.5 * (p_yp - p_ym) * dxi;
-    const double fz0 = s6 * c0 * 0.5 * (p_zp - p_zm) * dxi;
-    const double cxm = chempot_at(P, im, j, k, g);
-    const double cym = chempot_at(P, i, jm, k, g);
-    const double czm = chempot_at(P, i, j, km, g);
-    const double fxm = s6 * cxm * 0.5 * (p_c - __ldg(P + lin(imm, j, k, nx, ny))) * dxi;
-    const double fym = s6 * cym * 0.5 * (p_c - __ldg(P + lin(i, jmm, k, nx, ny))) * dxi;
-    const double fzm = s6 * czm * 0.5 * (p_c - __ldg(P + lin(i, j, kmm, nx, ny))) * dxi;
-    ru = ru + 0.5 * (fxm + fx0) * rhoi;
-    rv = rv + 0.5 * (fym + fy0) * rhoi;
-    rw = rw + 0.5 * (fzm + fz0) * rhoi;
+  const size_t plane = (size_t)nx * ny;
+  const int i0 = blockIdx.x * MTX, j0 = blockIdx.y * MTY;
+  const int k0 = blockIdx.z * MZC;
+  const int k1 = min(k0 + MZC, nz);
+  const int tid = threadIdx.x;
+
+  // per-thread in-plane source offsets of the elements this thread copies
+  int uoff[UCP], poff[PCP];
+#pragma unroll
+  for (int c = 0; c < UCP; ++c) {
+    const int e = tid + c * MNT;
+    uoff[c] = -1;
+    if (e < UPL) {
+      const int y = e / UPX, x = e - y * UPX;
+      uoff[c] = wrap_small(j0 - 1 + y, ny) * nx + wrap_small(i0 - 1 + x, nx);
+    }
   }
-  const size_t c = lin(i, j, k, nx, ny);
-  const double dt = g.dt, al = a.alpha, be = a.beta;
-  const double ruo = a.ru[c], rvo = a.rv[c], rwo = a.rw[c];
-  a.un[c] = u0 + dt * (al * ru - be * ruo);
-  a.vn[c] = v0 + dt * (al * rv - be * rvo);
-  a.wn[c] = w0 + dt * (al * rw - be * rwo);
-  a.ru[c] = ru;
-  a.rv[c] = rv;
-  a.rw[c] = rw;
+#pragma unroll
+  for (int c = 0; c < PCP; ++c) {
+    const int e = tid + c * MNT;
+    poff[c] = -1;
+    if (PHI && e < PPL) {
+      const int y = e / PPX, x = e - y * PPX;
+      poff[c] = wrap_small(j0 - 2 + y, ny) * nx + wrap_small(i0 - 2 + x, nx);
+    }
+  }
+  auto issue_plane = [&](int m) {
+    const int kw = wrap_small(m, nz);
+    const size_t base = (size_t)kw * plane;
+    const int su = (m - k0 + 8) & 3;
+#pragma unroll
+    for (int c = 0; c < UCP; ++c) {
+      if (uoff[c] >= 0) {
+        const int e = tid + c * MNT;
+        __pipeline_memcpy_async(&S.u[su][e], a.u + base + uoff[c], 8);
+        __pipeline_memcpy_async(&S.v[su][e], a.v + base + uoff[c], 8);
+        __pipeline_memcpy_async(&S.w[su][e], a.w + base + uoff[c], 8);
+      }
+    }
+    if constexpr (PHI) {
+      const int sp = (m - k0 + 10) % 5;
+#pragma unroll
+      for (int c = 0; c < PCP; ++c) {
+        if (poff[c] >= 0) {
+          const int e = tid + c * MNT;
+          __pipeline_memcpy_async(&reinterpret_cast<MomSmem<true>&>(S).phi[sp][e], a.phi + base + poff[c], 8);
+        }
+      }
+    }
+    __pipeline_commit();
+  };
+  // phi ring only (planes k0-2 .. k0-1 before the u ring starts)
+  auto issue_phi = [&](int m) {
+    if constexpr (PHI) {
+      const int kw = wrap_small(m, nz);
+      const size_t base = (size_t)kw * plane;
+      const int sp = (m - k0 + 10) % 5;
+#pragma unroll
+      for (int c = 0; c < PCP; ++c) {
+        if (poff[c] >= 0) {
+          const int e = tid + c * MNT;
+          __pipeline_memcpy_async(&reinterpret_cast<MomSmem<true>&>(S).phi[sp][e], a.phi + base + poff[c], 8);
+        }
+      }
+    }
+    __pipeline_commit();
+  };
+
+  const double eps = g.eps, epsi = g.epsi, ddxi = g.ddxi, dxi = g.dxi;
+  const double s6 = 6.0 * g.sigma;
+  // chemical potential (multi/main.f90:735) of plane m over the CPX x CPY region
+  auto chempot_plane = [&](int m) {
+    if constexpr (PHI) {
+      auto& P = reinterpret_cast<MomSmem<true>&>(S).phi;
+      const int pm = (m - k0 + 9) % 5, p0 = (m - k0 + 10) % 5, pp = (m - k0 + 11) % 5;
+      const int sc = (m - k0 + 4) & 1;
+      for (int e = tid; e < CPL; e += MNT) {
+        const int y = e / CPX, x = e - y * CPX;
+        const int q = (y + 1) * PPX + (x + 1);  // phi index of (i0-1+x, j0-1+y)
+        const double c = P[p0][q];
+        const double s = P[p0][q + 1] + P[p0][q - 1] + P[p0][q + PPX] + P[p0][q - PPX] + P[pp][q] + P[pm][q];
+        reinterpret_cast<MomSmem<true>&>(S).cp[sc][e] = c * (1.0 - c) * (1.0 - 2.0 * c) * epsi - eps * (s - 6.0 * c) * ddxi;
+      }
+    }
+  };
+
+  // prologue: phi k0-2, k0-1; u/v/w + phi k0-1, k0, k0+1
+  issue_phi(k0 - 2);
+  issue_plane(k0 - 1);
+  issue_plane(k0);
+  issue_plane(k0 + 1);
+  __pipeline_wait_prior(0);
+  __syncthreads();
+  chempot_plane(k0 - 1);
+
+  const double mu_ = a.sc->mean[0], mv_ = a.sc->mean[1], mw_ = a.sc->mean[2];
+  const int tx = tid % MTX, ty = tid / MTX;
+  const int i = i0 + tx, j = j0 + ty;
+  const bool own = i < nx && j < ny;
+  const double* t = a.tabs;
+  const double sxi = own ? __ldg(t + i) : 0.0, cxi = own ? __ldg(t + nx + i) : 0.0;
+  const double syj = own ? __ldg(t + 2 * nx + j) : 0.0, cyj = own ? __ldg(t + 2 * nx + ny + j) : 0.0;
+  const double mu = g.mu, rhoi = g.rhoi, dt = g.dt, al = a.alpha, be = a.beta;
+  const int uq = (ty + 1) * UPX + (tx + 1);   // own cell in the u/v/w plane
+  const int pq = (ty + 2) * PPX + (tx + 2);   // own cell in the phi plane
+  const int cq = (ty + 1) * CPX + (tx + 1);   // own cell in the chempot plane
+
+  for (int k = k0; k < k1; ++k) {
+    const size_t c = (size_t)k * plane + (size_t)(own ? j : 0) * nx + (own ? i : 0);
+    double ruo = 0.0, rvo = 0.0, rwo = 0.0;
+    if (own) {
+      ruo = a.ru[c];
+      rvo = a.rv[c];
+      rwo = a.rw[c];
+    }
+    // plane k+1 landed (issued one iteration ago); everyone is done with iteration k-1
+    __pipeline_wait_prior(0);
+    __syncthreads();
+    issue_plane(k + 2);
+    chempot_plane(k);
+    __syncthreads();
+    if (own) {
+      const int sm = (k - k0 + 7) & 3, s0 = (k - k0 + 8) & 3, sp = (k - k0 + 9) & 3;
+      const double* U0 = S.u[s0];
+      const double* V0 = S.v[s0];
+      const double* W0 = S.w[s0];
+      const double u0 = U0[uq] - mu_, v0 = V0[uq] - mv_, w0 = W0[uq] - mw_;
+      const double uxp = U0[uq + 1] - mu_, uxm = U0[uq - 1] - mu_, uyp = U0[uq + UPX] - mu_, uym = U0[uq - UPX] - mu_;
+      const double uzp = S.u[sp][uq] - mu_, uzm = S.u[sm][uq] - mu_;
+      const double vxp = V0[uq + 1] - mv_, vxm = V0[uq - 1] - mv_, vyp = V0[uq + UPX] - mv_, vym = V0[uq - UPX] - mv_;
+      const double vzp = S.v[sp][uq] - mv_, vzm = S.v[sm][uq] - mv_;
+      const double wxp = W0[uq + 1] - mw_, wxm = W0[uq - 1] - mw_, wyp = W0[uq + UPX] - mw_, wym = W0[uq - UPX] - mw_;
+      const double wzp = S.w[sp][uq] - mw_, wzm = S.w[sm][uq] - mw_;
+      const double v_imjp = V0[uq + UPX - 1] - mv_, w_imkp = S.w[sp][uq - 1] - mw_, u_ipjm = U0[uq - UPX + 1] - mu_;
+      const double w_jmkp = S.w[sp][uq - UPX] - mw_, u_ipkm = S.u[sm][uq + 1] - mu_, v_jpkm = S.v[sm][uq + UPX] - mv_;
+      // multi/main.f90:672-694
+      double h11 = (uxp + u0) * (uxp + u0) - (u0 + uxm) * (u0 + uxm);
+      double h12 = (uyp + u0) * (vyp + v_imjp) - (u0 + uym) * (v0 + vxm);
+      double h13 = (uzp + u0) * (wzp + w_imkp) - (u0 + uzm) * (w0 + wxm);
+      double ru = -(h11 * 0.25 * dxi + h12 * 0.25 * dxi + h13 * 0.25 * dxi);
+      double h21 = (uxp + u_ipjm) * (vxp + v0) - (u0 + uym) * (v0 + vxm);
+      double h22 = (vyp + v0) * (vyp + v0) - (v0 + vym) * (v0 + vym);
+      double h23 = (wzp + w_jmkp) * (vzp + v0) - (w0 + wym) * (v0 + vzm);
+      double rv = -(h21 * 0.25 * dxi + h22 * 0.25 * dxi + h23 * 0.25 * dxi);
+      double h31 = (wxp + w0) * (uxp + u_ipkm) - (w0 + wxm) * (u0 + uzm);
+      double h32 = (vyp + v_jpkm) * (wyp + w0) - (v0 + vzm) * (w0 + wym);
+      double h33 = (wzp + w0) * (wzp + w0) - (w0 + wzm) * (w0 + wzm);
+      double rw = -(h31 * 0.25 * dxi + h32 * 0.25 * dxi + h33 * 0.25 * dxi);
+      // :696-707
+      ru = ru + (mu * (uxp - 2.0 * u0 + uxm) * ddxi + mu * (uyp - 2.0 * u0 + uym) * ddxi +
+                 mu * (uzp - 2.0 * u0 + uzm) * ddxi) * rhoi;
+      rv = rv + (mu * (vxp - 2.0 * v0 + vxm) * ddxi + mu * (vyp - 2.0 * v0 + vym) * ddxi +
+                 mu * (vzp - 2.0 * v0 + vzm) * ddxi) * rhoi;
+      rw = rw + (mu * (wxp - 2.0 * w0 + wxm) * ddxi + mu * (wyp - 2.0 * w0 + wym) * ddxi +
+                 mu * (wzp - 2.0 * w0 + wzm) * ddxi) * rhoi;
+      // :712-714
+      const double szk = __ldg(t + 2 * nx + 2 * ny + k), czk = __ldg(t + 2 * nx + 2 * ny + nz + k);
+      ru = ru + g.f3 * szk + g.f2 * cyj;
+      rv = rv + g.f1 * sxi + g.f3 * czk;
+      rw = rw + g.f2 * syj + g.f1 * cxi;
+      if constexpr (PHI) {
+        // :737-739 at the cell and at its -x/-y/-z neighbours, :768-770 face average
+        auto& SP = reinterpret_cast<MomSmem<true>&>(S);
+        const int pmm = (k - k0 + 8) % 5, pm = (k - k0 + 9) % 5, p0 = (k - k0 + 10) % 5, pp = (k - k0 + 11) % 5;
+        const int c0s = (k - k0 + 4) & 1, cms = (k - k0 + 3) & 1;
+        const double* P0 = SP.phi[p0];
+        const double pc = P0[pq];
+        const double c0 = SP.cp[c0s][cq];
+        const double fx0 = s6 * c0 * 0.5 * (P0[pq + 1] - P0[pq - 1]) * dxi;
+        const double fy0 = s6 * c0 * 0.5 * (P0[pq + PPX] - P0[pq - PPX]) * dxi;
+        const double fz0 = s6 * c0 * 0.5 * (SP.phi[pp][pq] - SP.phi[pm][pq]) * dxi;
+        const double fxm = s6 * SP.cp[c0s][cq - 1] * 0.5 * (pc - P0[pq - 2]) * dxi;
+        const double fym = s6 * SP.cp[c0s][cq - CPX] * 0.5 * (pc - P0[pq - 2 * PPX]) * dxi;
+        const double fzm = s6 * SP.cp[cms][cq] * 0.5 * (pc - SP.phi[pmm][pq]) * dxi;
+        ru = ru + 0.5 * (fxm + fx0) * rhoi;
+        rv = rv + 0.5 * (fym + fy0) * rhoi;
+        rw = rw + 0.5 * (fzm + fz0) * rhoi;
+      }
+      a.un[c] = u0 + dt * (al * ru - be * ruo);
+      a.vn[c] = v0 + dt * (al * rv - be * rvo);
+      a.wn[c] = w0 + dt * (al * rw - be * rwo);
+      a.ru[c] = ru;
+      a.rv[c] = rv;
+      a.rw[c] = rw;
+    }
+  }
+  __pipeline_wait_prior(0);
+}
+
+template <bool PHI>
+static cudaError_t launch_mom_t(const MomArgs& a, cudaStream_t st) {
+  const size_t smem = sizeof(MomSmem<PHI>);
+  static int attr_set[64] = {0};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 64 && !attr_set[dev]) {
+    cudaError_t e = cudaFuncSetAttribute(k_mom<PHI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attr_set[dev] = 1;
+  }
+  dim3 grd((a.g.nx + MTX - 1) / MTX, (a.g.ny + MTY - 1) / MTY, (a.g.nz + MZC - 1) / MZC);
+  k_mom<PHI><<<grd, MNT, smem, st>>>(a);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_mom(const MomArgs& a, cudaStream_t st) {
-  dim3 blk(32, 4, 2);
-  dim3 grd((a.g.nx + 31) / 32, (a.g.ny + 3) / 4, (a.g.nz + 1) / 2);
-  if (a.phi) k_mom<true><<<grd, blk, 0, st>>>(a);
-  else k_mom<false><<<grd, blk, 0, st>>>(a);
-  return cudaGetLastError();
+  return a.phi ? launch_mom_t<true>(a, st) : launch_mom_t<false>(a, st);
 }
 
 }  // namespace mhit

@@ -2,77 +2,119 @@
 //
 // The reference makes five passes with three stored intermediates (psidi, tanh_psi and the
 // three normal components) and six halo exchanges.  Here a block owns a PTX x PTY column of
-// cells and marches up a chunk of z planes keeping two rings of three planes in shared
-// memory:
-//   psi   = eps log((min(phi,1)+1e-16)/(1-min(phi,1)+1e-16))           (:527-528), halo 2
-//   F     = 1/4 (1 - tanh(psi/(2 eps))^2) n/(|n|+1e-16), n = central psi differences
-//           (:530, :559-561, :586-589, :609-614), halo 1
-// and writes only phi^{n+1} and rhsphi_o.  psi and F are recomputed for the halo of the tile
-// (x-y recompute factor (PTX+4)(PTY+4)/(PTX PTY)).  gamma = 1.0*gumax is read from the
-// device scalars written by the previous projection (:536, :998-1002).
+// cells and marches up a chunk of z planes, keeping three rings of planes in shared memory:
+//   phi  planes k-1..k+3 (k+3 in flight via cp.async), x/y halo 2
+//   psi  = eps log((min(phi,1)+1e-16)/(1-min(phi,1)+1e-16))          (:527-528), halo 2
+//   F    = 1/4 (1 - t^2) n/(|n|+1e-16), n = central psi differences (:559-561, :586-589,
+//          :609-614), halo 1, with t = tanh(psi/(2 eps)) (:530)
+// and writes only phi^{n+1} and rhsphi_o.  psi and F are recomputed on the x-y halo of the
+// tile (factors (PTX+4)(PTY+4)/(PTX PTY) and (PTX+2)(PTY+2)/(PTX PTY)).
+//
+// t is evaluated in closed form: tanh(log(r)/2) = (r-1)/(r+1) with r = (val+1e-16)/(1-val+1e-16)
+// gives t = (2 val - 1)/(1 + 2e-16) exactly in real arithmetic; in float64 it agrees with the
+// reference's tanh(0.5*psi/eps) to 2.2e-16 over the whole range of phi (a NaN psi, from
+// phi < -1e-16, still gives a NaN t as in the reference).
+//
+// gamma = 1.0*gumax is read from the device scalars written by the previous projection
+// (:536, :998-1002); u, v, w are the stored fields minus the lazily removed mean.
+#include <cuda_pipeline.h>
+
 #include "common.cuh"
 #include "kernels.h"
 
 namespace mhit {
 
-constexpr int PTX = 32, PTY = 8;
-constexpr int PHX = PTX + 4, PHY = PTY + 4;  // psi tile (halo 2)
-constexpr int PFX = PTX + 2, PFY = PTY + 2;  // F tile (halo 1)
-constexpr int PNT = PTX * PTY;
-constexpr int PZCHUNK = 32;
+constexpr int PTX = 32, PTY = 16, PNT = PTX * PTY;
+constexpr int PZC = 32;                      // z planes per block
+constexpr int PHX = PTX + 4, PHY = PTY + 4;  // phi / psi plane (halo 2)
+constexpr int PHL = PHX * PHY;
+constexpr int PFX = PTX + 2, PFY = PTY + 2;  // F plane (halo 1)
+constexpr int PFL = PFX * PFY;
+constexpr int PCPY = (PHL + PNT - 1) / PNT;
 constexpr double ENUM = 1.0e-16;
+constexpr double TNORM = 1.0 / (1.0 + 2.0 * ENUM);
 
-__device__ __forceinline__ int wrapn(int i, int n) {
-  i %= n;
-  return i < 0 ? i + n : i;
+struct PhaseSmem {
+  double phi[5][PHL];
+  double psi[3][PHL];
+  double F[3][3][PFL];
+};
+
+__device__ __forceinline__ int pmodi(int x, int n) {
+  x %= n;
+  return x < 0 ? x + n : x;
 }
 
-__global__ void __launch_bounds__(PNT) k_phase(PhaseArgs a) {
-  __shared__ double spsi[3][PHY][PHX];
-  __shared__ double sF[3][3][PFY][PFX];
+__global__ void __launch_bounds__(PNT, 2) k_phase(PhaseArgs a) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  PhaseSmem& S = *reinterpret_cast<PhaseSmem*>(smraw);
   const Geo& g = a.g;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const size_t plane = (size_t)nx * ny;
   const int i0 = blockIdx.x * PTX, j0 = blockIdx.y * PTY;
-  const int k0 = blockIdx.z * PZCHUNK;
-  const int k1 = min(k0 + PZCHUNK, nz);
+  const int k0 = blockIdx.z * PZC;
+  const int k1 = min(k0 + PZC, nz);
   const int tid = threadIdx.x;
-  const double eps = g.eps, epsi = g.epsi;
-  const double* __restrict__ phi = a.phi;
+  const double eps = g.eps;
+  const double* __restrict__ phig = a.phi;
 
-  auto slot = [&](int m) { return (m - k0 + 6) % 3; };
-  auto psi_plane = [&](int m) {
-    const int kw = wrapn(m, nz);
-    const int s = slot(m);
-    for (int e = tid; e < PHX * PHY; e += PNT) {
+  int poff[PCPY];
+#pragma unroll
+  for (int c = 0; c < PCPY; ++c) {
+    const int e = tid + c * PNT;
+    poff[c] = -1;
+    if (e < PHL) {
       const int y = e / PHX, x = e - y * PHX;
-      const int gi = wrapn(i0 - 2 + x, nx), gj = wrapn(j0 - 2 + y, ny);
-      const double val = fmin(__ldg(phi + lin(gi, gj, kw, nx, ny)), 1.0);
-      spsi[s][y][x] = eps * log((val + ENUM) / (1.0 - val + ENUM));
+      poff[c] = pmodi(j0 - 2 + y, ny) * nx + pmodi(i0 - 2 + x, nx);
+    }
+  }
+  auto slotP = [&](int m) { return (m - k0 + 7) % 5; };
+  auto slot3 = [&](int m) { return (m - k0 + 6) % 3; };
+  auto issue_phi = [&](int m) {
+    const size_t base = (size_t)pmodi(m, nz) * plane;
+    double* dst = S.phi[slotP(m)];
+#pragma unroll
+    for (int c = 0; c < PCPY; ++c)
+      if (poff[c] >= 0) __pipeline_memcpy_async(dst + tid + c * PNT, phig + base + poff[c], 8);
+  };
+  auto psi_plane = [&](int m) {
+    const double* P = S.phi[slotP(m)];
+    double* Q = S.psi[slot3(m)];
+    for (int e = tid; e < PHL; e += PNT) {
+      const double val = fmin(P[e], 1.0);
+      Q[e] = eps * log((val + ENUM) / (1.0 - val + ENUM));
     }
   };
   auto F_plane = [&](int m) {
-    const int sm = slot(m - 1), s0 = slot(m), sp = slot(m + 1);
-    const int sf = slot(m);
-    for (int e = tid; e < PFX * PFY; e += PNT) {
+    const double* Qm = S.psi[slot3(m - 1)];
+    const double* Q0 = S.psi[slot3(m)];
+    const double* Qp = S.psi[slot3(m + 1)];
+    const double* P = S.phi[slotP(m)];
+    const int sf = slot3(m);
+    for (int e = tid; e < PFL; e += PNT) {
       const int y = e / PFX, x = e - y * PFX;
-      const int px = x + 1, py = y + 1;
-      const double ps = spsi[s0][py][px];
-      double nxr = spsi[s0][py][px + 1] - spsi[s0][py][px - 1];
-      double nyr = spsi[s0][py + 1][px] - spsi[s0][py - 1][px];
-      double nzr = spsi[sp][py][px] - spsi[sm][py][px];
+      const int q = (y + 1) * PHX + (x + 1);
+      double nxr = Q0[q + 1] - Q0[q - 1];
+      double nyr = Q0[q + PHX] - Q0[q - PHX];
+      double nzr = Qp[q] - Qm[q];
       const double normag = 1.0 / (sqrt(nxr * nxr + nyr * nyr + nzr * nzr) + ENUM);
       nxr = nxr * normag;
       nyr = nyr * normag;
       nzr = nzr * normag;
-      const double t = tanh(0.5 * ps * epsi);
+      const double ps = Q0[q];
+      const double t = (ps == ps) ? (2.0 * fmin(P[q], 1.0) - 1.0) * TNORM : ps;
       const double fac = 0.25 * (1.0 - t * t);
-      sF[sf][0][y][x] = fac * nxr;
-      sF[sf][1][y][x] = fac * nyr;
-      sF[sf][2][y][x] = fac * nzr;
+      S.F[sf][0][e] = fac * nxr;
+      S.F[sf][1][e] = fac * nyr;
+      S.F[sf][2][e] = fac * nzr;
     }
   };
 
-  // prologue: psi k0-2..k0+1, F k0-1, k0
+  // prologue: phi k0-2..k0+2, psi k0-2..k0+1, F k0-1, k0
+  for (int m = k0 - 2; m <= k0 + 2; ++m) issue_phi(m);
+  __pipeline_commit();
+  __pipeline_wait_prior(0);
+  __syncthreads();
   psi_plane(k0 - 2);
   psi_plane(k0 - 1);
   psi_plane(k0);
@@ -82,7 +124,6 @@ __global__ void __launch_bounds__(PNT) k_phase(PhaseArgs a) {
   psi_plane(k0 + 1);
   __syncthreads();
   F_plane(k0);
-  __syncthreads();
 
   const double gamma = 1.0 * a.sc->gumax;
   const double mu_ = a.sc->mean[0], mv_ = a.sc->mean[1], mw_ = a.sc->mean[2];
@@ -90,48 +131,74 @@ __global__ void __launch_bounds__(PNT) k_phase(PhaseArgs a) {
   const int tx = tid % PTX, ty = tid / PTX;
   const int i = i0 + tx, j = j0 + ty;
   const bool own = (i < nx) && (j < ny);
-  const int ip = wrapp(i % nx, nx), im = wrapm(i % nx, nx);
-  const int jp = wrapp(j % ny, ny), jm = wrapm(j % ny, ny);
+  const int ip = own ? wrapp(i, nx) : 0, jp = own ? wrapp(j, ny) : 0;
+  const int hq = (ty + 2) * PHX + (tx + 2);  // own cell in the phi/psi plane
+  const int fq = (ty + 1) * PFX + (tx + 1);  // own cell in the F plane
 
   for (int k = k0; k < k1; ++k) {
+    // operands from HBM for this plane, issued before the barriers
+    const size_t row = (size_t)k * plane + (size_t)(own ? j : 0) * nx;
+    const int kp = wrapp(k, nz);
+    double u0 = 0, uxp = 0, v0 = 0, vyp = 0, w0 = 0, wzp = 0, ro = 0;
+    if (own) {
+      u0 = __ldg(a.u + row + i);
+      uxp = __ldg(a.u + row + ip);
+      v0 = __ldg(a.v + row + i);
+      vyp = __ldg(a.v + (size_t)k * plane + (size_t)jp * nx + i);
+      w0 = __ldg(a.w + row + i);
+      wzp = __ldg(a.w + (size_t)kp * plane + (size_t)j * nx + i);
+      ro = a.rphio[row + i];
+    }
+    __pipeline_wait_prior(0);
+    __syncthreads();
+    issue_phi(k + 3);
+    __pipeline_commit();
     psi_plane(k + 2);
     __syncthreads();
     F_plane(k + 1);
     __syncthreads();
     if (own) {
-      const int kp = wrapp(k, nz), km = wrapm(k, nz);
-      const size_t c = lin(i, j, k, nx, ny);
-      const double p0 = __ldg(phi + c);
-      const double pxp = __ldg(phi + lin(ip, j, k, nx, ny)), pxm = __ldg(phi + lin(im, j, k, nx, ny));
-      const double pyp = __ldg(phi + lin(i, jp, k, nx, ny)), pym = __ldg(phi + lin(i, jm, k, nx, ny));
-      const double pzp = __ldg(phi + lin(i, j, kp, nx, ny)), pzm = __ldg(phi + lin(i, j, km, nx, ny));
-      const double u0 = __ldg(a.u + c) - mu_, uxp = __ldg(a.u + lin(ip, j, k, nx, ny)) - mu_;
-      const double v0 = __ldg(a.v + c) - mv_, vyp = __ldg(a.v + lin(i, jp, k, nx, ny)) - mv_;
-      const double w0 = __ldg(a.w + c) - mw_, wzp = __ldg(a.w + lin(i, j, kp, nx, ny)) - mw_;
-      // :551-557
+      u0 -= mu_;
+      uxp -= mu_;
+      v0 -= mv_;
+      vyp -= mv_;
+      w0 -= mw_;
+      wzp -= mw_;
+      const double* P0 = S.phi[slotP(k)];
+      const double p0 = P0[hq];
+      const double pxp = P0[hq + 1], pxm = P0[hq - 1], pyp = P0[hq + PHX], pym = P0[hq - PHX];
+      const double pzp = S.phi[slotP(k + 1)][hq], pzm = S.phi[slotP(k - 1)][hq];
+      // multi/main.f90:551-557
       double rhs = -((uxp * 0.5 * (pxp + p0) - u0 * 0.5 * (p0 + pxm)) * dxi) -
                    (vyp * 0.5 * (pyp + p0) - v0 * 0.5 * (p0 + pym)) * dxi -
                    (wzp * 0.5 * (pzp + p0) - w0 * 0.5 * (p0 + pzm)) * dxi +
                    gamma * (eps * (pxp - 2.0 * p0 + pxm) * ddxi + eps * (pyp - 2.0 * p0 + pym) * ddxi +
                             eps * (pzp - 2.0 * p0 + pzm) * ddxi);
       // :609-614
-      const int fx = tx + 1, fy = ty + 1;
-      const int s0 = slot(k), sm = slot(k - 1), sp = slot(k + 1);
-      rhs = rhs - gamma * ((sF[s0][0][fy][fx + 1] - sF[s0][0][fy][fx - 1]) * 0.5 * dxi +
-                           (sF[s0][1][fy + 1][fx] - sF[s0][1][fy - 1][fx]) * 0.5 * dxi +
-                           (sF[sp][2][fy][fx] - sF[sm][2][fy][fx]) * 0.5 * dxi);
+      const double* F0x = S.F[slot3(k)][0];
+      const double* F0y = S.F[slot3(k)][1];
+      rhs = rhs - gamma * ((F0x[fq + 1] - F0x[fq - 1]) * 0.5 * dxi + (F0y[fq + PFX] - F0y[fq - PFX]) * 0.5 * dxi +
+                           (S.F[slot3(k + 1)][2][fq] - S.F[slot3(k - 1)][2][fq]) * 0.5 * dxi);
       // :625-626
-      const double ro = a.rphio[c];
-      a.phin[c] = p0 + dt * (a.alpha * rhs - a.beta * ro);
-      a.rphio[c] = rhs;
+      a.phin[row + i] = p0 + dt * (a.alpha * rhs - a.beta * ro);
+      a.rphio[row + i] = rhs;
     }
-    __syncthreads();
   }
+  __pipeline_wait_prior(0);
 }
 
 cudaError_t launch_phase(const PhaseArgs& a, cudaStream_t st) {
-  dim3 grd((a.g.nx + PTX - 1) / PTX, (a.g.ny + PTY - 1) / PTY, (a.g.nz + PZCHUNK - 1) / PZCHUNK);
-  k_phase<<<grd, PNT, 0, st>>>(a);
+  const size_t smem = sizeof(PhaseSmem);
+  static int attr_set[64] = {0};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 64 && !attr_set[dev]) {
+    cudaError_t e = cudaFuncSetAttribute(k_phase, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attr_set[dev] = 1;
+  }
+  dim3 grd((a.g.nx + PTX - 1) / PTX, (a.g.ny + PTY - 1) / PTY, (a.g.nz + PZC - 1) / PZC);
+  k_phase<<<grd, PNT, smem, st>>>(a);
   return cudaGetLastError();
 }
 
