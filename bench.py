@@ -125,7 +125,7 @@ def workload(n, seed_drops=1, seed_vel=2):
     phi = synth.drops_phi(n, synth.drop_centres(64, seed_drops), radius, eps)
     sigma = synth.sigma_from_weber(rho, 1.0, radius, we)
     prm = dict(nx=n, dt=2e-4, mu=0.003, rho=rho, f1=1.0, f2=1.0, f3=1.0, k0=2.0, radius=radius, sigma=sigma,
-               epsr=1.0, phiflag=1, partflag=0)
+               epsr=1.0, phiflag=1, partflag=0, acdi_clamp=1)
     return prm, u, v, w, phi
 
 

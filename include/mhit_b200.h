@@ -67,6 +67,8 @@ typedef struct mhit_params {
   int yz_shift;              /* 1: the reference's labelling of y/z planes (forcing/tracers) */
   int use_graph;             /* 1: replay steps from a captured CUDA graph */
   int device;                /* CUDA device ordinal */
+  int acdi_clamp;            /* 0: reference psi (phi < -1e-16 gives NaN, multi/main.f90:527-528);
+                                1: phi also clamped below at 0 before the log (opt-in deviation) */
 } mhit_params;
 
 /* Run control lines of input.inp (multi/readinput.f90:14-19, 34-35). */

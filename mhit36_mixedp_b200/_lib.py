@@ -36,7 +36,7 @@ class MhitParams(_c.Structure):
         ("radius", _c.c_double), ("sigma", _c.c_double), ("epsr", _c.c_double),
         ("phiflag", _c.c_int), ("partflag", _c.c_int), ("npart", _c.c_int),
         ("poisson", _c.c_int), ("laplacian", _c.c_int), ("interp", _c.c_int),
-        ("yz_shift", _c.c_int), ("use_graph", _c.c_int), ("device", _c.c_int),
+        ("yz_shift", _c.c_int), ("use_graph", _c.c_int), ("device", _c.c_int), ("acdi_clamp", _c.c_int),
     ]
 
 

@@ -99,6 +99,7 @@ class Params:
     interp: str = "linear1d"
     yz_shift: int = 1
     use_graph: bool = True
+    acdi_clamp: int = 0
     device: int = 0
 
     def __post_init__(self):
@@ -108,7 +109,7 @@ class Params:
     def to_c(self) -> MhitParams:
         c = MhitParams()
         _check(_lib.load().mhit_params_default(ctypes.byref(c)))
-        for f in ("nx", "ny", "nz", "phiflag", "partflag", "npart", "yz_shift", "device"):
+        for f in ("nx", "ny", "nz", "phiflag", "partflag", "npart", "yz_shift", "device", "acdi_clamp"):
             setattr(c, f, int(getattr(self, f)))
         for f in ("dt", "mu", "rho", "f1", "f2", "f3", "k0", "radius", "sigma", "epsr"):
             setattr(c, f, float(getattr(self, f)))

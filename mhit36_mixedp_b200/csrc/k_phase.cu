@@ -15,6 +15,9 @@
 // reference's tanh(0.5*psi/eps) to 2.2e-16 over the whole range of phi (a NaN psi, from
 // phi < -1e-16, still gives a NaN t as in the reference).
 //
+// With PhaseArgs::clamp (opt-in, off by default) phi is also clamped below at 0 before the
+// log, so a cell undershooting to phi < -1e-16 no longer turns psi into NaN.
+//
 // gamma = 1.0*gumax is read from the device scalars written by the previous projection
 // (:536, :998-1002); u, v, w are the stored fields minus the lazily removed mean.
 #include <cuda_pipeline.h>
@@ -56,6 +59,7 @@ __global__ void __launch_bounds__(PNT, 2) k_phase(PhaseArgs a) {
   const int k1 = min(k0 + PZC, nz);
   const int tid = threadIdx.x;
   const double eps = g.eps;
+  const int clamp = a.clamp;
   const double* __restrict__ phig = a.phi;
 
   int poff[PCPY];
@@ -81,7 +85,8 @@ __global__ void __launch_bounds__(PNT, 2) k_phase(PhaseArgs a) {
     const double* P = S.phi[slotP(m)];
     double* Q = S.psi[slot3(m)];
     for (int e = tid; e < PHL; e += PNT) {
-      const double val = fmin(P[e], 1.0);
+      double val = fmin(P[e], 1.0);
+      if (clamp) val = fmax(val, 0.0);
       Q[e] = eps * log((val + ENUM) / (1.0 - val + ENUM));
     }
   };
@@ -102,7 +107,9 @@ __global__ void __launch_bounds__(PNT, 2) k_phase(PhaseArgs a) {
       nyr = nyr * normag;
       nzr = nzr * normag;
       const double ps = Q0[q];
-      const double t = (ps == ps) ? (2.0 * fmin(P[q], 1.0) - 1.0) * TNORM : ps;
+      double val = fmin(P[q], 1.0);
+      if (clamp) val = fmax(val, 0.0);
+      const double t = (ps == ps) ? (2.0 * val - 1.0) * TNORM : ps;
       const double fac = 0.25 * (1.0 - t * t);
       S.F[sf][0][e] = fac * nxr;
       S.F[sf][1][e] = fac * nyr;

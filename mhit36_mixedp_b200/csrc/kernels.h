@@ -33,6 +33,7 @@ struct PhaseArgs {
   double* rphio;        // rhsphi_o (read, then overwritten)
   const DevScalars* sc;
   double alpha, beta;
+  int clamp;            // 1: phi clamped to [0,1] before the log
 };
 cudaError_t launch_phase(const PhaseArgs& a, cudaStream_t st);
 

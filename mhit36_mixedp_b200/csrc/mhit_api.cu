@@ -191,6 +191,7 @@ static int enqueue_stage(mhit_ctx* c, int stage, double alpha, double beta, int 
       a.sc = c->sc;
       a.alpha = alpha;
       a.beta = beta;
+      a.clamp = p.acdi_clamp;
       MHIT_CUDA_TRY(launch_phase(a, c->st));
       return MHIT_OK;
     }
@@ -554,6 +555,7 @@ int mhit_init(const mhit_params* p, mhit_ctx** out) {
   if (p->interp != MHIT_INTERP_LINEAR1D && p->interp != MHIT_INTERP_TRILINEAR)
     return set_error(MHIT_ERR_ARG, "interp must be MHIT_INTERP_LINEAR1D or MHIT_INTERP_TRILINEAR");
   if (p->yz_shift != 0 && p->yz_shift != 1) return set_error(MHIT_ERR_ARG, "yz_shift must be 0 or 1");
+  if (p->acdi_clamp != 0 && p->acdi_clamp != 1) return set_error(MHIT_ERR_ARG, "acdi_clamp must be 0 or 1");
   int ndev = 0;
   cudaError_t e = cudaGetDeviceCount(&ndev);
   if (e != cudaSuccess) return set_cuda_error(e, "cudaGetDeviceCount", __FILE__, __LINE__);

@@ -12,7 +12,7 @@ _c = ctypes
 class OrcParams(_c.Structure):
     _fields_ = [("nx", _c.c_int), ("ny", _c.c_int), ("nz", _c.c_int)] + \
                [(f, _c.c_double) for f in ("dt", "mu", "rho", "f1", "f2", "f3", "k0", "radius", "sigma", "epsr")] + \
-               [(f, _c.c_int) for f in ("phiflag", "partflag", "poisson", "laplacian", "yz_shift", "interp")]
+               [(f, _c.c_int) for f in ("phiflag", "partflag", "poisson", "laplacian", "yz_shift", "interp", "acdi_clamp")]
 
 
 _lib = None
@@ -55,6 +55,7 @@ class COracle:
         p.laplacian = {"exact": 0, "modified": 1}[laplacian]
         p.interp = {"linear1d": 0, "trilinear": 1}[interp]
         p.yz_shift = yz_shift
+        p.acdi_clamp = int(kw.get("acdi_clamp", 0))
         self.n = nx
         self.phiflag = p.phiflag
         self.h = lib().orc_create(_c.byref(p))

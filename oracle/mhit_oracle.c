@@ -21,7 +21,7 @@
 typedef struct {
   int nx, ny, nz;
   double dt, mu, rho, f1, f2, f3, k0, radius, sigma, epsr;
-  int phiflag, partflag, poisson, laplacian, yz_shift, interp;
+  int phiflag, partflag, poisson, laplacian, yz_shift, interp, acdi_clamp;
 } orc_params;
 
 typedef struct {
@@ -310,6 +310,7 @@ static void phase(orc_state* s) {
   LOOP3 {
     size_t c = IDX(i, j, k);
     double val = fmin(phi[c], 1.0);
+    if (s->p.acdi_clamp) val = fmax(val, 0.0);
     psi[c] = eps * log((val + ENUM) / (1.0 - val + ENUM));
     th[c] = tanh(0.5 * psi[c] * epsi);
   }

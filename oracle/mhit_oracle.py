@@ -60,6 +60,7 @@ class Params:
     laplacian: str = "exact"       # "exact" k^2 (multi/main.f90:889) | "modified" (2-2cos)/dx^2
     yz_shift: int = 1              # 1: reference labelling of y/z planes, 0: grid aligned
     interp: str = "linear1d"       # "linear1d" (multi/particles.f90:114-117) | "trilinear"
+    acdi_clamp: int = 0            # 1: also clamp phi >= 0 before the log (opt-in deviation)
 
     def __post_init__(self):
         if self.ny == 0:
@@ -275,6 +276,8 @@ def phase_step(p: Params, st: State):
     eps, epsi, dxi, ddxi = p.eps, p.epsi, p.dxi, p.ddxi
     # :522-534
     val = np.minimum(phi, 1.0)
+    if p.acdi_clamp:
+        val = np.maximum(val, 0.0)
     psidi = eps * np.log((val + ENUM) / (1.0 - val + ENUM))
     tanh_psi = np.tanh(0.5 * psidi * epsi)
     gamma = 1.0 * st.gumax  # :536

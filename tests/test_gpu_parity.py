@@ -81,6 +81,48 @@ def test_acdi_fp64(gpu, n):
         assert e < TOL64, (f, e)
 
 
+def test_acdi_fp64_64_multichunk(gpu):
+    """64^3: several x tiles and z chunks of the marching phase/momentum kernels."""
+    prm, u, v, w, phi, part = make_case(64, phiflag=1)
+    st, out, dg, _ = run_both(prm, u, v, w, phi, part, 4)
+    for f in ("u", "v", "w", "phi"):
+        e = relerr(out[f], getattr(st, f))
+        assert e < TOL64, (f, e)
+
+
+def planted_undershoot(n):
+    prm, u, v, w, phi, part = make_case(n, phiflag=1)
+    phi = phi.copy()
+    phi[n // 2, n // 3, n // 4] = -1e-15  # below -1e-16: the reference's psi is log(<0) = NaN
+    return prm, u, v, w, phi
+
+
+def test_acdi_negative_phi_reference_semantics(gpu):
+    """Default: psi = eps log((min(phi,1)+1e-16)/(...)) as multi/main.f90:527-528, so phi < -1e-16
+    gives NaN like the reference; the library reports it as MhitNaNError."""
+    from mhit36_mixedp_b200 import MhitNaNError
+    prm, u, v, w, phi = planted_undershoot(16)
+    op = orc.Params(**{k: prm[k] for k in prm if k in orc.Params.__dataclass_fields__})
+    st = orc.new_state(op, u, v, w, phi=phi)
+    with np.errstate(invalid="ignore"):
+        orc.step(op, st)
+    assert np.isnan(st.phi).any()
+    with Solver(Params(**prm)) as s:
+        s.upload(u, v, w, phi)
+        with pytest.raises(MhitNaNError):
+            s.step(1)
+
+
+def test_acdi_clamp_matches_oracle(gpu):
+    prm, u, v, w, phi = planted_undershoot(32)
+    prm["acdi_clamp"] = 1
+    st, out, dg, _ = run_both(prm, u, v, w, phi, None, 3)
+    for f in ("u", "v", "w", "phi"):
+        assert np.isfinite(out[f]).all()
+        e = relerr(out[f], getattr(st, f))
+        assert e < TOL64, (f, e)
+
+
 @pytest.mark.parametrize("interp", ["linear1d", "trilinear"])
 def test_tracers_fp64(gpu, interp):
     prm, u, v, w, phi, part = make_case(32, partflag=1, npart=500, interp=interp)

@@ -83,7 +83,7 @@ def test_stages_ns(gpu, n):
             assert abs(d["mean"][q] - means[q]) < 1e-14
 
 
-@pytest.mark.parametrize("n", [16, 32])
+@pytest.mark.parametrize("n", [16, 32, 64])
 def test_stage_phase(gpu, n):
     op, st, s = setup(n, phiflag=1)
     with s:

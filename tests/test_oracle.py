@@ -120,6 +120,28 @@ def test_forcing_tables_reference_labelling():
     np.testing.assert_array_equal(t0[2], t0[0])
 
 
+def test_negative_phi_nan_and_clamp():
+    """phi < -1e-16 makes the reference's psi NaN (multi/main.f90:527-528 clamps only above);
+    acdi_clamp=1 clamps below as well and stays finite, equal to the unclamped step elsewhere."""
+    prm, u, v, w, phi, _ = case_inputs("acdi_tracers")
+    prm = dict(prm, partflag=0)
+    phi = phi.copy()
+    phi[3, 4, 5] = -1e-15
+    a = orc.new_state(orc.Params(**prm), u, v, w, phi=phi)
+    with np.errstate(invalid="ignore"):
+        orc.step(orc.Params(**prm), a)
+    assert np.isnan(a.phi).any()
+    b = orc.new_state(orc.Params(acdi_clamp=1, **prm), u, v, w, phi=phi)
+    orc.step(orc.Params(acdi_clamp=1, **prm), b)
+    assert np.isfinite(b.phi).all() and np.isfinite(b.u).all()
+    from oracle.coracle import COracle
+    c = COracle(acdi_clamp=1, **prm)
+    c.set_fields(u, v, w, phi)
+    c.step(1)
+    f = c.fields()
+    assert np.max(np.abs(f["phi"] - b.phi)) < 1e-14
+
+
 def test_mean_removed_and_gumax_signed():
     prm, u, v, w, _, _ = case_inputs("ns_fp64")
     op = orc.Params(**prm)
