@@ -38,9 +38,9 @@ constexpr double ENUM = 1.0e-16;
 constexpr double TNORM = 1.0 / (1.0 + 2.0 * ENUM);
 
 struct PhaseSmem {
-  double phi[5][PHL];
-  double psi[3][PHL];
-  double F[3][3][PFL];
+  double phi[6][PHL];   // planes k-2..k+3 (k+4 in flight while iteration k runs)
+  double psi[4][PHL];   // planes k..k+3
+  double F[3][3][PFL];  // planes k-1..k+1
 };
 
 __device__ __forceinline__ int pmodi(int x, int n) {
@@ -48,6 +48,8 @@ __device__ __forceinline__ int pmodi(int x, int n) {
   return x < 0 ? x + n : x;
 }
 
+// Software pipeline, two barriers per output plane k:
+//   B1; cp.async phi(k+4); { psi(k+3), F(k+1) } as one task list; B2; out(k)
 __global__ void __launch_bounds__(PNT, 2) k_phase(PhaseArgs a) {
   extern __shared__ __align__(16) unsigned char smraw[];
   PhaseSmem& S = *reinterpret_cast<PhaseSmem*>(smraw);
@@ -72,65 +74,59 @@ __global__ void __launch_bounds__(PNT, 2) k_phase(PhaseArgs a) {
       poff[c] = pmodi(j0 - 2 + y, ny) * nx + pmodi(i0 - 2 + x, nx);
     }
   }
-  auto slotP = [&](int m) { return (m - k0 + 7) % 5; };
+  auto slot6 = [&](int m) { return (m - k0 + 8) % 6; };
+  auto slot4 = [&](int m) { return (m - k0 + 8) & 3; };
   auto slot3 = [&](int m) { return (m - k0 + 6) % 3; };
   auto issue_phi = [&](int m) {
     const size_t base = (size_t)pmodi(m, nz) * plane;
-    double* dst = S.phi[slotP(m)];
+    double* dst = S.phi[slot6(m)];
 #pragma unroll
     for (int c = 0; c < PCPY; ++c)
       if (poff[c] >= 0) __pipeline_memcpy_async(dst + tid + c * PNT, phig + base + poff[c], 8);
   };
-  auto psi_plane = [&](int m) {
-    const double* P = S.phi[slotP(m)];
-    double* Q = S.psi[slot3(m)];
-    for (int e = tid; e < PHL; e += PNT) {
-      double val = fmin(P[e], 1.0);
-      if (clamp) val = fmax(val, 0.0);
-      Q[e] = eps * log((val + ENUM) / (1.0 - val + ENUM));
-    }
+  // psi of one element of plane m (multi/main.f90:527-528)
+  auto psi_elem = [&](int m, int e) {
+    double val = fmin(S.phi[slot6(m)][e], 1.0);
+    if (clamp) val = fmax(val, 0.0);
+    S.psi[slot4(m)][e] = eps * log((val + ENUM) / (1.0 - val + ENUM));
   };
-  auto F_plane = [&](int m) {
-    const double* Qm = S.psi[slot3(m - 1)];
-    const double* Q0 = S.psi[slot3(m)];
-    const double* Qp = S.psi[slot3(m + 1)];
-    const double* P = S.phi[slotP(m)];
+  // F of one element of plane m (multi/main.f90:530, 559-561, 586-589, 609-614)
+  auto F_elem = [&](int m, int e) {
+    const double* Qm = S.psi[slot4(m - 1)];
+    const double* Q0 = S.psi[slot4(m)];
+    const double* Qp = S.psi[slot4(m + 1)];
+    const int y = e / PFX, x = e - y * PFX;
+    const int q = (y + 1) * PHX + (x + 1);
+    double nxr = Q0[q + 1] - Q0[q - 1];
+    double nyr = Q0[q + PHX] - Q0[q - PHX];
+    double nzr = Qp[q] - Qm[q];
+    const double normag = 1.0 / (sqrt(nxr * nxr + nyr * nyr + nzr * nzr) + ENUM);
+    nxr = nxr * normag;
+    nyr = nyr * normag;
+    nzr = nzr * normag;
+    const double ps = Q0[q];
+    double val = fmin(S.phi[slot6(m)][q], 1.0);
+    if (clamp) val = fmax(val, 0.0);
+    const double t = (ps == ps) ? (2.0 * val - 1.0) * TNORM : ps;
+    const double fac = 0.25 * (1.0 - t * t);
     const int sf = slot3(m);
-    for (int e = tid; e < PFL; e += PNT) {
-      const int y = e / PFX, x = e - y * PFX;
-      const int q = (y + 1) * PHX + (x + 1);
-      double nxr = Q0[q + 1] - Q0[q - 1];
-      double nyr = Q0[q + PHX] - Q0[q - PHX];
-      double nzr = Qp[q] - Qm[q];
-      const double normag = 1.0 / (sqrt(nxr * nxr + nyr * nyr + nzr * nzr) + ENUM);
-      nxr = nxr * normag;
-      nyr = nyr * normag;
-      nzr = nzr * normag;
-      const double ps = Q0[q];
-      double val = fmin(P[q], 1.0);
-      if (clamp) val = fmax(val, 0.0);
-      const double t = (ps == ps) ? (2.0 * val - 1.0) * TNORM : ps;
-      const double fac = 0.25 * (1.0 - t * t);
-      S.F[sf][0][e] = fac * nxr;
-      S.F[sf][1][e] = fac * nyr;
-      S.F[sf][2][e] = fac * nzr;
-    }
+    S.F[sf][0][e] = fac * nxr;
+    S.F[sf][1][e] = fac * nyr;
+    S.F[sf][2][e] = fac * nzr;
   };
 
-  // prologue: phi k0-2..k0+2, psi k0-2..k0+1, F k0-1, k0
-  for (int m = k0 - 2; m <= k0 + 2; ++m) issue_phi(m);
+  // prologue: phi k0-2..k0+3; psi k0-2..k0+2 (ring of 4); F k0-1, k0
+  for (int m = k0 - 2; m <= k0 + 3; ++m) issue_phi(m);
   __pipeline_commit();
   __pipeline_wait_prior(0);
   __syncthreads();
-  psi_plane(k0 - 2);
-  psi_plane(k0 - 1);
-  psi_plane(k0);
+  for (int e = tid; e < 3 * PHL; e += PNT) psi_elem(k0 - 2 + e / PHL, e % PHL);
   __syncthreads();
-  F_plane(k0 - 1);
+  for (int e = tid; e < PFL; e += PNT) F_elem(k0 - 1, e);
   __syncthreads();
-  psi_plane(k0 + 1);
+  for (int e = tid; e < 2 * PHL; e += PNT) psi_elem(k0 + 1 + e / PHL, e % PHL);
   __syncthreads();
-  F_plane(k0);
+  for (int e = tid; e < PFL; e += PNT) F_elem(k0, e);
 
   const double gamma = 1.0 * a.sc->gumax;
   const double mu_ = a.sc->mean[0], mv_ = a.sc->mean[1], mw_ = a.sc->mean[2];
@@ -158,11 +154,12 @@ __global__ void __launch_bounds__(PNT, 2) k_phase(PhaseArgs a) {
     }
     __pipeline_wait_prior(0);
     __syncthreads();
-    issue_phi(k + 3);
+    issue_phi(k + 4);
     __pipeline_commit();
-    psi_plane(k + 2);
-    __syncthreads();
-    F_plane(k + 1);
+    for (int e = tid; e < PHL + PFL; e += PNT) {
+      if (e < PHL) psi_elem(k + 3, e);
+      else F_elem(k + 1, e - PHL);
+    }
     __syncthreads();
     if (own) {
       u0 -= mu_;
@@ -171,10 +168,10 @@ __global__ void __launch_bounds__(PNT, 2) k_phase(PhaseArgs a) {
       vyp -= mv_;
       w0 -= mw_;
       wzp -= mw_;
-      const double* P0 = S.phi[slotP(k)];
+      const double* P0 = S.phi[slot6(k)];
       const double p0 = P0[hq];
       const double pxp = P0[hq + 1], pxm = P0[hq - 1], pyp = P0[hq + PHX], pym = P0[hq - PHX];
-      const double pzp = S.phi[slotP(k + 1)][hq], pzm = S.phi[slotP(k - 1)][hq];
+      const double pzp = S.phi[slot6(k + 1)][hq], pzm = S.phi[slot6(k - 1)][hq];
       // multi/main.f90:551-557
       double rhs = -((uxp * 0.5 * (pxp + p0) - u0 * 0.5 * (p0 + pxm)) * dxi) -
                    (vyp * 0.5 * (pyp + p0) - v0 * 0.5 * (p0 + pym)) * dxi -
