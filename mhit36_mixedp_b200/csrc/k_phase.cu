@@ -84,19 +84,16 @@ __global__ void __launch_bounds__(PNT, 2) k_phase(PhaseArgs a) {
     for (int c = 0; c < PCPY; ++c)
       if (poff[c] >= 0) __pipeline_memcpy_async(dst + tid + c * PNT, phig + base + poff[c], 8);
   };
-  // psi of one element of plane m (multi/main.f90:527-528)
-  auto psi_elem = [&](int m, int e) {
-    double val = fmin(S.phi[slot6(m)][e], 1.0);
+  // psi of element e of a plane (multi/main.f90:527-528)
+  auto psi_at = [&](const double* __restrict__ P, double* __restrict__ Q, int e) {
+    double val = fmin(P[e], 1.0);
     if (clamp) val = fmax(val, 0.0);
-    S.psi[slot4(m)][e] = eps * log((val + ENUM) / (1.0 - val + ENUM));
+    Q[e] = eps * log((val + ENUM) / (1.0 - val + ENUM));
   };
-  // F of one element of plane m (multi/main.f90:530, 559-561, 586-589, 609-614)
-  auto F_elem = [&](int m, int e) {
-    const double* Qm = S.psi[slot4(m - 1)];
-    const double* Q0 = S.psi[slot4(m)];
-    const double* Qp = S.psi[slot4(m + 1)];
-    const int y = e / PFX, x = e - y * PFX;
-    const int q = (y + 1) * PHX + (x + 1);
+  // F of one element (multi/main.f90:530, 559-561, 586-589, 609-614); q: psi-plane index,
+  // f: F-plane index
+  auto F_at = [&](const double* __restrict__ Qm, const double* __restrict__ Q0, const double* __restrict__ Qp,
+                  const double* __restrict__ P, double* __restrict__ Fd, int q, int f) {
     double nxr = Q0[q + 1] - Q0[q - 1];
     double nyr = Q0[q + PHX] - Q0[q - PHX];
     double nzr = Qp[q] - Qm[q];
@@ -105,14 +102,24 @@ __global__ void __launch_bounds__(PNT, 2) k_phase(PhaseArgs a) {
     nyr = nyr * normag;
     nzr = nzr * normag;
     const double ps = Q0[q];
-    double val = fmin(S.phi[slot6(m)][q], 1.0);
+    double val = fmin(P[q], 1.0);
     if (clamp) val = fmax(val, 0.0);
     const double t = (ps == ps) ? (2.0 * val - 1.0) * TNORM : ps;
     const double fac = 0.25 * (1.0 - t * t);
-    const int sf = slot3(m);
-    S.F[sf][0][e] = fac * nxr;
-    S.F[sf][1][e] = fac * nyr;
-    S.F[sf][2][e] = fac * nzr;
+    Fd[f] = fac * nxr;
+    Fd[PFL + f] = fac * nyr;
+    Fd[2 * PFL + f] = fac * nzr;
+  };
+  auto F_plane_all = [&](int m) {
+    const double* Qm = S.psi[slot4(m - 1)];
+    const double* Q0 = S.psi[slot4(m)];
+    const double* Qp = S.psi[slot4(m + 1)];
+    const double* P = S.phi[slot6(m)];
+    double* Fd = S.F[slot3(m)][0];
+    for (int e = tid; e < PFL; e += PNT) {
+      const int y = e / PFX, x = e - y * PFX;
+      F_at(Qm, Q0, Qp, P, Fd, (y + 1) * PHX + (x + 1), e);
+    }
   };
 
   // prologue: phi k0-2..k0+3; psi k0-2..k0+2 (ring of 4); F k0-1, k0
@@ -120,13 +127,38 @@ __global__ void __launch_bounds__(PNT, 2) k_phase(PhaseArgs a) {
   __pipeline_commit();
   __pipeline_wait_prior(0);
   __syncthreads();
-  for (int e = tid; e < 3 * PHL; e += PNT) psi_elem(k0 - 2 + e / PHL, e % PHL);
+  for (int e = tid; e < 3 * PHL; e += PNT) {
+    const int m = k0 - 2 + e / PHL;
+    psi_at(S.phi[slot6(m)], S.psi[slot4(m)], e % PHL);
+  }
   __syncthreads();
-  for (int e = tid; e < PFL; e += PNT) F_elem(k0 - 1, e);
+  F_plane_all(k0 - 1);
   __syncthreads();
-  for (int e = tid; e < 2 * PHL; e += PNT) psi_elem(k0 + 1 + e / PHL, e % PHL);
+  for (int e = tid; e < 2 * PHL; e += PNT) {
+    const int m = k0 + 1 + e / PHL;
+    psi_at(S.phi[slot6(m)], S.psi[slot4(m)], e % PHL);
+  }
   __syncthreads();
-  for (int e = tid; e < PFL; e += PNT) F_elem(k0, e);
+  F_plane_all(k0);
+
+  // this thread's share of the per-plane task list {psi(k+3) elements, F(k+1) elements}
+  constexpr int NTASK = (PHL + PFL + PNT - 1) / PNT;
+  int tq[NTASK], tf[NTASK];  // psi task: tq = e, tf = -1; F task: tq = psi index, tf = F index
+#pragma unroll
+  for (int r = 0; r < NTASK; ++r) {
+    const int t = tid + r * PNT;
+    if (t < PHL) {
+      tq[r] = t;
+      tf[r] = -1;
+    } else if (t < PHL + PFL) {
+      const int e = t - PHL, y = e / PFX, x = e - y * PFX;
+      tq[r] = (y + 1) * PHX + (x + 1);
+      tf[r] = e;
+    } else {
+      tq[r] = -1;
+      tf[r] = -1;
+    }
+  }
 
   const double gamma = 1.0 * a.sc->gumax;
   const double mu_ = a.sc->mean[0], mv_ = a.sc->mean[1], mw_ = a.sc->mean[2];
@@ -137,28 +169,46 @@ __global__ void __launch_bounds__(PNT, 2) k_phase(PhaseArgs a) {
   const int ip = own ? wrapp(i, nx) : 0, jp = own ? wrapp(j, ny) : 0;
   const int hq = (ty + 2) * PHX + (tx + 2);  // own cell in the phi/psi plane
   const int fq = (ty + 1) * PFX + (tx + 1);  // own cell in the F plane
+  // running pointers to the own cell of plane k (and its +x, +y, +z neighbours)
+  const size_t c0 = (size_t)k0 * plane + (size_t)(own ? j : 0) * nx + (own ? i : 0);
+  const double* pu = a.u + c0;
+  const double* pv = a.v + c0;
+  const double* pw = a.w + c0;
+  const ptrdiff_t dux = (ptrdiff_t)ip - (own ? i : 0);
+  const ptrdiff_t dvy = ((ptrdiff_t)jp - (own ? j : 0)) * nx;
+  double* pphin = a.phin + c0;
+  double* prphi = a.rphio + c0;
 
   for (int k = k0; k < k1; ++k) {
     // operands from HBM for this plane, issued before the barriers
-    const size_t row = (size_t)k * plane + (size_t)(own ? j : 0) * nx;
-    const int kp = wrapp(k, nz);
+    const ptrdiff_t dwz = (k + 1 == nz) ? -(ptrdiff_t)(nz - 1) * (ptrdiff_t)plane : (ptrdiff_t)plane;
     double u0 = 0, uxp = 0, v0 = 0, vyp = 0, w0 = 0, wzp = 0, ro = 0;
     if (own) {
-      u0 = __ldg(a.u + row + i);
-      uxp = __ldg(a.u + row + ip);
-      v0 = __ldg(a.v + row + i);
-      vyp = __ldg(a.v + (size_t)k * plane + (size_t)jp * nx + i);
-      w0 = __ldg(a.w + row + i);
-      wzp = __ldg(a.w + (size_t)kp * plane + (size_t)j * nx + i);
-      ro = a.rphio[row + i];
+      u0 = __ldg(pu);
+      uxp = __ldg(pu + dux);
+      v0 = __ldg(pv);
+      vyp = __ldg(pv + dvy);
+      w0 = __ldg(pw);
+      wzp = __ldg(pw + dwz);
+      ro = *prphi;
     }
     __pipeline_wait_prior(0);
     __syncthreads();
     issue_phi(k + 4);
     __pipeline_commit();
-    for (int e = tid; e < PHL + PFL; e += PNT) {
-      if (e < PHL) psi_elem(k + 3, e);
-      else F_elem(k + 1, e - PHL);
+    {
+      const double* P3 = S.phi[slot6(k + 3)];
+      double* Q3 = S.psi[slot4(k + 3)];
+      const double* Qm = S.psi[slot4(k)];
+      const double* Q0 = S.psi[slot4(k + 1)];
+      const double* Qp = S.psi[slot4(k + 2)];
+      const double* P1 = S.phi[slot6(k + 1)];
+      double* Fd = S.F[slot3(k + 1)][0];
+#pragma unroll
+      for (int r = 0; r < NTASK; ++r) {
+        if (tf[r] >= 0) F_at(Qm, Q0, Qp, P1, Fd, tq[r], tf[r]);
+        else if (tq[r] >= 0) psi_at(P3, Q3, tq[r]);
+      }
     }
     __syncthreads();
     if (own) {
@@ -184,9 +234,14 @@ __global__ void __launch_bounds__(PNT, 2) k_phase(PhaseArgs a) {
       rhs = rhs - gamma * ((F0x[fq + 1] - F0x[fq - 1]) * 0.5 * dxi + (F0y[fq + PFX] - F0y[fq - PFX]) * 0.5 * dxi +
                            (S.F[slot3(k + 1)][2][fq] - S.F[slot3(k - 1)][2][fq]) * 0.5 * dxi);
       // :625-626
-      a.phin[row + i] = p0 + dt * (a.alpha * rhs - a.beta * ro);
-      a.rphio[row + i] = rhs;
+      *pphin = p0 + dt * (a.alpha * rhs - a.beta * ro);
+      *prphi = rhs;
     }
+    pu += plane;
+    pv += plane;
+    pw += plane;
+    pphin += plane;
+    prphi += plane;
   }
   __pipeline_wait_prior(0);
 }
