@@ -41,6 +41,8 @@ def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--input", help="input.inp to read (multi/readinput.f90 format)")
     ap.add_argument("--n", type=int, default=64)
+    ap.add_argument("--ny", type=int, help="grid points in y (default n)")
+    ap.add_argument("--nz", type=int, help="grid points in z (default n)")
     ap.add_argument("--steps", type=int, help="steps to run (default tfin - tstart)")
     ap.add_argument("--phiflag", type=int, default=0)
     ap.add_argument("--poisson", default="fp64", choices=["fp64", "fp32"])
@@ -53,7 +55,8 @@ def main(argv=None):
     args = ap.parse_args(argv)
 
     run = {"restart": 0, "tstart": 0, "tfin": 10, "dump": 10 ** 9, "inflow": 0, "inphi": 0}
-    kw = dict(nx=args.n, phiflag=args.phiflag, poisson=args.poisson, laplacian=args.laplacian, device=args.device)
+    kw = dict(nx=args.n, ny=args.ny or args.n, nz=args.nz or args.n, phiflag=args.phiflag, poisson=args.poisson,
+              laplacian=args.laplacian, device=args.device)
     if args.input:
         prm, run = api.read_input(args.input, **kw)
     else:
@@ -63,7 +66,7 @@ def main(argv=None):
     n = args.n
     phi = None
     if args.synthetic:
-        u, v, w = synth.solenoidal_velocity(n, 2)
+        u, v, w = synth.solenoidal_velocity(n, 2, ny=prm.ny, nz=prm.nz)
         if prm.phiflag:
             prm.radius, prm.sigma = 0.3, synth.sigma_from_weber(prm.rho, 1.0, 0.3, 1.0)
             phi = synth.drops_phi(n, synth.drop_centres(64, 1), prm.radius, prm.epsr * 2 * math.pi / n)
