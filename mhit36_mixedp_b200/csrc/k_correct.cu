@@ -15,40 +15,56 @@ namespace mhit {
 
 constexpr int CNT = 256;
 
+constexpr int CTX = 32, CTY = 8, CZC = 16;  // x-y tile and z chunk of k_correct
+
+// One thread per (i, j) column of the tile, marching up CZC planes: p(i,j,k-1) is carried in a
+// register from the previous plane, p(i-1,j,k) comes from the neighbouring lane, p(i,j-1,k)
+// from L1 (the row of the warp below in the same block).
 template <typename T>
 __global__ void __launch_bounds__(CNT) k_correct(CorrectArgs a) {
   const Geo& g = a.g;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
-  const size_t ntot = (size_t)nx * ny * nz;
+  const size_t plane = (size_t)nx * ny;
   const T* __restrict__ p = static_cast<const T*>(a.p);
   const double cc = g.dt / g.rho, dxi = g.dxi;
+  const int lane = threadIdx.x, ty = threadIdx.y;
+  const int i = blockIdx.x * CTX + lane, j = blockIdx.y * CTY + ty;
+  const int k0 = blockIdx.z * CZC, k1 = min(k0 + CZC, nz);
+  const bool own = i < nx && j < ny;
+  const int ic = own ? i : 0, jc = own ? j : 0;
+  const int im = wrapm(ic, nx), jm = wrapm(jc, ny);
   double su = 0.0, sv = 0.0, sw = 0.0;
   double mu = -INFINITY, mv = -INFINITY, mw = -INFINITY;
-  const size_t stride = (size_t)gridDim.x * CNT;
-  for (size_t c = (size_t)blockIdx.x * CNT + threadIdx.x; c < ntot; c += stride) {
-    const int i = (int)(c % nx);
-    const size_t r = c / nx;
-    const int j = (int)(r % ny), k = (int)(r / ny);
+  size_t c = (size_t)k0 * plane + (size_t)jc * nx + ic;
+  const ptrdiff_t dxm = (ptrdiff_t)im - ic, dym = ((ptrdiff_t)jm - jc) * nx;
+  double pkm = (double)p[(size_t)wrapm(k0, nz) * plane + (size_t)jc * nx + ic];
+  for (int k = k0; k < k1; ++k, c += plane) {
     const double pc = (double)p[c];
-    const double pxm = (double)p[c - i + wrapm(i, nx)];
-    const double pym = (double)p[lin(i, wrapm(j, ny), k, nx, ny)];
-    const double pzm = (double)p[lin(i, j, wrapm(k, nz), nx, ny)];
-    const double uu = a.u[c] - cc * (pc - pxm) * dxi;
-    const double vv = a.v[c] - cc * (pc - pym) * dxi;
-    const double ww = a.w[c] - cc * (pc - pzm) * dxi;
-    a.u[c] = uu;
-    a.v[c] = vv;
-    a.w[c] = ww;
-    su += uu;
-    sv += vv;
-    sw += ww;
-    mu = fmax(mu, uu);
-    mv = fmax(mv, vv);
-    mw = fmax(mw, ww);
+    double pxm = __shfl_up_sync(0xffffffffu, pc, 1);
+    if (lane == 0 || nx < CTX) pxm = (double)p[c + dxm];
+    const double pym = (double)p[c + dym];
+    const double uo = a.u[c], vo = a.v[c], wo = a.w[c];
+    // multi/main.f90:953-955
+    const double uu = uo - cc * (pc - pxm) * dxi;
+    const double vv = vo - cc * (pc - pym) * dxi;
+    const double ww = wo - cc * (pc - pkm) * dxi;
+    pkm = pc;
+    if (own) {
+      a.u[c] = uu;
+      a.v[c] = vv;
+      a.w[c] = ww;
+      su += uu;
+      sv += vv;
+      sw += ww;
+      mu = fmax(mu, uu);
+      mv = fmax(mv, vv);
+      mw = fmax(mw, ww);
+    }
   }
   // block reduction (fixed tree)
   __shared__ double red[6][CNT / 32];
   double vals[6] = {su, sv, sw, mu, mv, mw};
+  const int t = ty * CTX + lane;
 #pragma unroll
   for (int q = 0; q < 6; ++q) {
     double x = vals[q];
@@ -57,14 +73,14 @@ __global__ void __launch_bounds__(CNT) k_correct(CorrectArgs a) {
       const double y = __shfl_down_sync(0xffffffffu, x, o);
       x = q < 3 ? x + y : fmax(x, y);
     }
-    if ((threadIdx.x & 31) == 0) red[q][threadIdx.x >> 5] = x;
+    if (lane == 0) red[q][t >> 5] = x;
   }
   __syncthreads();
-  if (threadIdx.x < 6) {
-    const int q = threadIdx.x;
-    double x = red[q][0];
-    for (int wv = 1; wv < CNT / 32; ++wv) x = q < 3 ? x + red[q][wv] : fmax(x, red[q][wv]);
-    a.partials[(size_t)blockIdx.x * 6 + q] = x;
+  if (t < 6) {
+    double x = red[t][0];
+    for (int wv = 1; wv < CNT / 32; ++wv) x = t < 3 ? x + red[t][wv] : fmax(x, red[t][wv]);
+    const size_t bid = ((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+    a.partials[bid * 6 + t] = x;
   }
 }
 
@@ -115,16 +131,19 @@ __global__ void __launch_bounds__(1024) k_finalize(const double* __restrict__ pa
   }
 }
 
+static dim3 correct_grid(const Geo& g) {
+  return dim3((g.nx + CTX - 1) / CTX, (g.ny + CTY - 1) / CTY, (g.nz + CZC - 1) / CZC);
+}
+
 int correct_blocks(const Geo& g) {
-  const size_t n = (size_t)g.nx * g.ny * g.nz;
-  size_t b = (n + CNT * 4 - 1) / (CNT * 4);
-  const size_t cap = 148 * 8;
-  return (int)(b < cap ? (b < 1 ? 1 : b) : cap);
+  const dim3 d = correct_grid(g);
+  return (int)(d.x * d.y * d.z);
 }
 
 cudaError_t launch_correct(const CorrectArgs& a, cudaStream_t st) {
-  if (a.fp32) k_correct<float><<<a.nblocks, CNT, 0, st>>>(a);
-  else k_correct<double><<<a.nblocks, CNT, 0, st>>>(a);
+  const dim3 grd = correct_grid(a.g), blk(CTX, CTY);
+  if (a.fp32) k_correct<float><<<grd, blk, 0, st>>>(a);
+  else k_correct<double><<<grd, blk, 0, st>>>(a);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   k_finalize<<<1, 1024, 0, st>>>(a.partials, a.nblocks, a.g, a.sc);

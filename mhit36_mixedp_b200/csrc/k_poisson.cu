@@ -12,6 +12,8 @@
 // every tile row starts on a 128-byte boundary.  Half-length real transforms: the x line of
 // nx reals is packed as nx/2 complex (even + i*odd), transformed, and untangled with the
 // exp(-2 pi i k/nx) twiddles (and the mirror image for C2R).
+#include <cuda_pipeline.h>
+
 #include "common.cuh"
 #include "fft_core.cuh"
 #include "kernels.h"
@@ -45,13 +47,12 @@ k_div_fftx(const double* __restrict__ u, const double* __restrict__ v, const dou
   const int nlines = ny * nz;
   const int line0 = blockIdx.x * B;
 
+#pragma unroll 4
   for (int e = threadIdx.x; e < M * B; e += NT) {
     const int b = e / M, n = e - b * M;
-    const int line = line0 + b;
+    const int line = min(line0 + b, nlines - 1);  // a tail tile repeats the last line
     Cx<T> z;
-    z.x = (T)0;
-    z.y = (T)0;
-    if (line < nlines) {
+    {
       const int k = line / ny, j = line - k * ny;
       const int jp = wrapp(j, ny), kp = wrapp(k, nz);
       const int i = 2 * n;
@@ -127,13 +128,11 @@ k_fftx_inv(const Cx<T>* __restrict__ spec, T* __restrict__ p, const Cx<T>* __res
   const int pitch = g.pitch;
   for (int e = threadIdx.x; e < (M + 1) * B; e += NT) {
     const int b = e / (M + 1), kx = e - b * (M + 1);
-    const int line = line0 + b;
-    Cx<T> z;
-    z.x = (T)0;
-    z.y = (T)0;
-    if (line < nlines) z = spec[(size_t)line * pitch + kx];
-    s[sw<B>(kx, b)] = z;
+    const int line = min(line0 + b, nlines - 1);  // a tail tile repeats the last line
+    __pipeline_memcpy_async(&s[sw<B>(kx, b)], &spec[(size_t)line * pitch + kx], sizeof(Cx<T>));
   }
+  __pipeline_commit();
+  __pipeline_wait_prior(0);
   __syncthreads();
   // Z[k] = (X[k] + X*[M-k]) + i W^-k (X[k] - X*[M-k]); imaginary parts of X[0], X[M] ignored
   for (int e = threadIdx.x; e < (M / 2 + 1) * B; e += NT) {
@@ -185,18 +184,19 @@ k_fft_cols(Cx<T>* __restrict__ spec, const Cx<T>* __restrict__ tw, Geo g, size_t
   const int outer = blockIdx.y;
   const int nkx = g.nkx;
   Cx<T>* base = spec + (size_t)outer * stride_outer + kx0;
+  // The row pitch is a multiple of 16 complex and the padding columns stay zero, so every
+  // B-wide tile is in bounds: all loads of the tile go out back to back as async copies.
   for (int e = threadIdx.x; e < N * B; e += NT) {
     const int n = e / B, b = e - n * B;
-    Cx<T> z;
-    z.x = (T)0;
-    z.y = (T)0;
-    if (kx0 + b < nkx) z = base[(size_t)n * stride_n + b];
-    s[sw<B>(n, b)] = z;
+    __pipeline_memcpy_async(&s[sw<B>(n, b)], &base[(size_t)n * stride_n + b], sizeof(Cx<T>));
   }
+  __pipeline_commit();
+  __pipeline_wait_prior(0);
   __syncthreads();
   fft_tile<T, N, B, NT, MODE == 1>(s, tw, 1);
   if constexpr (MODE == 2) {
-    // multi/main.f90:889-895: phi3d = -phi3d/k2/(nx*ny*nz) in FP64, phi3d(1,1,1) = 0
+    // multi/main.f90:889-895: phi3d = -phi3d/k2/(nx*ny*nz) in FP64, phi3d(1,1,1) = 0.
+    // One reciprocal of k2*N per element (within 2 ulp of the reference's two divides).
     const double ky2 = k2y[outer];
     for (int e = threadIdx.x; e < N * B; e += NT) {
       const int n = e / B, b = e - n * B;
@@ -204,8 +204,9 @@ k_fft_cols(Cx<T>* __restrict__ spec, const Cx<T>* __restrict__ tw, Geo g, size_t
       if (kx < nkx) {
         const double k2 = (k2x[kx] + ky2) + k2z[n];
         const Cx<T> z = s[sw<B>(n, b)];
-        double re = (-(double)z.x) / k2 / ntot;
-        double im = (-(double)z.y) / k2 / ntot;
+        const double inv = 1.0 / (k2 * ntot);
+        double re = -(double)z.x * inv;
+        double im = -(double)z.y * inv;
         if (kx == 0 && outer == 0 && n == 0) { re = 0.0; im = 0.0; }
         s[sw<B>(n, b)] = cx<T>((T)re, (T)im);
       }
