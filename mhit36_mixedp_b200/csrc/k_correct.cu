@@ -15,56 +15,90 @@ namespace mhit {
 
 constexpr int CNT = 256;
 
-constexpr int CTX = 32, CTY = 8, CZC = 16;  // x-y tile and z chunk of k_correct
+constexpr int CTX = 32, CTY = 16, CZC = 16;  // x-y tile and z chunk of k_correct
 
-// One thread per (i, j) column of the tile, marching up CZC planes: p(i,j,k-1) is carried in a
-// register from the previous plane, p(i-1,j,k) comes from the neighbouring lane, p(i,j-1,k)
-// from L1 (the row of the warp below in the same block).
+template <typename T> struct Pair;
+template <> struct Pair<double> {
+  using V = double2;
+};
+template <> struct Pair<float> {
+  using V = float2;
+};
+
+// Each thread owns two adjacent x cells (16-byte loads of u, v, w) of one tile row and marches
+// up CZC planes two at a time: p(k-1) is carried in registers from the previous plane,
+// p(i-1) comes from the neighbouring lane of the 16-lane row, p(j-1) from L1.
 template <typename T>
 __global__ void __launch_bounds__(CNT) k_correct(CorrectArgs a) {
+  using PV = typename Pair<T>::V;
   const Geo& g = a.g;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const size_t plane = (size_t)nx * ny;
   const T* __restrict__ p = static_cast<const T*>(a.p);
+  double* __restrict__ U = a.u;
+  double* __restrict__ V = a.v;
+  double* __restrict__ W = a.w;
   const double cc = g.dt / g.rho, dxi = g.dxi;
-  const int lane = threadIdx.x, ty = threadIdx.y;
-  const int i = blockIdx.x * CTX + lane, j = blockIdx.y * CTY + ty;
+  const int lx = threadIdx.x & 15, ty = threadIdx.x >> 4;  // 16 lanes x 16 rows
+  const int i = blockIdx.x * CTX + 2 * lx, j = blockIdx.y * CTY + ty;
   const int k0 = blockIdx.z * CZC, k1 = min(k0 + CZC, nz);
   const bool own = i < nx && j < ny;
   const int ic = own ? i : 0, jc = own ? j : 0;
   const int im = wrapm(ic, nx), jm = wrapm(jc, ny);
+  const bool edge = (lx == 0) || (nx < CTX);
   double su = 0.0, sv = 0.0, sw = 0.0;
   double mu = -INFINITY, mv = -INFINITY, mw = -INFINITY;
-  size_t c = (size_t)k0 * plane + (size_t)jc * nx + ic;
-  const ptrdiff_t dxm = (ptrdiff_t)im - ic, dym = ((ptrdiff_t)jm - jc) * nx;
-  double pkm = (double)p[(size_t)wrapm(k0, nz) * plane + (size_t)jc * nx + ic];
-  for (int k = k0; k < k1; ++k, c += plane) {
-    const double pc = (double)p[c];
-    double pxm = __shfl_up_sync(0xffffffffu, pc, 1);
-    if (lane == 0 || nx < CTX) pxm = (double)p[c + dxm];
-    const double pym = (double)p[c + dym];
-    const double uo = a.u[c], vo = a.v[c], wo = a.w[c];
+  const size_t r0 = (size_t)jc * nx + ic;
+  const ptrdiff_t dym = ((ptrdiff_t)jm - jc) * nx;
+  PV pk = *reinterpret_cast<const PV*>(p + (size_t)wrapm(k0, nz) * plane + r0);
+  double pkm0 = (double)pk.x, pkm1 = (double)pk.y;
+  auto plane_step = [&](size_t c, const PV pc2, const PV py2, const T pxm_edge, const double2 uo, const double2 vo,
+                        const double2 wo) {
+    const double pc0 = (double)pc2.x, pc1 = (double)pc2.y;
+    double pxm0 = __shfl_up_sync(0xffffffffu, pc1, 1, 16);
+    if (edge) pxm0 = (double)pxm_edge;
     // multi/main.f90:953-955
-    const double uu = uo - cc * (pc - pxm) * dxi;
-    const double vv = vo - cc * (pc - pym) * dxi;
-    const double ww = wo - cc * (pc - pkm) * dxi;
-    pkm = pc;
+    const double u0 = uo.x - cc * (pc0 - pxm0) * dxi, u1 = uo.y - cc * (pc1 - pc0) * dxi;
+    const double v0 = vo.x - cc * (pc0 - (double)py2.x) * dxi, v1 = vo.y - cc * (pc1 - (double)py2.y) * dxi;
+    const double w0 = wo.x - cc * (pc0 - pkm0) * dxi, w1 = wo.y - cc * (pc1 - pkm1) * dxi;
+    pkm0 = pc0;
+    pkm1 = pc1;
     if (own) {
-      a.u[c] = uu;
-      a.v[c] = vv;
-      a.w[c] = ww;
-      su += uu;
-      sv += vv;
-      sw += ww;
-      mu = fmax(mu, uu);
-      mv = fmax(mv, vv);
-      mw = fmax(mw, ww);
+      *reinterpret_cast<double2*>(U + c) = make_double2(u0, u1);
+      *reinterpret_cast<double2*>(V + c) = make_double2(v0, v1);
+      *reinterpret_cast<double2*>(W + c) = make_double2(w0, w1);
+      su += u0 + u1;
+      sv += v0 + v1;
+      sw += w0 + w1;
+      mu = fmax(mu, fmax(u0, u1));
+      mv = fmax(mv, fmax(v0, v1));
+      mw = fmax(mw, fmax(w0, w1));
     }
+  };
+  int k = k0;
+  for (; k + 1 < k1; k += 2) {
+    const size_t ca = (size_t)k * plane + r0, cb = ca + plane;
+    const PV pa = *reinterpret_cast<const PV*>(p + ca), pb = *reinterpret_cast<const PV*>(p + cb);
+    const PV ya = *reinterpret_cast<const PV*>(p + ca + dym), yb = *reinterpret_cast<const PV*>(p + cb + dym);
+    const T xa = edge ? p[ca - ic + im] : (T)0, xb = edge ? p[cb - ic + im] : (T)0;
+    const double2 ua = *reinterpret_cast<const double2*>(U + ca), ub = *reinterpret_cast<const double2*>(U + cb);
+    const double2 va = *reinterpret_cast<const double2*>(V + ca), vb = *reinterpret_cast<const double2*>(V + cb);
+    const double2 wa = *reinterpret_cast<const double2*>(W + ca), wb = *reinterpret_cast<const double2*>(W + cb);
+    plane_step(ca, pa, ya, xa, ua, va, wa);
+    plane_step(cb, pb, yb, xb, ub, vb, wb);
+  }
+  if (k < k1) {
+    const size_t ca = (size_t)k * plane + r0;
+    const PV pa = *reinterpret_cast<const PV*>(p + ca);
+    const PV ya = *reinterpret_cast<const PV*>(p + ca + dym);
+    const T xa = edge ? p[ca - ic + im] : (T)0;
+    plane_step(ca, pa, ya, xa, *reinterpret_cast<const double2*>(U + ca), *reinterpret_cast<const double2*>(V + ca),
+               *reinterpret_cast<const double2*>(W + ca));
   }
   // block reduction (fixed tree)
   __shared__ double red[6][CNT / 32];
   double vals[6] = {su, sv, sw, mu, mv, mw};
-  const int t = ty * CTX + lane;
+  const int t = threadIdx.x, lane = t & 31;
 #pragma unroll
   for (int q = 0; q < 6; ++q) {
     double x = vals[q];
@@ -141,7 +175,7 @@ int correct_blocks(const Geo& g) {
 }
 
 cudaError_t launch_correct(const CorrectArgs& a, cudaStream_t st) {
-  const dim3 grd = correct_grid(a.g), blk(CTX, CTY);
+  const dim3 grd = correct_grid(a.g), blk(CNT);
   if (a.fp32) k_correct<float><<<grd, blk, 0, st>>>(a);
   else k_correct<double><<<grd, blk, 0, st>>>(a);
   cudaError_t e = cudaGetLastError();

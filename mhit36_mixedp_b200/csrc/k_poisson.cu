@@ -47,7 +47,6 @@ k_div_fftx(const double* __restrict__ u, const double* __restrict__ v, const dou
   const int nlines = ny * nz;
   const int line0 = blockIdx.x * B;
 
-#pragma unroll 4
   for (int e = threadIdx.x; e < M * B; e += NT) {
     const int b = e / M, n = e - b * M;
     const int line = min(line0 + b, nlines - 1);  // a tail tile repeats the last line
