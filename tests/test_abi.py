@@ -29,6 +29,41 @@ def test_library_exports_every_declared_symbol():
     assert set(names) <= set(_lib.SIGNATURES), set(names) - set(_lib.SIGNATURES)
 
 
+def struct_fields(src, name):
+    body = re.search(r"typedef struct %s \{(.*?)\} %s;" % (name, name), src, flags=re.S).group(1)
+    body = re.sub(r"/\*.*?\*/", "", body, flags=re.S)
+    out = []
+    for decl in body.split(";"):
+        decl = decl.strip()
+        if not decl:
+            continue
+        names = decl.split(None, 1)[1] if not decl.startswith("long long") else decl.split(None, 2)[2]
+        for n in names.split(","):
+            out.append(re.sub(r"\[.*\]", "", n).strip())
+    return out
+
+
+def test_ctypes_structs_match_header():
+    src = open(HEADER).read()
+    assert struct_fields(src, "mhit_params") == [f for f, _ in _lib.MhitParams._fields_]
+    assert struct_fields(src, "mhit_run") == [f for f, _ in _lib.MhitRun._fields_]
+    assert struct_fields(src, "mhit_diag") == [f for f, _ in _lib.MhitDiag._fields_]
+
+
+def test_fortran_module_matches_header():
+    f90 = open(os.path.join(ROOT, "mhit36_mixedp_b200", "fortran", "mhit_gpu.f90")).read()
+    body = re.search(r"type, bind\(C\) :: mhit_params(.*?)end type", f90, flags=re.S).group(1)
+    names = []
+    for line in body.splitlines():
+        if "::" in line:
+            names += [n.strip() for n in line.split("::")[1].split(",")]
+    assert names == [f for f, _ in _lib.MhitParams._fields_]
+    # every C entry point used by a Fortran host is bound
+    for fn in ("mhit_init", "mhit_step", "mhit_upload_fields", "mhit_download_fields", "mhit_read_input",
+               "mhit_write_field", "mhit_read_field", "mhit_diagnostics", "mhit_destroy"):
+        assert f'name="{fn}"' in f90, fn
+
+
 def test_abi_version():
     assert api.abi_version() == 1
 
