@@ -176,6 +176,23 @@ int mhit_profile_step(mhit_ctx* ctx, double* ms, const char** names, int* nstage
 #define MHIT_BUF_RW 11
 #define MHIT_BUF_RPHI 12
 #define MHIT_BUF_SPEC 13
+/* No-allocation field statistics.  This entry point has no counterpart in the reference.
+ * For callers that cannot let the library allocate device memory -- a host whose device arrays
+ * belong to its own runtime (OpenACC / CUDA Fortran) and only wants statistics of fields it
+ * already holds, or a run with the GPU's memory nearly fully committed, where an extra cudaMalloc
+ * can fail and a cudaFree synchronises the device.  Computes, from caller-owned device arrays
+ * u, v, w (x-fastest nx*ny*nz float64), stats[0] = max|div u|, stats[1] = KE = 0.5 <u.u>,
+ * stats[2] = 2 nu <S_ij S_ij> -- the same quantities as mhit_diagnostics -- into the caller's
+ * device array stats[3], on `stream` (a cudaStream_t, NULL for the default stream).
+ * It calls no cudaMalloc/cudaFree: its only scratch is a file-scope device array with one slot
+ * per z plane, so nz may not exceed MHIT_STATS_NOALLOC_MAX_PLANES (MHIT_ERR_ARG otherwise).
+ * The first call on a device looks up that array's device address (cudaGetSymbolAddress, no
+ * allocation); make that first call before any stream capture.  All calls share the array:
+ * calls whose kernels overlap on the GPU race and must be serialised by the caller. */
+#define MHIT_STATS_NOALLOC_MAX_PLANES 1024
+int mhit_field_stats_noalloc(int nx, int ny, int nz, double nu, const double* u, const double* v, const double* w,
+                             double* stats, void* stream);
+
 int mhit_debug_run_stage(mhit_ctx* ctx, int stage);
 int mhit_debug_commit_step(mhit_ctx* ctx);
 long long mhit_debug_buffer_len(mhit_ctx* ctx, int which);

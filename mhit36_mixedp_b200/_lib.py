@@ -70,6 +70,8 @@ SIGNATURES = {
     "mhit_read_field": (_c.c_int, [_c.c_void_p, _c.c_char_p, _c.c_int]),
     "mhit_time_steps": (_c.c_int, [_c.c_void_p, _c.c_int, _dp]),
     "mhit_profile_step": (_c.c_int, [_c.c_void_p, _dp, _P(_c.c_char_p), _P(_c.c_int)]),
+    "mhit_field_stats_noalloc": (_c.c_int, [_c.c_int, _c.c_int, _c.c_int, _c.c_double, _c.c_void_p, _c.c_void_p,
+                                            _c.c_void_p, _c.c_void_p, _c.c_void_p]),
     "mhit_debug_run_stage": (_c.c_int, [_c.c_void_p, _c.c_int]),
     "mhit_debug_commit_step": (_c.c_int, [_c.c_void_p]),
     "mhit_debug_buffer_len": (_c.c_longlong, [_c.c_void_p, _c.c_int]),
