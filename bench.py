@@ -44,6 +44,13 @@ BYTES_PER_POINT = {
     "fp64": {"k_phase": 56, "k_mom": 104, "k_div_fftx": 32, "k_fft_cols_yfwd": 16, "k_fft_cols_zsolve": 16,
              "k_fft_cols_yinv": 16, "k_fftx_inv": 16, "k_correct+k_finalize": 56},
 }
+# DRAM bytes per grid point and launch measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum
+# of one launch / cells): k_phase, k_mom from profiles/k_phase_k_mom_ns_acdi_256.md (256^3); the
+# Poisson and projection kernels from profiles/poisson_projection_fp32_512x512x256.md.  Traffic
+# scales with the cell count for these streaming kernels, so a launch at 512^3 moves 8x the bytes.
+TRAFFIC_PER_POINT = {"k_phase": 56.1, "k_mom": 104.5, "k_div_fftx": 28.4, "k_fft_cols_yfwd": 7.5,
+                     "k_fft_cols_zsolve": 7.5, "k_fft_cols_yinv": 7.5, "k_fftx_inv": 7.5,
+                     "k_correct+k_finalize": 51.2}
 # the step-level model: NS+ACDI 256 B/pt (FP32 Poisson), 280 B/pt (FP64)
 STEP_BYTES = {"fp32": 256, "fp64": 280}
 
@@ -263,14 +270,8 @@ def main():
         dom_bytes = BYTES_PER_POINT["fp32"][dom] * npts
         achieved = dom_bytes / (st[dom] * 1e-3) / 1e9
         traffic = None
-        tpath = os.path.join(ROOT, "profiles", "traffic_per_point.json")
-        if os.path.exists(tpath):
-            try:
-                tj = json.load(open(tpath))
-                if dom in tj:
-                    traffic = tj[dom] * npts
-            except Exception:
-                traffic = None
+        if dom in TRAFFIC_PER_POINT:
+            traffic = TRAFFIC_PER_POINT[dom] * npts
         roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                 "algorithmic_bytes_per_launch": dom_bytes, "launch_ms": st[dom]}
