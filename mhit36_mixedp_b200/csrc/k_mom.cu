@@ -14,9 +14,9 @@
 // so every input byte crosses HBM once (plus the x/y halo re-read from L2) and the chemical
 // potential is evaluated once per cell.
 //
-// The velocity read here is the stored one minus the running mean of the previous
-// projection (DevScalars::mean); subtracting on read is exactly the reference's
-// u = u - gumean (:977-981) done lazily.
+// The velocity used here is the stored one minus the running mean of the previous projection
+// (DevScalars::mean), subtracted once per shared-memory element; this is exactly the
+// reference's u = u - gumean (:977-981) done lazily.
 #include <cuda_pipeline.h>
 
 #include "common.cuh"
@@ -45,9 +45,9 @@ template <> struct MomSmem<true> {
   double cp[2][CPL];
 };
 
-__device__ __forceinline__ int wrap_small(int x, int n) {
-  // x in [-n, 2n)
-  return x < 0 ? x + n : (x >= n ? x - n : x);
+__device__ __forceinline__ int pmod_int(int x, int n) {
+  x %= n;
+  return x < 0 ? x + n : x;
 }
 
 template <bool PHI>
@@ -70,7 +70,7 @@ __global__ void __launch_bounds__(MNT, 3) k_mom(MomArgs a) {
     uoff[c] = -1;
     if (e < UPL) {
       const int y = e / UPX, x = e - y * UPX;
-      uoff[c] = wrap_small(j0 - 1 + y, ny) * nx + wrap_small(i0 - 1 + x, nx);
+      uoff[c] = pmod_int(j0 - 1 + y, ny) * nx + pmod_int(i0 - 1 + x, nx);
     }
   }
 #pragma unroll
@@ -79,11 +79,11 @@ __global__ void __launch_bounds__(MNT, 3) k_mom(MomArgs a) {
     poff[c] = -1;
     if (PHI && e < PPL) {
       const int y = e / PPX, x = e - y * PPX;
-      poff[c] = wrap_small(j0 - 2 + y, ny) * nx + wrap_small(i0 - 2 + x, nx);
+      poff[c] = pmod_int(j0 - 2 + y, ny) * nx + pmod_int(i0 - 2 + x, nx);
     }
   }
   auto issue_plane = [&](int m) {
-    const int kw = wrap_small(m, nz);
+    const int kw = pmod_int(m, nz);
     const size_t base = (size_t)kw * plane;
     const int su = (m - k0 + 8) & 3;
 #pragma unroll
@@ -110,7 +110,7 @@ __global__ void __launch_bounds__(MNT, 3) k_mom(MomArgs a) {
   // phi ring only (planes k0-2 .. k0-1 before the u ring starts)
   auto issue_phi = [&](int m) {
     if constexpr (PHI) {
-      const int kw = wrap_small(m, nz);
+      const int kw = pmod_int(m, nz);
       const size_t base = (size_t)kw * plane;
       const int sp = (m - k0 + 10) % 5;
 #pragma unroll
@@ -142,16 +142,34 @@ __global__ void __launch_bounds__(MNT, 3) k_mom(MomArgs a) {
     }
   };
 
+  // The lazily removed mean of the last projection is subtracted once per shared-memory
+  // element, by the thread that copied it, right after its copy landed.
+  const double mu_ = a.sc->mean[0], mv_ = a.sc->mean[1], mw_ = a.sc->mean[2];
+  auto fix_mean = [&](int m) {
+    const int su = (m - k0 + 8) & 3;
+#pragma unroll
+    for (int c = 0; c < UCP; ++c) {
+      if (uoff[c] >= 0) {
+        const int e = tid + c * MNT;
+        S.u[su][e] = S.u[su][e] - mu_;
+        S.v[su][e] = S.v[su][e] - mv_;
+        S.w[su][e] = S.w[su][e] - mw_;
+      }
+    }
+  };
+
   // prologue: phi k0-2, k0-1; u/v/w + phi k0-1, k0, k0+1
   issue_phi(k0 - 2);
   issue_plane(k0 - 1);
   issue_plane(k0);
   issue_plane(k0 + 1);
   __pipeline_wait_prior(0);
+  fix_mean(k0 - 1);
+  fix_mean(k0);
+  fix_mean(k0 + 1);
   __syncthreads();
   chempot_plane(k0 - 1);
 
-  const double mu_ = a.sc->mean[0], mv_ = a.sc->mean[1], mw_ = a.sc->mean[2];
   const int tx = tid % MTX, ty = tid / MTX;
   const int i = i0 + tx, j = j0 + ty;
   const bool own = i < nx && j < ny;
@@ -159,6 +177,8 @@ __global__ void __launch_bounds__(MNT, 3) k_mom(MomArgs a) {
   const double sxi = own ? __ldg(t + i) : 0.0, cxi = own ? __ldg(t + nx + i) : 0.0;
   const double syj = own ? __ldg(t + 2 * nx + j) : 0.0, cyj = own ? __ldg(t + 2 * nx + ny + j) : 0.0;
   const double mu = g.mu, rhoi = g.rhoi, dt = g.dt, al = a.alpha, be = a.beta;
+  // (h*0.25)*dxi == h*(0.25*dxi) exactly: scaling by 0.25 does not round
+  const double q4 = 0.25 * dxi;
   const int uq = (ty + 1) * UPX + (tx + 1);   // own cell in the u/v/w plane
   const int pq = (ty + 2) * PPX + (tx + 2);   // own cell in the phi plane
   const int cq = (ty + 1) * CPX + (tx + 1);   // own cell in the chempot plane
@@ -173,6 +193,7 @@ __global__ void __launch_bounds__(MNT, 3) k_mom(MomArgs a) {
     }
     // plane k+1 landed (issued one iteration ago); everyone is done with iteration k-1
     __pipeline_wait_prior(0);
+    fix_mean(k + 1);
     __syncthreads();
     issue_plane(k + 2);
     chempot_plane(k);
@@ -182,28 +203,28 @@ __global__ void __launch_bounds__(MNT, 3) k_mom(MomArgs a) {
       const double* U0 = S.u[s0];
       const double* V0 = S.v[s0];
       const double* W0 = S.w[s0];
-      const double u0 = U0[uq] - mu_, v0 = V0[uq] - mv_, w0 = W0[uq] - mw_;
-      const double uxp = U0[uq + 1] - mu_, uxm = U0[uq - 1] - mu_, uyp = U0[uq + UPX] - mu_, uym = U0[uq - UPX] - mu_;
-      const double uzp = S.u[sp][uq] - mu_, uzm = S.u[sm][uq] - mu_;
-      const double vxp = V0[uq + 1] - mv_, vxm = V0[uq - 1] - mv_, vyp = V0[uq + UPX] - mv_, vym = V0[uq - UPX] - mv_;
-      const double vzp = S.v[sp][uq] - mv_, vzm = S.v[sm][uq] - mv_;
-      const double wxp = W0[uq + 1] - mw_, wxm = W0[uq - 1] - mw_, wyp = W0[uq + UPX] - mw_, wym = W0[uq - UPX] - mw_;
-      const double wzp = S.w[sp][uq] - mw_, wzm = S.w[sm][uq] - mw_;
-      const double v_imjp = V0[uq + UPX - 1] - mv_, w_imkp = S.w[sp][uq - 1] - mw_, u_ipjm = U0[uq - UPX + 1] - mu_;
-      const double w_jmkp = S.w[sp][uq - UPX] - mw_, u_ipkm = S.u[sm][uq + 1] - mu_, v_jpkm = S.v[sm][uq + UPX] - mv_;
+      const double u0 = U0[uq], v0 = V0[uq], w0 = W0[uq];
+      const double uxp = U0[uq + 1], uxm = U0[uq - 1], uyp = U0[uq + UPX], uym = U0[uq - UPX];
+      const double uzp = S.u[sp][uq], uzm = S.u[sm][uq];
+      const double vxp = V0[uq + 1], vxm = V0[uq - 1], vyp = V0[uq + UPX], vym = V0[uq - UPX];
+      const double vzp = S.v[sp][uq], vzm = S.v[sm][uq];
+      const double wxp = W0[uq + 1], wxm = W0[uq - 1], wyp = W0[uq + UPX], wym = W0[uq - UPX];
+      const double wzp = S.w[sp][uq], wzm = S.w[sm][uq];
+      const double v_imjp = V0[uq + UPX - 1], w_imkp = S.w[sp][uq - 1], u_ipjm = U0[uq - UPX + 1];
+      const double w_jmkp = S.w[sp][uq - UPX], u_ipkm = S.u[sm][uq + 1], v_jpkm = S.v[sm][uq + UPX];
       // multi/main.f90:672-694
       double h11 = (uxp + u0) * (uxp + u0) - (u0 + uxm) * (u0 + uxm);
       double h12 = (uyp + u0) * (vyp + v_imjp) - (u0 + uym) * (v0 + vxm);
       double h13 = (uzp + u0) * (wzp + w_imkp) - (u0 + uzm) * (w0 + wxm);
-      double ru = -(h11 * 0.25 * dxi + h12 * 0.25 * dxi + h13 * 0.25 * dxi);
+      double ru = -(h11 * q4 + h12 * q4 + h13 * q4);
       double h21 = (uxp + u_ipjm) * (vxp + v0) - (u0 + uym) * (v0 + vxm);
       double h22 = (vyp + v0) * (vyp + v0) - (v0 + vym) * (v0 + vym);
       double h23 = (wzp + w_jmkp) * (vzp + v0) - (w0 + wym) * (v0 + vzm);
-      double rv = -(h21 * 0.25 * dxi + h22 * 0.25 * dxi + h23 * 0.25 * dxi);
+      double rv = -(h21 * q4 + h22 * q4 + h23 * q4);
       double h31 = (wxp + w0) * (uxp + u_ipkm) - (w0 + wxm) * (u0 + uzm);
       double h32 = (vyp + v_jpkm) * (wyp + w0) - (v0 + vzm) * (w0 + wym);
       double h33 = (wzp + w0) * (wzp + w0) - (w0 + wzm) * (w0 + wzm);
-      double rw = -(h31 * 0.25 * dxi + h32 * 0.25 * dxi + h33 * 0.25 * dxi);
+      double rw = -(h31 * q4 + h32 * q4 + h33 * q4);
       // :696-707
       ru = ru + (mu * (uxp - 2.0 * u0 + uxm) * ddxi + mu * (uyp - 2.0 * u0 + uym) * ddxi +
                  mu * (uzp - 2.0 * u0 + uzm) * ddxi) * rhoi;

@@ -163,6 +163,7 @@ __global__ void __launch_bounds__(PNT, 2) k_phase(PhaseArgs a) {
   const double gamma = 1.0 * a.sc->gumax;
   const double mu_ = a.sc->mean[0], mv_ = a.sc->mean[1], mw_ = a.sc->mean[2];
   const double dxi = g.dxi, ddxi = g.ddxi, dt = g.dt;
+  const double hdxi = 0.5 * dxi;  // (x*0.5)*dxi == x*(0.5*dxi) exactly
   const int tx = tid % PTX, ty = tid / PTX;
   const int i = i0 + tx, j = j0 + ty;
   const bool own = (i < nx) && (j < ny);
@@ -231,8 +232,8 @@ __global__ void __launch_bounds__(PNT, 2) k_phase(PhaseArgs a) {
       // :609-614
       const double* F0x = S.F[slot3(k)][0];
       const double* F0y = S.F[slot3(k)][1];
-      rhs = rhs - gamma * ((F0x[fq + 1] - F0x[fq - 1]) * 0.5 * dxi + (F0y[fq + PFX] - F0y[fq - PFX]) * 0.5 * dxi +
-                           (S.F[slot3(k + 1)][2][fq] - S.F[slot3(k - 1)][2][fq]) * 0.5 * dxi);
+      rhs = rhs - gamma * ((F0x[fq + 1] - F0x[fq - 1]) * hdxi + (F0y[fq + PFX] - F0y[fq - PFX]) * hdxi +
+                           (S.F[slot3(k + 1)][2][fq] - S.F[slot3(k - 1)][2][fq]) * hdxi);
       // :625-626
       *pphin = p0 + dt * (a.alpha * rhs - a.beta * ro);
       *prphi = rhs;

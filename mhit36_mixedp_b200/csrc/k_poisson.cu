@@ -32,15 +32,16 @@ template <> __device__ __forceinline__ void store2<float>(float* p, float a, flo
   *reinterpret_cast<float2*>(p) = make_float2(a, b);
 }
 
-constexpr int XPASS_THREADS = 256;
+// x-pass threads: one butterfly of the largest radix per thread (as the column passes)
+template <typename T, int M> __host__ __device__ constexpr int xpass_threads() { return fft_threads<M, Tile<T>::B>(); }
 
 // ------------------------------------------------------------------ forward x + divergence
 template <typename T, int M>
-__global__ void __launch_bounds__(XPASS_THREADS)
+__global__ void __launch_bounds__(xpass_threads<T, M>())
 k_div_fftx(const double* __restrict__ u, const double* __restrict__ v, const double* __restrict__ w,
            Cx<T>* __restrict__ spec, const Cx<T>* __restrict__ twx, Geo g, double cdiv) {
   constexpr int B = Tile<T>::B;
-  constexpr int NT = XPASS_THREADS;
+  constexpr int NT = xpass_threads<T, M>();
   extern __shared__ __align__(16) unsigned char smraw[];
   Cx<T>* s = reinterpret_cast<Cx<T>*>(smraw);
   const int nx = 2 * M, ny = g.ny, nz = g.nz;
@@ -115,10 +116,10 @@ k_div_fftx(const double* __restrict__ u, const double* __restrict__ v, const dou
 
 // ------------------------------------------------------------------ inverse x -> pressure
 template <typename T, int M>
-__global__ void __launch_bounds__(XPASS_THREADS)
+__global__ void __launch_bounds__(xpass_threads<T, M>())
 k_fftx_inv(const Cx<T>* __restrict__ spec, T* __restrict__ p, const Cx<T>* __restrict__ twx, Geo g) {
   constexpr int B = Tile<T>::B;
-  constexpr int NT = XPASS_THREADS;
+  constexpr int NT = xpass_threads<T, M>();
   extern __shared__ __align__(16) unsigned char smraw[];
   Cx<T>* s = reinterpret_cast<Cx<T>*>(smraw);
   const int nx = 2 * M;
@@ -234,7 +235,7 @@ static cudaError_t launch_xfwd_m(const PoissonArgs& a, cudaStream_t st) {
   cudaError_t e = prep_smem(kern, smem);
   if (e != cudaSuccess) return e;
   const int nlines = a.g.ny * a.g.nz;
-  kern<<<(nlines + B - 1) / B, XPASS_THREADS, smem, st>>>(a.u, a.v, a.w, (Cx<T>*)a.spec, (const Cx<T>*)a.twx,
+  kern<<<(nlines + B - 1) / B, xpass_threads<T, M>(), smem, st>>>(a.u, a.v, a.w, (Cx<T>*)a.spec, (const Cx<T>*)a.twx,
                                                           a.g, a.cdiv);
   return cudaGetLastError();
 }
@@ -247,7 +248,7 @@ static cudaError_t launch_xinv_m(const PoissonArgs& a, cudaStream_t st) {
   cudaError_t e = prep_smem(kern, smem);
   if (e != cudaSuccess) return e;
   const int nlines = a.g.ny * a.g.nz;
-  kern<<<(nlines + B - 1) / B, XPASS_THREADS, smem, st>>>((const Cx<T>*)a.spec, (T*)a.p, (const Cx<T>*)a.twx, a.g);
+  kern<<<(nlines + B - 1) / B, xpass_threads<T, M>(), smem, st>>>((const Cx<T>*)a.spec, (T*)a.p, (const Cx<T>*)a.twx, a.g);
   return cudaGetLastError();
 }
 
