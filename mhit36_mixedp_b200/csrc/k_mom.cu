@@ -14,9 +14,9 @@
 // so every input byte crosses HBM once (plus the x/y halo re-read from L2) and the chemical
 // potential is evaluated once per cell.
 //
-// The velocity used here is the stored one minus the running mean of the previous projection
-// (DevScalars::mean), subtracted once per shared-memory element; this is exactly the
-// reference's u = u - gumean (:977-981) done lazily.
+// The velocity read here is the stored one minus the running mean of the previous
+// projection (DevScalars::mean); subtracting on read is exactly the reference's
+// u = u - gumean (:977-981) done lazily.
 #include <cuda_pipeline.h>
 
 #include "common.cuh"
@@ -142,21 +142,7 @@ __global__ void __launch_bounds__(MNT, 3) k_mom(MomArgs a) {
     }
   };
 
-  // The lazily removed mean of the last projection is subtracted once per shared-memory
-  // element, by the thread that copied it, right after its copy landed.
   const double mu_ = a.sc->mean[0], mv_ = a.sc->mean[1], mw_ = a.sc->mean[2];
-  auto fix_mean = [&](int m) {
-    const int su = (m - k0 + 8) & 3;
-#pragma unroll
-    for (int c = 0; c < UCP; ++c) {
-      if (uoff[c] >= 0) {
-        const int e = tid + c * MNT;
-        S.u[su][e] = S.u[su][e] - mu_;
-        S.v[su][e] = S.v[su][e] - mv_;
-        S.w[su][e] = S.w[su][e] - mw_;
-      }
-    }
-  };
 
   // prologue: phi k0-2, k0-1; u/v/w + phi k0-1, k0, k0+1
   issue_phi(k0 - 2);
@@ -164,9 +150,6 @@ __global__ void __launch_bounds__(MNT, 3) k_mom(MomArgs a) {
   issue_plane(k0);
   issue_plane(k0 + 1);
   __pipeline_wait_prior(0);
-  fix_mean(k0 - 1);
-  fix_mean(k0);
-  fix_mean(k0 + 1);
   __syncthreads();
   chempot_plane(k0 - 1);
 
@@ -193,7 +176,6 @@ __global__ void __launch_bounds__(MNT, 3) k_mom(MomArgs a) {
     }
     // plane k+1 landed (issued one iteration ago); everyone is done with iteration k-1
     __pipeline_wait_prior(0);
-    fix_mean(k + 1);
     __syncthreads();
     issue_plane(k + 2);
     chempot_plane(k);
@@ -203,15 +185,15 @@ __global__ void __launch_bounds__(MNT, 3) k_mom(MomArgs a) {
       const double* U0 = S.u[s0];
       const double* V0 = S.v[s0];
       const double* W0 = S.w[s0];
-      const double u0 = U0[uq], v0 = V0[uq], w0 = W0[uq];
-      const double uxp = U0[uq + 1], uxm = U0[uq - 1], uyp = U0[uq + UPX], uym = U0[uq - UPX];
-      const double uzp = S.u[sp][uq], uzm = S.u[sm][uq];
-      const double vxp = V0[uq + 1], vxm = V0[uq - 1], vyp = V0[uq + UPX], vym = V0[uq - UPX];
-      const double vzp = S.v[sp][uq], vzm = S.v[sm][uq];
-      const double wxp = W0[uq + 1], wxm = W0[uq - 1], wyp = W0[uq + UPX], wym = W0[uq - UPX];
-      const double wzp = S.w[sp][uq], wzm = S.w[sm][uq];
-      const double v_imjp = V0[uq + UPX - 1], w_imkp = S.w[sp][uq - 1], u_ipjm = U0[uq - UPX + 1];
-      const double w_jmkp = S.w[sp][uq - UPX], u_ipkm = S.u[sm][uq + 1], v_jpkm = S.v[sm][uq + UPX];
+      const double u0 = U0[uq] - mu_, v0 = V0[uq] - mv_, w0 = W0[uq] - mw_;
+      const double uxp = U0[uq + 1] - mu_, uxm = U0[uq - 1] - mu_, uyp = U0[uq + UPX] - mu_, uym = U0[uq - UPX] - mu_;
+      const double uzp = S.u[sp][uq] - mu_, uzm = S.u[sm][uq] - mu_;
+      const double vxp = V0[uq + 1] - mv_, vxm = V0[uq - 1] - mv_, vyp = V0[uq + UPX] - mv_, vym = V0[uq - UPX] - mv_;
+      const double vzp = S.v[sp][uq] - mv_, vzm = S.v[sm][uq] - mv_;
+      const double wxp = W0[uq + 1] - mw_, wxm = W0[uq - 1] - mw_, wyp = W0[uq + UPX] - mw_, wym = W0[uq - UPX] - mw_;
+      const double wzp = S.w[sp][uq] - mw_, wzm = S.w[sm][uq] - mw_;
+      const double v_imjp = V0[uq + UPX - 1] - mv_, w_imkp = S.w[sp][uq - 1] - mw_, u_ipjm = U0[uq - UPX + 1] - mu_;
+      const double w_jmkp = S.w[sp][uq - UPX] - mw_, u_ipkm = S.u[sm][uq + 1] - mu_, v_jpkm = S.v[sm][uq + UPX] - mv_;
       // multi/main.f90:672-694
       double h11 = (uxp + u0) * (uxp + u0) - (u0 + uxm) * (u0 + uxm);
       double h12 = (uyp + u0) * (vyp + v_imjp) - (u0 + uym) * (v0 + vxm);
