@@ -197,9 +197,6 @@ int mhit_debug_run_stage(mhit_ctx* ctx, int stage);
 int mhit_debug_commit_step(mhit_ctx* ctx);
 long long mhit_debug_buffer_len(mhit_ctx* ctx, int which);
 int mhit_debug_get_buffer(mhit_ctx* ctx, int which, double* out);
-/* y[i] = the device logarithm used for the ACDI distance function (psi, multi/main.f90:528),
- * evaluated on the GPU for n host values; lets a test bound its error against a reference log. */
-int mhit_debug_fastlog(const double* x, double* y, int n);
 
 #ifdef __cplusplus
 }

@@ -76,7 +76,6 @@ SIGNATURES = {
     "mhit_debug_commit_step": (_c.c_int, [_c.c_void_p]),
     "mhit_debug_buffer_len": (_c.c_longlong, [_c.c_void_p, _c.c_int]),
     "mhit_debug_get_buffer": (_c.c_int, [_c.c_void_p, _c.c_int, _dp]),
-    "mhit_debug_fastlog": (_c.c_int, [_dp, _dp, _c.c_int]),
 }
 
 STAGES = ["tracer", "phase", "momentum", "xfwd", "yfwd", "zsolve", "yinv", "xinv", "correct"]

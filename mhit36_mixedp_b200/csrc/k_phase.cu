@@ -15,9 +15,6 @@
 // reference's tanh(0.5*psi/eps) to 2.2e-16 over the whole range of phi (a NaN psi, from
 // phi < -1e-16, still gives a NaN t as in the reference).
 //
-// The logarithm is the table-driven fast_log of fastlog.cuh (within 2 ulp of a correctly
-// rounded log; non-positive and NaN arguments keep CUDA's log semantics).
-//
 // With PhaseArgs::clamp (opt-in, off by default) phi is also clamped below at 0 before the
 // log, so a cell undershooting to phi < -1e-16 no longer turns psi into NaN.
 //
@@ -26,7 +23,6 @@
 #include <cuda_pipeline.h>
 
 #include "common.cuh"
-#include "fastlog.cuh"
 #include "kernels.h"
 
 namespace mhit {
@@ -67,7 +63,6 @@ __global__ void __launch_bounds__(PNT, 2) k_phase(PhaseArgs a) {
   const double eps = g.eps;
   const int clamp = a.clamp;
   const double* __restrict__ phig = a.phi;
-  const double* __restrict__ logtab = a.logtab;
 
   int poff[PCPY];
 #pragma unroll
@@ -93,7 +88,7 @@ __global__ void __launch_bounds__(PNT, 2) k_phase(PhaseArgs a) {
   auto psi_at = [&](const double* __restrict__ P, double* __restrict__ Q, int e) {
     double val = fmin(P[e], 1.0);
     if (clamp) val = fmax(val, 0.0);
-    Q[e] = eps * fast_log((val + ENUM) / (1.0 - val + ENUM), logtab);
+    Q[e] = eps * log((val + ENUM) / (1.0 - val + ENUM));
   };
   // F of one element (multi/main.f90:530, 559-561, 586-589, 609-614); q: psi-plane index,
   // f: F-plane index

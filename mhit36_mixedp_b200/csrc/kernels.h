@@ -1,10 +1,6 @@
 // Host-side launchers of the timestep kernels (internal to libmhit_b200.so).
 #pragma once
 #include <cuda_runtime.h>
-
-#include <string>
-#include <vector>
-
 #include "common.cuh"
 
 namespace mhit {
@@ -38,7 +34,6 @@ struct PhaseArgs {
   const DevScalars* sc;
   double alpha, beta;
   int clamp;            // 1: phi clamped to [0,1] before the log
-  const double* logtab; // fastlog.cuh table (FASTLOG_TABLE_LEN doubles)
 };
 cudaError_t launch_phase(const PhaseArgs& a, cudaStream_t st);
 
@@ -94,6 +89,5 @@ cudaError_t launch_tracer(const TracerArgs& a, cudaStream_t st);
 
 // ---------------------------------------------------------------- utilities
 cudaError_t launch_fill(double* p, size_t n, double v, cudaStream_t st);
-std::vector<double> fastlog_table();
 
 }  // namespace mhit

@@ -63,7 +63,6 @@ struct mhit_ctx {
   void *twx = nullptr, *twy = nullptr, *twz = nullptr;
   double *k2x = nullptr, *k2y = nullptr, *k2z = nullptr;
   double* tabs = nullptr;
-  double* logtab = nullptr;
   double* partials = nullptr;
   int nblk = 0;
   DevScalars* sc = nullptr;
@@ -193,7 +192,6 @@ static int enqueue_stage(mhit_ctx* c, int stage, double alpha, double beta, int 
       a.alpha = alpha;
       a.beta = beta;
       a.clamp = p.acdi_clamp;
-      a.logtab = c->logtab;
       MHIT_CUDA_TRY(launch_phase(a, c->st));
       return MHIT_OK;
     }
@@ -429,7 +427,6 @@ void mhit_destroy(mhit_ctx* c) {
   cudaFree(c->k2y);
   cudaFree(c->k2z);
   cudaFree(c->tabs);
-  cudaFree(c->logtab);
   cudaFree(c->partials);
   cudaFree(c->sc);
   cudaFree(c->part);
@@ -531,9 +528,6 @@ static int init_impl(const mhit_params* p, mhit_ctx* c) {
       }
     }
     if ((rc = upload_vec((void**)&c->tabs, t))) return rc;
-  }
-  {
-    if ((rc = upload_vec((void**)&c->logtab, fastlog_table()))) return rc;
   }
   c->nblk = correct_blocks(g);
   MHIT_CUDA_TRY(cudaMalloc(&c->partials, (size_t)c->nblk * 6 * sizeof(double)));
