@@ -3,7 +3,7 @@
 // The reference makes five passes with three stored intermediates (psidi, tanh_psi and the
 // three normal components) and six halo exchanges.  Here a block owns a PTX x PTY column of
 // cells and marches up a chunk of z planes, keeping three rings of planes in shared memory:
-//   phi  planes k-1..k+3 (k+3 in flight via cp.async), x/y halo 2
+//   phi  planes k-2..k+5 (two planes in flight via cp.async), x/y halo 2
 //   psi  = eps log((min(phi,1)+1e-16)/(1-min(phi,1)+1e-16))          (:527-528), halo 2
 //   F    = 1/4 (1 - t^2) n/(|n|+1e-16), n = central psi differences (:559-561, :586-589,
 //          :609-614), halo 1, with t = tanh(psi/(2 eps)) (:530)
@@ -28,7 +28,7 @@
 namespace mhit {
 
 constexpr int PTX = 32, PTY = 16, PNT = PTX * PTY;
-constexpr int PZC = 32;                      // z planes per block
+constexpr int PZC = 64;                      // z planes per block
 constexpr int PHX = PTX + 4, PHY = PTY + 4;  // phi / psi plane (halo 2)
 constexpr int PHL = PHX * PHY;
 constexpr int PFX = PTX + 2, PFY = PTY + 2;  // F plane (halo 1)
@@ -38,7 +38,7 @@ constexpr double ENUM = 1.0e-16;
 constexpr double TNORM = 1.0 / (1.0 + 2.0 * ENUM);
 
 struct PhaseSmem {
-  double phi[6][PHL];   // planes k-2..k+3 (k+4 in flight while iteration k runs)
+  double phi[7][PHL];   // planes k-2..k+4 (k+4, k+5 in flight while iteration k runs)
   double psi[4][PHL];   // planes k..k+3
   double F[3][3][PFL];  // planes k-1..k+1
 };
@@ -48,8 +48,8 @@ __device__ __forceinline__ int pmodi(int x, int n) {
   return x < 0 ? x + n : x;
 }
 
-// Software pipeline, two barriers per output plane k:
-//   B1; cp.async phi(k+4); { psi(k+3), F(k+1) } as one task list; B2; out(k)
+// Software pipeline, two barriers per output plane k, phi prefetched two planes ahead:
+//   wait phi(k+3); B1; cp.async phi(k+5); { psi(k+3), F(k+1) } as one task list; B2; out(k)
 __global__ void __launch_bounds__(PNT, 2) k_phase(PhaseArgs a) {
   extern __shared__ __align__(16) unsigned char smraw[];
   PhaseSmem& S = *reinterpret_cast<PhaseSmem*>(smraw);
@@ -74,12 +74,12 @@ __global__ void __launch_bounds__(PNT, 2) k_phase(PhaseArgs a) {
       poff[c] = pmodi(j0 - 2 + y, ny) * nx + pmodi(i0 - 2 + x, nx);
     }
   }
-  auto slot6 = [&](int m) { return (m - k0 + 8) % 6; };
+  auto slot7 = [&](int m) { return (m - k0 + 9) % 7; };
   auto slot4 = [&](int m) { return (m - k0 + 8) & 3; };
   auto slot3 = [&](int m) { return (m - k0 + 6) % 3; };
   auto issue_phi = [&](int m) {
     const size_t base = (size_t)pmodi(m, nz) * plane;
-    double* dst = S.phi[slot6(m)];
+    double* dst = S.phi[slot7(m)];
 #pragma unroll
     for (int c = 0; c < PCPY; ++c)
       if (poff[c] >= 0) __pipeline_memcpy_async(dst + tid + c * PNT, phig + base + poff[c], 8);
@@ -114,7 +114,7 @@ __global__ void __launch_bounds__(PNT, 2) k_phase(PhaseArgs a) {
     const double* Qm = S.psi[slot4(m - 1)];
     const double* Q0 = S.psi[slot4(m)];
     const double* Qp = S.psi[slot4(m + 1)];
-    const double* P = S.phi[slot6(m)];
+    const double* P = S.phi[slot7(m)];
     double* Fd = S.F[slot3(m)][0];
     for (int e = tid; e < PFL; e += PNT) {
       const int y = e / PFX, x = e - y * PFX;
@@ -125,18 +125,20 @@ __global__ void __launch_bounds__(PNT, 2) k_phase(PhaseArgs a) {
   // prologue: phi k0-2..k0+3; psi k0-2..k0+2 (ring of 4); F k0-1, k0
   for (int m = k0 - 2; m <= k0 + 3; ++m) issue_phi(m);
   __pipeline_commit();
-  __pipeline_wait_prior(0);
+  issue_phi(k0 + 4);
+  __pipeline_commit();
+  __pipeline_wait_prior(1);
   __syncthreads();
   for (int e = tid; e < 3 * PHL; e += PNT) {
     const int m = k0 - 2 + e / PHL;
-    psi_at(S.phi[slot6(m)], S.psi[slot4(m)], e % PHL);
+    psi_at(S.phi[slot7(m)], S.psi[slot4(m)], e % PHL);
   }
   __syncthreads();
   F_plane_all(k0 - 1);
   __syncthreads();
   for (int e = tid; e < 2 * PHL; e += PNT) {
     const int m = k0 + 1 + e / PHL;
-    psi_at(S.phi[slot6(m)], S.psi[slot4(m)], e % PHL);
+    psi_at(S.phi[slot7(m)], S.psi[slot4(m)], e % PHL);
   }
   __syncthreads();
   F_plane_all(k0);
@@ -193,17 +195,17 @@ __global__ void __launch_bounds__(PNT, 2) k_phase(PhaseArgs a) {
       wzp = __ldg(pw + dwz);
       ro = *prphi;
     }
-    __pipeline_wait_prior(0);
+    __pipeline_wait_prior(1);  // phi(k+3) landed; phi(k+4) may still be in flight
     __syncthreads();
-    issue_phi(k + 4);
+    issue_phi(k + 5);
     __pipeline_commit();
     {
-      const double* P3 = S.phi[slot6(k + 3)];
+      const double* P3 = S.phi[slot7(k + 3)];
       double* Q3 = S.psi[slot4(k + 3)];
       const double* Qm = S.psi[slot4(k)];
       const double* Q0 = S.psi[slot4(k + 1)];
       const double* Qp = S.psi[slot4(k + 2)];
-      const double* P1 = S.phi[slot6(k + 1)];
+      const double* P1 = S.phi[slot7(k + 1)];
       double* Fd = S.F[slot3(k + 1)][0];
 #pragma unroll
       for (int r = 0; r < NTASK; ++r) {
@@ -219,10 +221,10 @@ __global__ void __launch_bounds__(PNT, 2) k_phase(PhaseArgs a) {
       vyp -= mv_;
       w0 -= mw_;
       wzp -= mw_;
-      const double* P0 = S.phi[slot6(k)];
+      const double* P0 = S.phi[slot7(k)];
       const double p0 = P0[hq];
       const double pxp = P0[hq + 1], pxm = P0[hq - 1], pyp = P0[hq + PHX], pym = P0[hq - PHX];
-      const double pzp = S.phi[slot6(k + 1)][hq], pzm = S.phi[slot6(k - 1)][hq];
+      const double pzp = S.phi[slot7(k + 1)][hq], pzm = S.phi[slot7(k - 1)][hq];
       // multi/main.f90:551-557
       double rhs = -((uxp * 0.5 * (pxp + p0) - u0 * 0.5 * (p0 + pxm)) * dxi) -
                    (vyp * 0.5 * (pyp + p0) - v0 * 0.5 * (p0 + pym)) * dxi -
