@@ -208,6 +208,48 @@ def cpu_sample(n_sample=256, steps=3, n_target=512):
                       f"{steps} steps, best AB2 step x (512/{n_sample})^3 = {scale:g}"}
 
 
+def ensemble_workload():
+    """32 NS+ACDI boxes: 16 x 64^3, 10 x 128^3, 6 x 192^3; per-box seeds 100+b; nu ~ U[0.002,0.01],
+    We ~ U[0.5,5], 32-256 drops of radius 0.3 (eps = dx), FP32 Poisson, dt = 2e-4."""
+    from mhit36_mixedp_b200 import Params, synth
+    rng = np.random.default_rng(99)
+    sizes = [64] * 16 + [128] * 10 + [192] * 6
+    boxes = []
+    for b, n in enumerate(sizes):
+        nu = float(rng.uniform(0.002, 0.01))
+        we = float(rng.uniform(0.5, 5.0))
+        ndrops = int(rng.integers(32, 257))
+        u, v, w = synth.solenoidal_velocity(n, 100 + b)
+        phi = synth.drops_phi(n, synth.drop_centres(ndrops, 100 + b), 0.3, 2 * math.pi / n)
+        prm = Params(nx=n, dt=2e-4, mu=nu, rho=1.0, radius=0.3, sigma=synth.sigma_from_weber(1.0, 1.0, 0.3, we),
+                     phiflag=1, poisson="fp32", acdi_clamp=1)
+        boxes.append((prm, u, v, w, phi))
+    return boxes
+
+
+def run_ensemble(args):
+    from mhit36_mixedp_b200 import Ensemble
+    boxes = ensemble_workload()
+    with Ensemble([b[0] for b in boxes]) as ens:
+        tuning = ens.autotune(trials=2)
+        for box, (prm, u, v, w, phi) in zip(ens.boxes, boxes):
+            box.upload(u, v, w, phi)
+        ens.step(max(args.warmup, 3))
+        with Clocks(0) as clk:
+            ms = ens.time_steps(args.steps)
+        ens.step(0)
+    npts = sum(b[0].nx ** 3 for b in boxes)
+    peak, kind = peaks()
+    frac = STEP_BYTES["fp32"] * npts / (ms / args.steps * 1e-3) / 1e9 / peak
+    line = {"metric": "ms per ensemble step, 32 NS+ACDI boxes (16x64^3, 10x128^3, 6x192^3), FP32 Poisson",
+            "value": ms / args.steps, "unit": "ms/timestep", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": False, "data": "synthetic", "dtype": "f64+f32",
+            "config": {"workload": "ensemble", "boxes": len(boxes), "points": npts, "one_graph_launch_per_step": True},
+            "tuning": tuning, "step_roofline_frac": frac, "peak_kind": kind, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -216,7 +258,10 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--n", type=int, default=512)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ensemble", action="store_true", help="time the 32-box ensemble instead")
     args = ap.parse_args()
+    if args.ensemble:
+        return run_ensemble(args)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))

@@ -145,6 +145,24 @@ int mhit_read_field(mhit_ctx* ctx, const char* path, int fieldn);
 int mhit_time_steps(mhit_ctx* ctx, int nsteps, double* ms);
 int mhit_profile_step(mhit_ctx* ctx, double* ms, const char** names, int* nstages);
 
+/* Ensemble of independent boxes of uneven sizes (the reference runs one box per job; this is
+ * the batched mode of its timestep loop).  Every box is a full context -- upload, download,
+ * diagnostics and field files go through mhit_ensemble_box() and the single-box calls -- but
+ * the boxes advance together: mhit_ensemble_step runs each step after the first as ONE CUDA
+ * graph launch whose graph forks the boxes' step sequences onto concurrent streams ("lanes")
+ * and joins them.  All boxes must be at the same step (upload all, then step all).
+ * mhit_ensemble_autotune times the z-chunk of the phase and momentum kernels per box size and
+ * the number of lanes, keeps the fastest, and leaves every box zeroed: call it before the
+ * uploads.  mhit_ensemble_tuning reports the choices (arrays of nbox ints, may be NULL). */
+typedef struct mhit_ensemble mhit_ensemble;
+int mhit_ensemble_create(const mhit_params* params, int nbox, mhit_ensemble** out);
+void mhit_ensemble_destroy(mhit_ensemble* e);
+int mhit_ensemble_box(mhit_ensemble* e, int b, mhit_ctx** ctx);
+int mhit_ensemble_step(mhit_ensemble* e, int nsteps);
+int mhit_ensemble_time_steps(mhit_ensemble* e, int nsteps, double* ms);
+int mhit_ensemble_autotune(mhit_ensemble* e, int trials, int* nlanes);
+int mhit_ensemble_tuning(mhit_ensemble* e, int* nlanes, int* zchunk_phase, int* zchunk_mom);
+
 /* Test hooks (no reference counterpart): run one stage of the step pipeline on the current
  * buffers, read an internal buffer widened to float64, and commit the staged step.  They let
  * a test compare each kernel with the matching block of multi/main.f90.  Stage order:

@@ -4,12 +4,12 @@
 declared in ``include/mhit_b200.h``; ``api`` is the Python host side over it, ``fieldio`` the
 reference's field-file and input formats, ``synth`` the seeded synthetic initial conditions.
 """
-from .api import (FIELD_P, FIELD_PHI, FIELD_U, FIELD_V, FIELD_W, MhitArgError, MhitCFLError,
+from .api import (Ensemble, FIELD_P, FIELD_PHI, FIELD_U, FIELD_V, FIELD_W, MhitArgError, MhitCFLError,
                   MhitCudaError, MhitError, MhitIOError, MhitNaNError, MhitStateError, Params,
                   Solver, abi_version, read_input)
 
 __all__ = [
-    "Params", "Solver", "read_input", "abi_version", "MhitError", "MhitArgError", "MhitCudaError",
+    "Ensemble", "Params", "Solver", "read_input", "abi_version", "MhitError", "MhitArgError", "MhitCudaError",
     "MhitNaNError", "MhitCFLError", "MhitIOError", "MhitStateError",
     "FIELD_U", "FIELD_V", "FIELD_W", "FIELD_P", "FIELD_PHI",
 ]

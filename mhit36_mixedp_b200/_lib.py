@@ -70,6 +70,13 @@ SIGNATURES = {
     "mhit_read_field": (_c.c_int, [_c.c_void_p, _c.c_char_p, _c.c_int]),
     "mhit_time_steps": (_c.c_int, [_c.c_void_p, _c.c_int, _dp]),
     "mhit_profile_step": (_c.c_int, [_c.c_void_p, _dp, _P(_c.c_char_p), _P(_c.c_int)]),
+    "mhit_ensemble_create": (_c.c_int, [_P(MhitParams), _c.c_int, _P(_c.c_void_p)]),
+    "mhit_ensemble_destroy": (None, [_c.c_void_p]),
+    "mhit_ensemble_box": (_c.c_int, [_c.c_void_p, _c.c_int, _P(_c.c_void_p)]),
+    "mhit_ensemble_step": (_c.c_int, [_c.c_void_p, _c.c_int]),
+    "mhit_ensemble_time_steps": (_c.c_int, [_c.c_void_p, _c.c_int, _dp]),
+    "mhit_ensemble_autotune": (_c.c_int, [_c.c_void_p, _c.c_int, _P(_c.c_int)]),
+    "mhit_ensemble_tuning": (_c.c_int, [_c.c_void_p, _P(_c.c_int), _P(_c.c_int), _P(_c.c_int)]),
     "mhit_field_stats_noalloc": (_c.c_int, [_c.c_int, _c.c_int, _c.c_int, _c.c_double, _c.c_void_p, _c.c_void_p,
                                             _c.c_void_p, _c.c_void_p, _c.c_void_p]),
     "mhit_debug_run_stage": (_c.c_int, [_c.c_void_p, _c.c_int]),

@@ -145,18 +145,22 @@ def read_input(path: str, **overrides):
 class Solver:
     """One box on one GPU: ``init`` -> ``upload`` -> ``step`` ... -> ``download``."""
 
-    def __init__(self, params: Params):
+    def __init__(self, params: Params, _borrowed_ctx=None):
         self.params = params
         self._lib = _lib.load()
-        self._ctx = ctypes.c_void_p()
-        self._cp = params.to_c()
-        _check(self._lib.mhit_init(ctypes.byref(self._cp), ctypes.byref(self._ctx)))
+        self._owned = _borrowed_ctx is None
+        if self._owned:
+            self._ctx = ctypes.c_void_p()
+            self._cp = params.to_c()
+            _check(self._lib.mhit_init(ctypes.byref(self._cp), ctypes.byref(self._ctx)))
+        else:
+            self._ctx = _borrowed_ctx
 
     # -------------------------------------------------------------- lifecycle
     def close(self):
-        if self._ctx:
+        if self._ctx and self._owned:
             self._lib.mhit_destroy(self._ctx)
-            self._ctx = ctypes.c_void_p()
+        self._ctx = ctypes.c_void_p()
 
     def __enter__(self):
         return self
@@ -266,6 +270,67 @@ class Solver:
         n = ctypes.c_int(cap)
         _check(self._lib.mhit_profile_step(self._ctx, ms, names, ctypes.byref(n)))
         return {names[i].decode(): ms[i] for i in range(n.value) if ms[i] >= 0}
+
+
+class Ensemble:
+    """Independent boxes of uneven sizes advanced together, one CUDA-graph launch per step.
+
+    ``boxes[b]`` is a ``Solver`` view of box b (upload, download, diagnostics, field files);
+    ``step`` advances all boxes.  ``autotune`` picks the kernels' z-chunks per box size and the
+    number of concurrent streams; it zeroes the boxes, so call it before uploading.
+    """
+
+    def __init__(self, params_list):
+        self._lib = _lib.load()
+        self.params = list(params_list)
+        arr = (MhitParams * len(self.params))(*[p.to_c() for p in self.params])
+        self._e = ctypes.c_void_p()
+        _check(self._lib.mhit_ensemble_create(arr, len(self.params), ctypes.byref(self._e)))
+        self.boxes = []
+        for b, p in enumerate(self.params):
+            c = ctypes.c_void_p()
+            _check(self._lib.mhit_ensemble_box(self._e, b, ctypes.byref(c)))
+            self.boxes.append(Solver(p, _borrowed_ctx=c))
+
+    def close(self):
+        if self._e:
+            for s in self.boxes:
+                s.close()
+            self._lib.mhit_ensemble_destroy(self._e)
+            self._e = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, nsteps: int = 1):
+        _check(self._lib.mhit_ensemble_step(self._e, int(nsteps)))
+
+    def time_steps(self, nsteps: int) -> float:
+        ms = ctypes.c_double()
+        _check(self._lib.mhit_ensemble_time_steps(self._e, int(nsteps), ctypes.byref(ms)))
+        return ms.value
+
+    def autotune(self, trials: int = 2) -> dict:
+        n = ctypes.c_int()
+        _check(self._lib.mhit_ensemble_autotune(self._e, int(trials), ctypes.byref(n)))
+        return self.tuning()
+
+    def tuning(self) -> dict:
+        nb = len(self.params)
+        lanes = ctypes.c_int()
+        zp = (ctypes.c_int * nb)()
+        zm = (ctypes.c_int * nb)()
+        _check(self._lib.mhit_ensemble_tuning(self._e, ctypes.byref(lanes), zp, zm))
+        return {"lanes": lanes.value, "zchunk_phase": list(zp), "zchunk_mom": list(zm)}
 
 
 def abi_version() -> int:

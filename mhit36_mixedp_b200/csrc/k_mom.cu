@@ -25,7 +25,7 @@
 namespace mhit {
 
 constexpr int MTX = 32, MTY = 8, MNT = MTX * MTY;
-constexpr int MZC = 32;                       // z planes per block
+constexpr int MZC = 32;                       // default z planes per block
 constexpr int UPX = MTX + 2, UPY = MTY + 2;   // u/v/w plane (halo 1)
 constexpr int UPL = UPX * UPY;
 constexpr int PPX = MTX + 3, PPY = MTY + 3;   // phi plane: x,y in [-2, T+1)
@@ -58,8 +58,9 @@ __global__ void __launch_bounds__(MNT, 3) k_mom(MomArgs a) {
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const size_t plane = (size_t)nx * ny;
   const int i0 = blockIdx.x * MTX, j0 = blockIdx.y * MTY;
-  const int k0 = blockIdx.z * MZC;
-  const int k1 = min(k0 + MZC, nz);
+  const int zc = a.zchunk > 0 ? a.zchunk : MZC;
+  const int k0 = blockIdx.z * zc;
+  const int k1 = min(k0 + zc, nz);
   const int tid = threadIdx.x;
 
   // per-thread in-plane source offsets of the elements this thread copies
@@ -259,7 +260,8 @@ static cudaError_t launch_mom_t(const MomArgs& a, cudaStream_t st) {
     if (e != cudaSuccess) return e;
     attr_set[dev] = 1;
   }
-  dim3 grd((a.g.nx + MTX - 1) / MTX, (a.g.ny + MTY - 1) / MTY, (a.g.nz + MZC - 1) / MZC);
+  const int zc = a.zchunk > 0 ? a.zchunk : MZC;
+  dim3 grd((a.g.nx + MTX - 1) / MTX, (a.g.ny + MTY - 1) / MTY, (a.g.nz + zc - 1) / zc);
   k_mom<PHI><<<grd, MNT, smem, st>>>(a);
   return cudaGetLastError();
 }

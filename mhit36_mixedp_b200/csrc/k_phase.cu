@@ -28,7 +28,7 @@
 namespace mhit {
 
 constexpr int PTX = 32, PTY = 16, PNT = PTX * PTY;
-constexpr int PZC = 64;                      // z planes per block
+constexpr int PZC = 64;                      // default z planes per block
 constexpr int PHX = PTX + 4, PHY = PTY + 4;  // phi / psi plane (halo 2)
 constexpr int PHL = PHX * PHY;
 constexpr int PFX = PTX + 2, PFY = PTY + 2;  // F plane (halo 1)
@@ -57,8 +57,9 @@ __global__ void __launch_bounds__(PNT, 2) k_phase(PhaseArgs a) {
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const size_t plane = (size_t)nx * ny;
   const int i0 = blockIdx.x * PTX, j0 = blockIdx.y * PTY;
-  const int k0 = blockIdx.z * PZC;
-  const int k1 = min(k0 + PZC, nz);
+  const int zc = a.zchunk > 0 ? a.zchunk : PZC;
+  const int k0 = blockIdx.z * zc;
+  const int k1 = min(k0 + zc, nz);
   const int tid = threadIdx.x;
   const double eps = g.eps;
   const int clamp = a.clamp;
@@ -259,7 +260,8 @@ cudaError_t launch_phase(const PhaseArgs& a, cudaStream_t st) {
     if (e != cudaSuccess) return e;
     attr_set[dev] = 1;
   }
-  dim3 grd((a.g.nx + PTX - 1) / PTX, (a.g.ny + PTY - 1) / PTY, (a.g.nz + PZC - 1) / PZC);
+  const int zc = a.zchunk > 0 ? a.zchunk : PZC;
+  dim3 grd((a.g.nx + PTX - 1) / PTX, (a.g.ny + PTY - 1) / PTY, (a.g.nz + zc - 1) / zc);
   k_phase<<<grd, PNT, smem, st>>>(a);
   return cudaGetLastError();
 }

@@ -34,6 +34,7 @@ struct PhaseArgs {
   const DevScalars* sc;
   double alpha, beta;
   int clamp;            // 1: phi clamped to [0,1] before the log
+  int zchunk;           // z planes per block (0: default)
 };
 cudaError_t launch_phase(const PhaseArgs& a, cudaStream_t st);
 
@@ -47,6 +48,7 @@ struct MomArgs {
   const double* tabs;        // sx,cx (nx) sy,cy (ny) sz,cz (nz)
   const DevScalars* sc;
   double alpha, beta;
+  int zchunk;                // z planes per block (0: default)
 };
 cudaError_t launch_mom(const MomArgs& a, cudaStream_t st);
 

@@ -14,6 +14,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <algorithm>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -74,6 +75,7 @@ struct mhit_ctx {
   bool graph_built = false;
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
   cudaEvent_t ev[2 * ST_COUNT] = {};
+  int zchunk_phase = 0, zchunk_mom = 0;  // z planes per block of k_phase / k_mom (0: default)
 };
 
 // ------------------------------------------------------------------ helpers
@@ -192,6 +194,7 @@ static int enqueue_stage(mhit_ctx* c, int stage, double alpha, double beta, int 
       a.alpha = alpha;
       a.beta = beta;
       a.clamp = p.acdi_clamp;
+      a.zchunk = c->zchunk_phase;
       MHIT_CUDA_TRY(launch_phase(a, c->st));
       return MHIT_OK;
     }
@@ -212,6 +215,7 @@ static int enqueue_stage(mhit_ctx* c, int stage, double alpha, double beta, int 
       a.sc = c->sc;
       a.alpha = alpha;
       a.beta = beta;
+      a.zchunk = c->zchunk_mom;
       MHIT_CUDA_TRY(launch_mom(a, c->st));
       return MHIT_OK;
     }
@@ -862,6 +866,299 @@ int mhit_debug_get_buffer(mhit_ctx* c, int which, double* out) {
   } else {
     MHIT_CUDA_TRY(cudaMemcpyAsync(out, src, len * 8, cudaMemcpyDeviceToHost, c->st));
     MHIT_CUDA_TRY(cudaStreamSynchronize(c->st));
+  }
+  return MHIT_OK;
+}
+
+// ------------------------------------------------------------------ ensemble of boxes
+// Independent boxes of uneven sizes advanced together: every step after the first is ONE
+// graph launch whose graph forks the boxes' step sequences onto `nlanes` streams (boxes on
+// different lanes run concurrently, boxes on one lane back to back) and joins them.
+}  // extern "C"
+
+struct mhit_ensemble {
+  int nbox = 0;
+  std::vector<mhit_ctx*> box;
+  int dev = 0;
+  cudaStream_t st = nullptr;
+  int nlanes = 1;
+  std::vector<cudaStream_t> lanes;
+  cudaEvent_t fork = nullptr;
+  std::vector<cudaEvent_t> join;
+  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  bool built = false;
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+};
+
+static void ens_drop_graphs(mhit_ensemble* e) {
+  for (int i = 0; i < 2; ++i)
+    if (e->gexec[i]) {
+      cudaGraphExecDestroy(e->gexec[i]);
+      e->gexec[i] = nullptr;
+    }
+  e->built = false;
+}
+
+static int ens_set_lanes(mhit_ensemble* e, int nlanes) {
+  if (nlanes < 1) nlanes = 1;
+  if (nlanes > e->nbox) nlanes = e->nbox;
+  MHIT_CUDA_TRY(cudaStreamSynchronize(e->st));
+  for (cudaStream_t s : e->lanes) cudaStreamDestroy(s);
+  for (cudaEvent_t v : e->join) cudaEventDestroy(v);
+  e->lanes.assign(nlanes, nullptr);
+  e->join.assign(nlanes, nullptr);
+  for (int l = 0; l < nlanes; ++l) {
+    MHIT_CUDA_TRY(cudaStreamCreateWithFlags(&e->lanes[l], cudaStreamNonBlocking));
+    MHIT_CUDA_TRY(cudaEventCreateWithFlags(&e->join[l], cudaEventDisableTiming));
+  }
+  e->nlanes = nlanes;
+  ens_drop_graphs(e);
+  return MHIT_OK;
+}
+
+// One ensemble step on e->st (captured or eager): fork, per-box sequences on lanes, join.
+static int ens_enqueue(mhit_ensemble* e, double alpha, double beta, int cur) {
+  MHIT_CUDA_TRY(cudaEventRecord(e->fork, e->st));
+  for (int l = 0; l < e->nlanes; ++l) MHIT_CUDA_TRY(cudaStreamWaitEvent(e->lanes[l], e->fork, 0));
+  for (int b = 0; b < e->nbox; ++b) {
+    mhit_ctx* c = e->box[b];
+    cudaStream_t saved = c->st;
+    c->st = e->lanes[b % e->nlanes];
+    int rc = enqueue_step(c, alpha, beta, cur, false);
+    c->st = saved;
+    if (rc) return rc;
+  }
+  for (int l = 0; l < e->nlanes; ++l) {
+    MHIT_CUDA_TRY(cudaEventRecord(e->join[l], e->lanes[l]));
+    MHIT_CUDA_TRY(cudaStreamWaitEvent(e->st, e->join[l], 0));
+  }
+  return MHIT_OK;
+}
+
+static int ens_build(mhit_ensemble* e) {
+  for (int par = 0; par < 2; ++par) {
+    cudaGraph_t graph;
+    MHIT_CUDA_TRY(cudaStreamBeginCapture(e->st, cudaStreamCaptureModeThreadLocal));
+    int rc = ens_enqueue(e, 1.5, 0.5, par);
+    cudaError_t err = cudaStreamEndCapture(e->st, &graph);
+    if (rc) return rc;
+    if (err != cudaSuccess) return set_cuda_error(err, "cudaStreamEndCapture (ensemble)", __FILE__, __LINE__);
+    err = cudaGraphInstantiate(&e->gexec[par], graph, 0);
+    cudaGraphDestroy(graph);
+    if (err != cudaSuccess) return set_cuda_error(err, "cudaGraphInstantiate (ensemble)", __FILE__, __LINE__);
+  }
+  e->built = true;
+  return MHIT_OK;
+}
+
+static int ens_enqueue_steps(mhit_ensemble* e, int nsteps) {
+  for (int s = 0; s < nsteps; ++s) {
+    const long long n0 = e->box[0]->nstep;
+    const int cur = e->box[0]->cur;
+    for (mhit_ctx* c : e->box)
+      if (c->nstep != n0 || c->cur != cur)
+        return set_error(MHIT_ERR_STATE, "ensemble boxes are at different steps (upload or step all of them together)");
+    int rc;
+    if (n0 == 0) {
+      rc = ens_enqueue(e, 1.0, 0.0, cur);  // Euler first step, multi/main.f90:440-441
+    } else {
+      if (!e->built && (rc = ens_build(e))) return rc;
+      MHIT_CUDA_TRY(cudaGraphLaunch(e->gexec[cur], e->st));
+      rc = MHIT_OK;
+    }
+    if (rc) return rc;
+    for (mhit_ctx* c : e->box) {
+      c->cur ^= 1;
+      c->nstep++;
+    }
+  }
+  return MHIT_OK;
+}
+
+static int ens_check_flags(mhit_ensemble* e) {
+  MHIT_CUDA_TRY(cudaStreamSynchronize(e->st));
+  for (int b = 0; b < e->nbox; ++b) {
+    int rc;
+    if ((rc = fetch_scalars(e->box[b]))) return rc;
+    const int flag = e->box[b]->sc_host->flag;
+    if (flag & 1) return set_error(MHIT_ERR_NAN, "NaN in the velocity field of ensemble box " + std::to_string(b));
+    if (flag & 2) return set_error(MHIT_ERR_CFL, "CFL > 7 in ensemble box " + std::to_string(b));
+  }
+  return MHIT_OK;
+}
+
+// zero fields, empty history, Euler next (used around the autotuner's throwaway steps)
+static int reset_state(mhit_ctx* c) {
+  const size_t fb = c->n * sizeof(double);
+  for (int i = 0; i < 2; ++i) {
+    MHIT_CUDA_TRY(cudaMemsetAsync(c->U[i], 0, fb, c->st));
+    MHIT_CUDA_TRY(cudaMemsetAsync(c->V[i], 0, fb, c->st));
+    MHIT_CUDA_TRY(cudaMemsetAsync(c->W[i], 0, fb, c->st));
+    if (c->PHI[i]) MHIT_CUDA_TRY(cudaMemsetAsync(c->PHI[i], 0, fb, c->st));
+  }
+  c->cur = 0;
+  return reset_history(c);
+}
+
+extern "C" {
+
+int mhit_ensemble_create(const mhit_params* params, int nbox, mhit_ensemble** out) {
+  if (!params || !out || nbox < 1) return set_error(MHIT_ERR_ARG, "need at least one box");
+  *out = nullptr;
+  for (int b = 1; b < nbox; ++b)
+    if (params[b].device != params[0].device) return set_error(MHIT_ERR_ARG, "all ensemble boxes must use one device");
+  mhit_ensemble* e = new mhit_ensemble();
+  e->nbox = nbox;
+  e->dev = params[0].device;
+  int rc = MHIT_OK;
+  for (int b = 0; b < nbox && rc == MHIT_OK; ++b) {
+    mhit_ctx* c = nullptr;
+    rc = mhit_init(&params[b], &c);
+    if (rc == MHIT_OK) e->box.push_back(c);
+  }
+  if (rc == MHIT_OK) {
+    cudaError_t err = cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking);
+    if (err == cudaSuccess) err = cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming);
+    if (err == cudaSuccess) err = cudaEventCreate(&e->ev[0]);
+    if (err == cudaSuccess) err = cudaEventCreate(&e->ev[1]);
+    if (err != cudaSuccess) rc = set_cuda_error(err, "ensemble stream/events", __FILE__, __LINE__);
+  }
+  if (rc == MHIT_OK) rc = ens_set_lanes(e, nbox);
+  if (rc) {
+    std::string keep = g_err;
+    mhit_ensemble_destroy(e);
+    g_err = keep;
+    return rc;
+  }
+  *out = e;
+  return MHIT_OK;
+}
+
+void mhit_ensemble_destroy(mhit_ensemble* e) {
+  if (!e) return;
+  cudaSetDevice(e->dev);
+  if (e->st) cudaStreamSynchronize(e->st);
+  ens_drop_graphs(e);
+  for (cudaStream_t s : e->lanes) cudaStreamDestroy(s);
+  for (cudaEvent_t v : e->join) cudaEventDestroy(v);
+  if (e->fork) cudaEventDestroy(e->fork);
+  for (int i = 0; i < 2; ++i)
+    if (e->ev[i]) cudaEventDestroy(e->ev[i]);
+  if (e->st) cudaStreamDestroy(e->st);
+  for (mhit_ctx* c : e->box) mhit_destroy(c);
+  delete e;
+}
+
+int mhit_ensemble_box(mhit_ensemble* e, int b, mhit_ctx** ctx) {
+  if (!e || !ctx || b < 0 || b >= e->nbox) return set_error(MHIT_ERR_ARG, "box index out of range");
+  *ctx = e->box[b];
+  return MHIT_OK;
+}
+
+int mhit_ensemble_step(mhit_ensemble* e, int nsteps) {
+  if (!e || nsteps < 0) return set_error(MHIT_ERR_ARG, "bad argument");
+  MHIT_CUDA_TRY(cudaSetDevice(e->dev));
+  // fields uploaded through a box's own stream must be complete before the ensemble stream runs
+  for (mhit_ctx* c : e->box) MHIT_CUDA_TRY(cudaStreamSynchronize(c->st));
+  int rc;
+  if ((rc = ens_enqueue_steps(e, nsteps))) return rc;
+  return ens_check_flags(e);
+}
+
+int mhit_ensemble_time_steps(mhit_ensemble* e, int nsteps, double* ms) {
+  if (!e || !ms || nsteps < 0) return set_error(MHIT_ERR_ARG, "bad argument");
+  MHIT_CUDA_TRY(cudaSetDevice(e->dev));
+  for (mhit_ctx* c : e->box) MHIT_CUDA_TRY(cudaStreamSynchronize(c->st));
+  MHIT_CUDA_TRY(cudaEventRecord(e->ev[0], e->st));
+  int rc;
+  if ((rc = ens_enqueue_steps(e, nsteps))) return rc;
+  MHIT_CUDA_TRY(cudaEventRecord(e->ev[1], e->st));
+  MHIT_CUDA_TRY(cudaEventSynchronize(e->ev[1]));
+  float f = 0.f;
+  MHIT_CUDA_TRY(cudaEventElapsedTime(&f, e->ev[0], e->ev[1]));
+  *ms = f;
+  return MHIT_OK;
+}
+
+// Autotuner: for every class of equal boxes (grid, phase field on/off) time the z-chunk of
+// k_phase and k_mom over {8, 16, 32, 64} on the first box of the class (one profiled step per
+// candidate, best of `trials`), then time whole ensemble steps for 1, 2, 4, 8, ... lanes and
+// keep the fastest.  The timing steps run on zeroed fields and are thrown away: every box is
+// left zeroed with an empty history, so call this before uploading the initial fields.
+int mhit_ensemble_autotune(mhit_ensemble* e, int trials, int* nlanes_out) {
+  if (!e) return set_error(MHIT_ERR_ARG, "null ensemble");
+  if (trials < 1) trials = 1;
+  MHIT_CUDA_TRY(cudaSetDevice(e->dev));
+  int rc;
+  for (mhit_ctx* c : e->box)
+    if ((rc = reset_state(c))) return rc;
+  const int cand[4] = {8, 16, 32, 64};
+  std::vector<bool> done(e->nbox, false);
+  for (int b = 0; b < e->nbox; ++b) {
+    if (done[b]) continue;
+    mhit_ctx* c = e->box[b];
+    int best_p = 0, best_m = 0;
+    double tp = 1e30, tm = 1e30;
+    for (int q = 0; q < 4; ++q) {
+      if (cand[q] > c->g.nz) continue;
+      c->zchunk_phase = c->zchunk_mom = cand[q];
+      double bp = 1e30, bm = 1e30;
+      for (int t = 0; t < trials + 1; ++t) {
+        double ms[ST_COUNT];
+        int n = ST_COUNT;
+        if ((rc = mhit_profile_step(c, ms, nullptr, &n))) return rc;
+        if (t == 0) continue;  // first step after a reset is Euler
+        if (ms[ST_PHASE] >= 0) bp = std::min(bp, ms[ST_PHASE]);
+        bm = std::min(bm, ms[ST_MOM]);
+      }
+      if (bp < tp) {
+        tp = bp;
+        best_p = cand[q];
+      }
+      if (bm < tm) {
+        tm = bm;
+        best_m = cand[q];
+      }
+    }
+    for (int o = b; o < e->nbox; ++o) {
+      mhit_ctx* d = e->box[o];
+      if (d->g.nx == c->g.nx && d->g.ny == c->g.ny && d->g.nz == c->g.nz && d->prm.phiflag == c->prm.phiflag) {
+        d->zchunk_phase = best_p;
+        d->zchunk_mom = best_m;
+        done[o] = true;
+      }
+    }
+    if ((rc = reset_state(c))) return rc;
+  }
+  int best_l = e->nbox;
+  double best_t = 1e30;
+  for (int nl = 1;; nl *= 2) {
+    const int lanes = std::min(nl, e->nbox);
+    if ((rc = ens_set_lanes(e, lanes))) return rc;
+    for (mhit_ctx* c : e->box)
+      if ((rc = reset_state(c))) return rc;
+    double ms = 0.0;
+    if ((rc = ens_enqueue_steps(e, 2))) return rc;  // Euler + graph build
+    if ((rc = mhit_ensemble_time_steps(e, 2 * trials, &ms))) return rc;
+    if (ms < best_t) {
+      best_t = ms;
+      best_l = lanes;
+    }
+    if (lanes == e->nbox) break;
+  }
+  if ((rc = ens_set_lanes(e, best_l))) return rc;
+  for (mhit_ctx* c : e->box)
+    if ((rc = reset_state(c))) return rc;
+  if (nlanes_out) *nlanes_out = best_l;
+  return MHIT_OK;
+}
+
+int mhit_ensemble_tuning(mhit_ensemble* e, int* nlanes, int* zchunk_phase, int* zchunk_mom) {
+  if (!e) return set_error(MHIT_ERR_ARG, "null ensemble");
+  if (nlanes) *nlanes = e->nlanes;
+  for (int b = 0; b < e->nbox; ++b) {
+    if (zchunk_phase) zchunk_phase[b] = e->box[b]->zchunk_phase;
+    if (zchunk_mom) zchunk_mom[b] = e->box[b]->zchunk_mom;
   }
   return MHIT_OK;
 }

@@ -1,0 +1,71 @@
+"""Ensemble of boxes of uneven sizes: one graph launch per step must give exactly the fields of
+stepping every box on its own (the same kernels; z-chunk and stream choices of the autotuner do
+not change any cell's arithmetic), and the boxes must match the oracle."""
+import numpy as np
+import pytest
+
+from mhit36_mixedp_b200 import Ensemble, MhitStateError, Params, Solver, synth
+from oracle import mhit_oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+
+def box_cases():
+    specs = [(16, 0, "fp64"), (32, 1, "fp32"), (64, 1, "fp64"), (32, 0, "fp64")]
+    out = []
+    for b, (n, phiflag, poisson) in enumerate(specs):
+        prm = Params(nx=n, dt=5e-4, mu=0.004 + 0.001 * b, radius=0.3, sigma=0.5, phiflag=phiflag, poisson=poisson)
+        u, v, w = synth.solenoidal_velocity(n, 100 + b)
+        phi = synth.drops_phi(n, synth.drop_centres(4 + b, 200 + b), 0.3, 2 * np.pi / n) if phiflag else None
+        out.append((prm, u, v, w, phi))
+    return out
+
+
+def standalone(prm, u, v, w, phi, nsteps):
+    with Solver(prm) as s:
+        s.upload(u, v, w, phi)
+        s.step(nsteps)
+        return s.download()
+
+
+@pytest.mark.parametrize("tune", [False, True])
+def test_ensemble_matches_standalone(gpu, tune):
+    cases = box_cases()
+    with Ensemble([c[0] for c in cases]) as ens:
+        if tune:
+            t = ens.autotune(trials=1)
+            assert 1 <= t["lanes"] <= len(cases)
+            assert all(z in (8, 16, 32, 64) for z in t["zchunk_mom"])
+        for box, (prm, u, v, w, phi) in zip(ens.boxes, cases):
+            box.upload(u, v, w, phi)
+        ens.step(6)
+        got = [box.download() for box in ens.boxes]
+    for (prm, u, v, w, phi), g in zip(cases, got):
+        ref = standalone(prm, u, v, w, phi, 6)
+        for k in ref:
+            np.testing.assert_array_equal(g[k], ref[k])
+
+
+def test_ensemble_box_matches_oracle(gpu):
+    prm, u, v, w, phi = box_cases()[2]
+    with Ensemble([c[0] for c in box_cases()]) as ens:
+        for box, (p_, u_, v_, w_, phi_) in zip(ens.boxes, box_cases()):
+            box.upload(u_, v_, w_, phi_)
+        ens.step(4)
+        g = ens.boxes[2].download()
+    op = orc.Params(nx=64, dt=5e-4, mu=prm.mu, radius=0.3, sigma=0.5, phiflag=1)
+    st = orc.new_state(op, u, v, w, phi=phi)
+    orc.run(op, st, 4)
+    for k in ("u", "v", "w", "phi"):
+        ref = getattr(st, k)
+        assert np.max(np.abs(g[k] - ref)) / np.max(np.abs(ref)) < 1e-12
+
+
+def test_ensemble_requires_boxes_in_step(gpu):
+    cases = box_cases()[:2]
+    with Ensemble([c[0] for c in cases]) as ens:
+        for box, (prm, u, v, w, phi) in zip(ens.boxes, cases):
+            box.upload(u, v, w, phi)
+        ens.boxes[0].step(1)
+        with pytest.raises(MhitStateError):
+            ens.step(1)
