@@ -41,6 +41,8 @@ extern "C" {
 /* Poisson precision (multi/main.f90:844,853-912) */
 #define MHIT_POISSON_FP64 0    /* the intended FP64 solve of the main branch */
 #define MHIT_POISSON_FP32 1    /* this branch: rhs cast to FP32, FP32 transforms, FP32 pressure */
+#define MHIT_POISSON_FP32_REFINED 2 /* FP32 solve + one FP64 residual sweep (needs MHIT_LAP_MODIFIED):
+                                       r = rhs - L_h p32 in FP64, L_h d = r in FP32, p = p32 + d */
 
 /* Laplacian symbol of the spectral divide */
 #define MHIT_LAP_EXACT 0       /* exact integer k^2, as multi/main.f90:889 */
@@ -179,7 +181,8 @@ int mhit_ensemble_tuning(mhit_ensemble* e, int* nlanes, int* zchunk_phase, int* 
 #define MHIT_STAGE_ZSOLVE 5
 #define MHIT_STAGE_YINV 6
 #define MHIT_STAGE_XINV 7
-#define MHIT_STAGE_CORRECT 8
+#define MHIT_STAGE_REFINE 8
+#define MHIT_STAGE_CORRECT 9
 #define MHIT_BUF_U 0
 #define MHIT_BUF_V 1
 #define MHIT_BUF_W 2

@@ -19,7 +19,7 @@ MHIT_ERR_CFL = -4
 MHIT_ERR_IO = -5
 MHIT_ERR_STATE = -6
 
-POISSON = {"fp64": 0, "fp32": 1}
+POISSON = {"fp64": 0, "fp32": 1, "fp32_refined": 2}
 LAPLACIAN = {"exact": 0, "modified": 1}
 INTERP = {"linear1d": 0, "trilinear": 1}
 
@@ -85,7 +85,7 @@ SIGNATURES = {
     "mhit_debug_get_buffer": (_c.c_int, [_c.c_void_p, _c.c_int, _dp]),
 }
 
-STAGES = ["tracer", "phase", "momentum", "xfwd", "yfwd", "zsolve", "yinv", "xinv", "correct"]
+STAGES = ["tracer", "phase", "momentum", "xfwd", "yfwd", "zsolve", "yinv", "xinv", "refine", "correct"]
 BUFFERS = ["u", "v", "w", "un", "vn", "wn", "p", "phi", "phin", "ru", "rv", "rw", "rphi", "spec"]
 
 _lib = None

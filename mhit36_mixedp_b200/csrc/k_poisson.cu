@@ -36,10 +36,13 @@ template <> __device__ __forceinline__ void store2<float>(float* p, float a, flo
 template <typename T, int M> __host__ __device__ constexpr int xpass_threads() { return fft_threads<M, Tile<T>::B>(); }
 
 // ------------------------------------------------------------------ forward x + divergence
-template <typename T, int M>
+// RESID: transform the real FP32 field `rr` (the residual of the refinement sweep) instead of
+// the divergence of u*.
+template <typename T, int M, bool RESID>
 __global__ void __launch_bounds__(xpass_threads<T, M>())
 k_div_fftx(const double* __restrict__ u, const double* __restrict__ v, const double* __restrict__ w,
-           Cx<T>* __restrict__ spec, const Cx<T>* __restrict__ twx, Geo g, double cdiv) {
+           const float* __restrict__ rr, Cx<T>* __restrict__ spec, const Cx<T>* __restrict__ twx, Geo g,
+           double cdiv) {
   constexpr int B = Tile<T>::B;
   constexpr int NT = xpass_threads<T, M>();
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -52,7 +55,11 @@ k_div_fftx(const double* __restrict__ u, const double* __restrict__ v, const dou
     const int b = e / M, n = e - b * M;
     const int line = min(line0 + b, nlines - 1);  // a tail tile repeats the last line
     Cx<T> z;
-    {
+    if constexpr (RESID) {
+      const float2 r2 = __ldg(reinterpret_cast<const float2*>(rr + (size_t)line * nx + 2 * n));
+      z.x = (T)r2.x;
+      z.y = (T)r2.y;
+    } else {
       const int k = line / ny, j = line - k * ny;
       const int jp = wrapp(j, ny), kp = wrapp(k, nz);
       const int i = 2 * n;
@@ -231,12 +238,12 @@ template <typename T, int M>
 static cudaError_t launch_xfwd_m(const PoissonArgs& a, cudaStream_t st) {
   constexpr int B = Tile<T>::B;
   const size_t smem = (size_t)(M + 1) * B * sizeof(Cx<T>);
-  auto kern = k_div_fftx<T, M>;
+  auto kern = a.rreal ? k_div_fftx<T, M, true> : k_div_fftx<T, M, false>;
   cudaError_t e = prep_smem(kern, smem);
   if (e != cudaSuccess) return e;
   const int nlines = a.g.ny * a.g.nz;
-  kern<<<(nlines + B - 1) / B, xpass_threads<T, M>(), smem, st>>>(a.u, a.v, a.w, (Cx<T>*)a.spec, (const Cx<T>*)a.twx,
-                                                          a.g, a.cdiv);
+  kern<<<(nlines + B - 1) / B, xpass_threads<T, M>(), smem, st>>>(a.u, a.v, a.w, a.rreal, (Cx<T>*)a.spec,
+                                                                  (const Cx<T>*)a.twx, a.g, a.cdiv);
   return cudaGetLastError();
 }
 

@@ -44,11 +44,11 @@ int set_cuda_error(cudaError_t e, const char* expr, const char* file, int line) 
 using namespace mhit;
 
 enum {
-  ST_TRACER = 0, ST_PHASE, ST_MOM, ST_XFWD, ST_YFWD, ST_ZSOLVE, ST_YINV, ST_XINV, ST_CORRECT, ST_COUNT
+  ST_TRACER = 0, ST_PHASE, ST_MOM, ST_XFWD, ST_YFWD, ST_ZSOLVE, ST_YINV, ST_XINV, ST_REFINE, ST_CORRECT, ST_COUNT
 };
 static const char* kStageNames[ST_COUNT] = {"k_tracer", "k_phase", "k_mom", "k_div_fftx", "k_fft_cols_yfwd",
                                             "k_fft_cols_zsolve", "k_fft_cols_yinv", "k_fftx_inv",
-                                            "k_correct+k_finalize"};
+                                            "refine(k_residual+5 passes+k_combine)", "k_correct+k_finalize"};
 
 struct mhit_ctx {
   mhit_params prm;
@@ -60,6 +60,8 @@ struct mhit_ctx {
   double *RU = nullptr, *RV = nullptr, *RW = nullptr;
   double *PHI[2] = {}, *RPHI = nullptr;
   void* P = nullptr;
+  float* P2 = nullptr;    // refinement: residual, then the pressure correction (FP32)
+  double* P64 = nullptr;  // refinement: corrected pressure (FP64)
   void* spec = nullptr;
   void *twx = nullptr, *twy = nullptr, *twz = nullptr;
   double *k2x = nullptr, *k2y = nullptr, *k2z = nullptr;
@@ -79,7 +81,7 @@ struct mhit_ctx {
 };
 
 // ------------------------------------------------------------------ helpers
-static size_t tsize(const mhit_ctx* c) { return c->prm.poisson == MHIT_POISSON_FP32 ? 4 : 8; }
+static size_t tsize(const mhit_ctx* c) { return c->prm.poisson == MHIT_POISSON_FP64 ? 8 : 4; }
 
 static int check_ctx(mhit_ctx* c) {
   if (!c) return set_error(MHIT_ERR_ARG, "null context");
@@ -154,6 +156,7 @@ __global__ void k_clear_mean(DevScalars* sc) {
 static bool stage_runs(const mhit_ctx* c, int stage) {
   if (stage == ST_TRACER) return c->prm.partflag && c->np > 0;
   if (stage == ST_PHASE) return c->prm.phiflag != 0;
+  if (stage == ST_REFINE) return c->prm.poisson == MHIT_POISSON_FP32_REFINED;
   return true;
 }
 
@@ -223,10 +226,11 @@ static int enqueue_stage(mhit_ctx* c, int stage, double alpha, double beta, int 
     case ST_YFWD:
     case ST_ZSOLVE:
     case ST_YINV:
-    case ST_XINV: {
+    case ST_XINV:
+    case ST_REFINE: {
       PoissonArgs a;
       a.g = c->g;
-      a.fp32 = p.poisson == MHIT_POISSON_FP32;
+      a.fp32 = p.poisson != MHIT_POISSON_FP64;
       a.u = c->U[nxt];
       a.v = c->V[nxt];
       a.w = c->W[nxt];
@@ -240,7 +244,24 @@ static int enqueue_stage(mhit_ctx* c, int stage, double alpha, double beta, int 
       a.k2z = c->k2z;
       a.cdiv = p.rho * c->g.dxi / p.dt;  // (rho*dxi/dt), multi/main.f90:841
       a.ntot = (double)c->g.nx * (double)c->g.ny * (double)c->g.nz;
-      MHIT_CUDA_TRY(poisson_stage(a, stage - ST_XFWD, c->st));
+      if (stage != ST_REFINE) {
+        MHIT_CUDA_TRY(poisson_stage(a, stage - ST_XFWD, c->st));
+        return MHIT_OK;
+      }
+      // one FP64 residual sweep: r -> P2, L_h delta = r in FP32 (delta -> P2), P64 = P + P2
+      ResidArgs r;
+      r.g = c->g;
+      r.u = c->U[nxt];
+      r.v = c->V[nxt];
+      r.w = c->W[nxt];
+      r.p = static_cast<const float*>(c->P);
+      r.r = c->P2;
+      r.cdiv = a.cdiv;
+      MHIT_CUDA_TRY(launch_residual(r, c->st));
+      a.rreal = c->P2;
+      a.p = c->P2;
+      for (int s = 0; s < PSTAGE_COUNT; ++s) MHIT_CUDA_TRY(poisson_stage(a, s, c->st));
+      MHIT_CUDA_TRY(launch_combine(static_cast<const float*>(c->P), c->P2, c->P64, c->n, c->st));
       return MHIT_OK;
     }
     case ST_CORRECT: {
@@ -249,7 +270,8 @@ static int enqueue_stage(mhit_ctx* c, int stage, double alpha, double beta, int 
       a.u = c->U[nxt];
       a.v = c->V[nxt];
       a.w = c->W[nxt];
-      a.p = c->P;
+      const bool refined = p.poisson == MHIT_POISSON_FP32_REFINED;
+      a.p = refined ? static_cast<const void*>(c->P64) : c->P;
       a.fp32 = p.poisson == MHIT_POISSON_FP32;
       a.partials = c->partials;
       a.nblocks = c->nblk;
@@ -423,6 +445,8 @@ void mhit_destroy(mhit_ctx* c) {
   cudaFree(c->RW);
   cudaFree(c->RPHI);
   cudaFree(c->P);
+  cudaFree(c->P2);
+  cudaFree(c->P64);
   cudaFree(c->spec);
   cudaFree(c->twx);
   cudaFree(c->twy);
@@ -490,6 +514,11 @@ static int init_impl(const mhit_params* p, mhit_ctx* c) {
   if (p->phiflag) MHIT_CUDA_TRY(cudaMalloc(&c->RPHI, fb));
   const size_t ts = tsize(c);
   MHIT_CUDA_TRY(cudaMalloc(&c->P, n * ts));
+  if (p->poisson == MHIT_POISSON_FP32_REFINED) {
+    MHIT_CUDA_TRY(cudaMalloc(&c->P2, n * sizeof(float)));
+    MHIT_CUDA_TRY(cudaMalloc(&c->P64, n * sizeof(double)));
+    MHIT_CUDA_TRY(cudaMemset(c->P64, 0, n * sizeof(double)));
+  }
   MHIT_CUDA_TRY(cudaMemset(c->P, 0, n * ts));
   MHIT_CUDA_TRY(cudaMalloc(&c->spec, (size_t)g.pitch * g.ny * g.nz * 2 * ts));
   MHIT_CUDA_TRY(cudaMemset(c->spec, 0, (size_t)g.pitch * g.ny * g.nz * 2 * ts));
@@ -552,8 +581,11 @@ int mhit_init(const mhit_params* p, mhit_ctx** out) {
   }
   if (p->nx != 2 * (p->nx / 2) || !(p->dt > 0) || !(p->rho > 0) || !(p->epsr > 0))
     return set_error(MHIT_ERR_ARG, "dt, rho and epsr must be positive");
-  if (p->poisson != MHIT_POISSON_FP64 && p->poisson != MHIT_POISSON_FP32)
-    return set_error(MHIT_ERR_ARG, "poisson must be MHIT_POISSON_FP64 or MHIT_POISSON_FP32");
+  if (p->poisson != MHIT_POISSON_FP64 && p->poisson != MHIT_POISSON_FP32 && p->poisson != MHIT_POISSON_FP32_REFINED)
+    return set_error(MHIT_ERR_ARG, "poisson must be MHIT_POISSON_FP64, _FP32 or _FP32_REFINED");
+  if (p->poisson == MHIT_POISSON_FP32_REFINED && p->laplacian != MHIT_LAP_MODIFIED)
+    return set_error(MHIT_ERR_ARG, "MHIT_POISSON_FP32_REFINED needs laplacian = MHIT_LAP_MODIFIED (its residual is the "
+                                   "7-point operator)");
   if (p->laplacian != MHIT_LAP_EXACT && p->laplacian != MHIT_LAP_MODIFIED)
     return set_error(MHIT_ERR_ARG, "laplacian must be MHIT_LAP_EXACT or MHIT_LAP_MODIFIED");
   if (p->interp != MHIT_INTERP_LINEAR1D && p->interp != MHIT_INTERP_TRILINEAR)
@@ -696,7 +728,9 @@ int mhit_download_fields(mhit_ctx* c, double* u, double* v, double* w, double* p
     MHIT_CUDA_TRY(cudaMemcpyAsync(phi, c->PHI[c->cur], fb, cudaMemcpyDeviceToHost, c->st));
   }
   std::vector<float> pf;
-  if (p) {
+  if (p && c->P64) {
+    MHIT_CUDA_TRY(cudaMemcpyAsync(p, c->P64, fb, cudaMemcpyDeviceToHost, c->st));
+  } else if (p) {
     if (tsize(c) == 4) {
       pf.resize(n);
       MHIT_CUDA_TRY(cudaMemcpyAsync(pf.data(), c->P, n * 4, cudaMemcpyDeviceToHost, c->st));
@@ -712,7 +746,7 @@ int mhit_download_fields(mhit_ctx* c, double* u, double* v, double* w, double* p
     if (m != 0.0)
       for (size_t i = 0; i < n; ++i) outs[q][i] = outs[q][i] - m;
   }
-  if (p && tsize(c) == 4)
+  if (p && !c->P64 && tsize(c) == 4)
     for (size_t i = 0; i < n; ++i) p[i] = (double)pf[i];
   return MHIT_OK;
 }

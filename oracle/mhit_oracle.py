@@ -56,7 +56,7 @@ class Params:
     epsr: float = 1.0
     phiflag: int = 0
     partflag: int = 0
-    poisson: str = "fp64"          # "fp64" | "fp32"  (multi/main.f90:844,853-912)
+    poisson: str = "fp64"          # "fp64" | "fp32" (multi/main.f90:844,853-912) | "fp32_refined"
     laplacian: str = "exact"       # "exact" k^2 (multi/main.f90:889) | "modified" (2-2cos)/dx^2
     yz_shift: int = 1              # 1: reference labelling of y/z planes, 0: grid aligned
     interp: str = "linear1d"       # "linear1d" (multi/particles.f90:114-117) | "trilinear"
@@ -423,12 +423,21 @@ def poisson_solve(p: Params, rhsp):
             hat[0, 0, 0] = 0.0
             pr = np.fft.irfftn(hat, s=rhsp.shape, axes=(0, 1, 2), norm="forward")
             return pr
-        if p.poisson == "fp32":
-            r32 = rhsp.astype(np.float32)
-            hat = fft3_r2c_f32(r32)
-            hat = (-(hat.astype(np.complex128)) / k2 / float(n)).astype(np.complex64)
-            hat[0, 0, 0] = 0.0
-            return fft3_c2r_f32(hat, rhsp.shape)
+        if p.poisson in ("fp32", "fp32_refined"):
+            def solve32(rhs):
+                hat = fft3_r2c_f32(rhs.astype(np.float32))
+                hat = (-(hat.astype(np.complex128)) / k2 / float(n)).astype(np.complex64)
+                hat[0, 0, 0] = 0.0
+                return fft3_c2r_f32(hat, rhsp.shape)
+            p32 = solve32(rhsp)
+            if p.poisson == "fp32":
+                return p32
+            # one FP64 residual sweep: r = rhs - L_h p32 in FP64, L_h delta = r in FP32
+            q = p32.astype(np.float64)
+            lap = ((xp(q) - 2.0 * q + xm(q)) * p.ddxi + (yp(q) - 2.0 * q + ym(q)) * p.ddxi
+                   + (zp(q) - 2.0 * q + zm(q)) * p.ddxi)
+            delta = solve32(rhsp - lap)
+            return q + delta.astype(np.float64)
     raise ValueError(p.poisson)
 
 

@@ -149,3 +149,25 @@ def test_modified_laplacian_divergence(gpu):
         assert relerr(out[f], getattr(st, f)) < TOL64
     umax = max(np.abs(out[f]).max() for f in ("u", "v", "w"))
     assert dg["maxdiv"] < 1e-11 * umax * (32 / (2 * np.pi))
+
+
+def test_fp32_refined_recovers_fp64(gpu):
+    """FP32 Poisson + one FP64 residual sweep (modified Laplacian): u matches the FP64 solve and
+    the refined oracle to 1e-12 and the projected divergence is round-off, while the plain FP32
+    solve is off by ~1e-10."""
+    prm, u, v, w, phi, part = make_case(32, laplacian="modified", poisson="fp32_refined")
+    st, out, dg, _ = run_both(prm, u, v, w, phi, part, 5)
+    for f in ("u", "v", "w"):
+        assert relerr(out[f], getattr(st, f)) < TOL64, f
+    prm64 = dict(prm, poisson="fp64")
+    st64, out64, dg64, _ = run_both(prm64, u, v, w, phi, part, 5)
+    for f in ("u", "v", "w"):
+        assert relerr(out[f], out64[f]) < TOL64, f
+    umax = max(np.abs(out[f]).max() for f in ("u", "v", "w"))
+    assert dg["maxdiv"] < 1e-11 * umax * (32 / (2 * np.pi))
+
+
+def test_fp32_refined_needs_modified_laplacian(gpu):
+    from mhit36_mixedp_b200 import MhitArgError
+    with pytest.raises(MhitArgError, match="MODIFIED"):
+        Solver(Params(nx=32, poisson="fp32_refined"))
