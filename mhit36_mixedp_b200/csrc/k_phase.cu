@@ -1,14 +1,20 @@
 // ACDI phase-field transport: multi/main.f90:522-636 in one kernel.
 //
 // The reference makes five passes with three stored intermediates (psidi, tanh_psi and the
-// three normal components) and six halo exchanges.  Here a block owns a PTX x PTY column of
-// cells and marches up a chunk of z planes, keeping three rings of planes in shared memory:
-//   phi  planes k-2..k+5 (two planes in flight via cp.async), x/y halo 2
-//   psi  = eps log((min(phi,1)+1e-16)/(1-min(phi,1)+1e-16))          (:527-528), halo 2
-//   F    = 1/4 (1 - t^2) n/(|n|+1e-16), n = central psi differences (:559-561, :586-589,
-//          :609-614), halo 1, with t = tanh(psi/(2 eps)) (:530)
-// and writes only phi^{n+1} and rhsphi_o.  psi and F are recomputed on the x-y halo of the
-// tile (factors (PTX+4)(PTY+4)/(PTX PTY) and (PTX+2)(PTY+2)/(PTX PTY)).
+// three normal components) and six halo exchanges.  Here a block owns a TX x TY column of
+// cells and marches up a chunk of z planes.  It has one thread per position of the tile plus
+// its x/y halo of 2 ((TX+4)(TY+4) threads), and each thread keeps its own z column in
+// registers:
+//   phi  planes k-1..k+3 (k+3 loaded one plane ahead)
+//   psi  = eps log((min(phi,1)+1e-16)/(1-min(phi,1)+1e-16))            (:527-528), k..k+2
+//   Fz   of F = 1/4 (1 - t^2) n/(|n|+1e-16), n = central psi differences (:559-561,
+//        :586-589, :609-614), t = tanh(psi/(2 eps)) (:530),               planes k-1..k+1
+// Only x/y neighbours go through shared memory: psi(k+1), phi(k) and Fx, Fy(k), each
+// double-buffered.  Every shared read of plane k's iteration reads what the previous
+// iteration wrote, so one barrier per plane suffices.  psi is evaluated on the halo of 2 and F
+// on the halo of 1 (factors (TX+4)(TY+4)/(TX TY) and (TX+2)(TY+2)/(TX TY)); threads are
+// numbered so that the TX x TY output cells fill whole warps, then the F ring, then the outer
+// psi-only ring.  The kernel writes only phi^{n+1} and rhsphi_o.
 //
 // t is evaluated in closed form: tanh(log(r)/2) = (r-1)/(r+1) with r = (val+1e-16)/(1-val+1e-16)
 // gives t = (2 val - 1)/(1 + 2e-16) exactly in real arithmetic; in float64 it agrees with the
@@ -20,249 +26,201 @@
 //
 // gamma = 1.0*gumax is read from the device scalars written by the previous projection
 // (:536, :998-1002); u, v, w are the stored fields minus the lazily removed mean.
-#include <cuda_pipeline.h>
-
 #include "common.cuh"
 #include "kernels.h"
 
 namespace mhit {
 
-constexpr int PTX = 32, PTY = 16, PNT = PTX * PTY;
+constexpr int PTX = 32, PTY = 16;            // output cells per block in x, y
+constexpr int PHX = PTX + 4, PHY = PTY + 4;  // positions with the halo of 2
+constexpr int PNT = PHX * PHY;               // threads per block = positions
+constexpr int PNI = PTX * PTY;               // output cells
+constexpr int PNF = (PHX - 2) * (PHY - 2);   // F positions (halo 1)
 constexpr int PZC = 64;                      // default z planes per block
-constexpr int PHX = PTX + 4, PHY = PTY + 4;  // phi / psi plane (halo 2)
-constexpr int PHL = PHX * PHY;
-constexpr int PFX = PTX + 2, PFY = PTY + 2;  // F plane (halo 1)
-constexpr int PFL = PFX * PFY;
-constexpr int PCPY = (PHL + PNT - 1) / PNT;
 constexpr double ENUM = 1.0e-16;
 constexpr double TNORM = 1.0 / (1.0 + 2.0 * ENUM);
-
-struct PhaseSmem {
-  double phi[7][PHL];   // planes k-2..k+4 (k+4, k+5 in flight while iteration k runs)
-  double psi[4][PHL];   // planes k..k+3
-  double F[3][3][PFL];  // planes k-1..k+1
-};
 
 __device__ __forceinline__ int pmodi(int x, int n) {
   x %= n;
   return x < 0 ? x + n : x;
 }
 
-// Software pipeline, two barriers per output plane k, phi prefetched two planes ahead:
-//   wait phi(k+3); B1; cp.async phi(k+5); { psi(k+3), F(k+1) } as one task list; B2; out(k)
-__global__ void __launch_bounds__(PNT, 2) k_phase(PhaseArgs a) {
+// position of ring element r of the w x h rectangle perimeter starting at (x0, y0): top row,
+// bottom row, left column, right column
+__device__ __forceinline__ void ring_pos(int r, int x0, int y0, int w, int h, int& x, int& y) {
+  if (r < w) { x = x0 + r; y = y0; return; }
+  r -= w;
+  if (r < w) { x = x0 + r; y = y0 + h - 1; return; }
+  r -= w;
+  if (r < h - 2) { x = x0; y = y0 + 1 + r; return; }
+  r -= h - 2;
+  x = x0 + w - 1;
+  y = y0 + 1 + r;
+}
+
+template <bool CLAMP>
+__global__ void __launch_bounds__(PNT, 1) k_phase(PhaseArgs a) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  PhaseSmem& S = *reinterpret_cast<PhaseSmem*>(smraw);
+  // thread -> position (hx, hy) in the (PHX x PHY) grid of the tile with its halo
+  const int tid = threadIdx.x;
+  int hx, hy;
+  if (tid < PNI) {
+    hx = 2 + tid % PTX;
+    hy = 2 + tid / PTX;
+  } else if (tid < PNF) {
+    ring_pos(tid - PNI, 1, 1, PHX - 2, PHY - 2, hx, hy);
+  } else {
+    ring_pos(tid - PNF, 0, 0, PHX, PHY, hx, hy);
+  }
+  const int q = hy * PHX + hx;  // this position in a shared plane
+  // shared planes at this position: psi[2], phi[2], Fx[2], Fy[2]
+  double* sps = reinterpret_cast<double*>(smraw) + q;
+  double* sph = sps + 2 * PNT;
+  double* sfx = sph + 2 * PNT;
+  double* sfy = sfx + 2 * PNT;
+  auto slot = [](int m) { return (m & 1) * PNT; };
+
   const Geo& g = a.g;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
-  const size_t plane = (size_t)nx * ny;
+  const int plane = nx * ny, ntot = plane * nz;
   const int i0 = blockIdx.x * PTX, j0 = blockIdx.y * PTY;
   const int zc = a.zchunk > 0 ? a.zchunk : PZC;
-  const int k0 = blockIdx.z * zc;
-  const int k1 = min(k0 + zc, nz);
-  const int tid = threadIdx.x;
+  const int k0 = blockIdx.z * zc, k1 = min(k0 + zc, nz);
+  const int i = i0 - 2 + hx, j = j0 - 2 + hy;
+  const int col = pmodi(j, ny) * nx + pmodi(i, nx);
+  const bool frole = tid < PNF;
+  const bool orole = tid < PNI && i < nx && j < ny;
   const double eps = g.eps;
-  const int clamp = a.clamp;
   const double* __restrict__ phig = a.phi;
 
-  int poff[PCPY];
-#pragma unroll
-  for (int c = 0; c < PCPY; ++c) {
-    const int e = tid + c * PNT;
-    poff[c] = -1;
-    if (e < PHL) {
-      const int y = e / PHX, x = e - y * PHX;
-      poff[c] = pmodi(j0 - 2 + y, ny) * nx + pmodi(i0 - 2 + x, nx);
-    }
-  }
-  auto slot7 = [&](int m) { return (m - k0 + 9) % 7; };
-  auto slot4 = [&](int m) { return (m - k0 + 8) & 3; };
-  auto slot3 = [&](int m) { return (m - k0 + 6) % 3; };
-  auto issue_phi = [&](int m) {
-    const size_t base = (size_t)pmodi(m, nz) * plane;
-    double* dst = S.phi[slot7(m)];
-#pragma unroll
-    for (int c = 0; c < PCPY; ++c)
-      if (poff[c] >= 0) __pipeline_memcpy_async(dst + tid + c * PNT, phig + base + poff[c], 8);
+  auto clampv = [](double ph) {
+    double val = fmin(ph, 1.0);
+    if (CLAMP) val = fmax(val, 0.0);
+    return val;
   };
-  // psi of element e of a plane (multi/main.f90:527-528)
-  auto psi_at = [&](const double* __restrict__ P, double* __restrict__ Q, int e) {
-    double val = fmin(P[e], 1.0);
-    if (clamp) val = fmax(val, 0.0);
-    Q[e] = eps * log((val + ENUM) / (1.0 - val + ENUM));
+  auto psi_of = [&](double ph) {  // multi/main.f90:527-528
+    const double val = clampv(ph);
+    return eps * log((val + ENUM) / (1.0 - val + ENUM));
   };
-  // F of one element (multi/main.f90:530, 559-561, 586-589, 609-614); q: psi-plane index,
-  // f: F-plane index
-  auto F_at = [&](const double* __restrict__ Qm, const double* __restrict__ Q0, const double* __restrict__ Qp,
-                  const double* __restrict__ P, double* __restrict__ Fd, int q, int f) {
-    double nxr = Q0[q + 1] - Q0[q - 1];
-    double nyr = Q0[q + PHX] - Q0[q - PHX];
-    double nzr = Qp[q] - Qm[q];
-    const double normag = 1.0 / (sqrt(nxr * nxr + nyr * nyr + nzr * nzr) + ENUM);
+  // F of this position at one plane (multi/main.f90:530, 559-561, 586-589, 609-614): Q the
+  // plane's shared psi at this position, dz the psi difference along z, ph/ps this position's
+  // phi/psi.  The fused multiply-adds are written out, so the rounding does not depend on how
+  // the compiler contracts each copy of the loop body.
+  auto F_of = [&](const double* __restrict__ Q, double dz, double ph, double ps, double& fx, double& fy,
+                  double& fz) {
+    double nxr = Q[1] - Q[-1];
+    double nyr = Q[PHX] - Q[-PHX];
+    double nzr = dz;
+    const double n2 = __fma_rn(nzr, nzr, __fma_rn(nyr, nyr, __dmul_rn(nxr, nxr)));
+    const double normag = 1.0 / (sqrt(n2) + ENUM);
     nxr = nxr * normag;
     nyr = nyr * normag;
     nzr = nzr * normag;
-    const double ps = Q0[q];
-    double val = fmin(P[q], 1.0);
-    if (clamp) val = fmax(val, 0.0);
-    const double t = (ps == ps) ? (2.0 * val - 1.0) * TNORM : ps;
-    const double fac = 0.25 * (1.0 - t * t);
-    Fd[f] = fac * nxr;
-    Fd[PFL + f] = fac * nyr;
-    Fd[2 * PFL + f] = fac * nzr;
+    const double val = clampv(ph);
+    const double tt = (ps == ps) ? (2.0 * val - 1.0) * TNORM : ps;
+    const double fac = 0.25 * __fma_rn(-tt, tt, 1.0);
+    fx = fac * nxr;
+    fy = fac * nyr;
+    fz = fac * nzr;
   };
-  auto F_plane_all = [&](int m) {
-    const double* Qm = S.psi[slot4(m - 1)];
-    const double* Q0 = S.psi[slot4(m)];
-    const double* Qp = S.psi[slot4(m + 1)];
-    const double* P = S.phi[slot7(m)];
-    double* Fd = S.F[slot3(m)][0];
-    for (int e = tid; e < PFL; e += PNT) {
-      const int y = e / PFX, x = e - y * PFX;
-      F_at(Qm, Q0, Qp, P, Fd, (y + 1) * PHX + (x + 1), e);
-    }
-  };
-
-  // prologue: phi k0-2..k0+3; psi k0-2..k0+2 (ring of 4); F k0-1, k0
-  for (int m = k0 - 2; m <= k0 + 3; ++m) issue_phi(m);
-  __pipeline_commit();
-  issue_phi(k0 + 4);
-  __pipeline_commit();
-  __pipeline_wait_prior(1);
-  __syncthreads();
-  for (int e = tid; e < 3 * PHL; e += PNT) {
-    const int m = k0 - 2 + e / PHL;
-    psi_at(S.phi[slot7(m)], S.psi[slot4(m)], e % PHL);
-  }
-  __syncthreads();
-  F_plane_all(k0 - 1);
-  __syncthreads();
-  for (int e = tid; e < 2 * PHL; e += PNT) {
-    const int m = k0 + 1 + e / PHL;
-    psi_at(S.phi[slot7(m)], S.psi[slot4(m)], e % PHL);
-  }
-  __syncthreads();
-  F_plane_all(k0);
-
-  // this thread's share of the per-plane task list {psi(k+3) elements, F(k+1) elements}
-  constexpr int NTASK = (PHL + PFL + PNT - 1) / PNT;
-  int tq[NTASK], tf[NTASK];  // psi task: tq = e, tf = -1; F task: tq = psi index, tf = F index
-#pragma unroll
-  for (int r = 0; r < NTASK; ++r) {
-    const int t = tid + r * PNT;
-    if (t < PHL) {
-      tq[r] = t;
-      tf[r] = -1;
-    } else if (t < PHL + PFL) {
-      const int e = t - PHL, y = e / PFX, x = e - y * PFX;
-      tq[r] = (y + 1) * PHX + (x + 1);
-      tf[r] = e;
-    } else {
-      tq[r] = -1;
-      tf[r] = -1;
-    }
-  }
 
   const double gamma = 1.0 * a.sc->gumax;
   const double mu_ = a.sc->mean[0], mv_ = a.sc->mean[1], mw_ = a.sc->mean[2];
   const double dxi = g.dxi, ddxi = g.ddxi, dt = g.dt;
   const double hdxi = 0.5 * dxi;  // (x*0.5)*dxi == x*(0.5*dxi) exactly
-  const int tx = tid % PTX, ty = tid / PTX;
-  const int i = i0 + tx, j = j0 + ty;
-  const bool own = (i < nx) && (j < ny);
-  const int ip = own ? wrapp(i, nx) : 0, jp = own ? wrapp(j, ny) : 0;
-  const int hq = (ty + 2) * PHX + (tx + 2);  // own cell in the phi/psi plane
-  const int fq = (ty + 1) * PFX + (tx + 1);  // own cell in the F plane
-  // running pointers to the own cell of plane k (and its +x, +y, +z neighbours)
-  const size_t c0 = (size_t)k0 * plane + (size_t)(own ? j : 0) * nx + (own ? i : 0);
-  const double* pu = a.u + c0;
-  const double* pv = a.v + c0;
-  const double* pw = a.w + c0;
-  const ptrdiff_t dux = (ptrdiff_t)ip - (own ? i : 0);
-  const ptrdiff_t dvy = ((ptrdiff_t)jp - (own ? j : 0)) * nx;
-  double* pphin = a.phin + c0;
-  double* prphi = a.rphio + c0;
+  const double alpha = a.alpha, beta = a.beta;
+  int c = k0 * plane + col;  // own cell (output role)
+  const int dux = (i + 1 == nx) ? 1 - nx : 1;
+  const int dvy = (j + 1 == ny) ? (1 - ny) * nx : nx;
+  double w0 = orole ? __ldg(a.w + c) : 0.0;
 
-  for (int k = k0; k < k1; ++k) {
-    // operands from HBM for this plane, issued before the barriers
-    const ptrdiff_t dwz = (k + 1 == nz) ? -(ptrdiff_t)(nz - 1) * (ptrdiff_t)plane : (ptrdiff_t)plane;
-    double u0 = 0, uxp = 0, v0 = 0, vyp = 0, w0 = 0, wzp = 0, ro = 0;
-    if (own) {
-      u0 = __ldg(pu);
-      uxp = __ldg(pu + dux);
-      v0 = __ldg(pv);
-      vyp = __ldg(pv + dvy);
-      w0 = __ldg(pw);
-      wzp = __ldg(pw + dwz);
-      ro = *prphi;
+  // Iteration k computes psi(k+2), F(k+1) and the output plane k.  The loop starts four planes
+  // below the chunk: k0-4 and k0-3 only fill psi(k0-2), psi(k0-1), k0-2 and k0-1 add F(k0-1),
+  // F(k0).  Every psi and F is thus evaluated by the loop body, so the values of a plane do
+  // not depend on where a z chunk starts.  Register state entering iteration k: phi k-1..k+2,
+  // psi k, k+1, Fz k-1, k.
+  double f_m1 = 0.0, f_0 = 0.0, f_p1 = 0.0, f_p2 = phig[pmodi(k0 - 2, nz) * plane + col];
+  double s_0 = 0.0, s_p1 = 0.0, z_m1 = 0.0, z_0 = 0.0;
+  int o3 = pmodi(k0 - 1, nz) * plane + col;  // phi(k+3) of the first iteration
+
+#pragma unroll 2
+  for (int k = k0 - 4; k < k1; ++k) {
+    const bool out = orole && k >= k0;
+    const double f_p3 = (k + 1 < k1) ? phig[o3] : 0.0;
+    o3 += plane;
+    if (o3 >= ntot) o3 -= ntot;
+    double u0 = 0, uxp = 0, v0 = 0, vyp = 0, wzp = 0, ro = 0;
+    if (out) {
+      const int cz = (k + 1 == nz) ? c - (nz - 1) * plane : c + plane;
+      u0 = __ldg(a.u + c);
+      uxp = __ldg(a.u + c + dux);
+      v0 = __ldg(a.v + c);
+      vyp = __ldg(a.v + c + dvy);
+      wzp = __ldg(a.w + cz);
+      ro = a.rphio[c];
     }
-    __pipeline_wait_prior(1);  // phi(k+3) landed; phi(k+4) may still be in flight
-    __syncthreads();
-    issue_phi(k + 5);
-    __pipeline_commit();
-    {
-      const double* P3 = S.phi[slot7(k + 3)];
-      double* Q3 = S.psi[slot4(k + 3)];
-      const double* Qm = S.psi[slot4(k)];
-      const double* Q0 = S.psi[slot4(k + 1)];
-      const double* Qp = S.psi[slot4(k + 2)];
-      const double* P1 = S.phi[slot7(k + 1)];
-      double* Fd = S.F[slot3(k + 1)][0];
-#pragma unroll
-      for (int r = 0; r < NTASK; ++r) {
-        if (tf[r] >= 0) F_at(Qm, Q0, Qp, P1, Fd, tq[r], tf[r]);
-        else if (tq[r] >= 0) psi_at(P3, Q3, tq[r]);
-      }
+    // psi(k+2) of this position; phi(k+1) for the next plane's neighbours
+    const double s_p2 = psi_of(f_p2);
+    sps[slot(k + 2)] = s_p2;
+    sph[slot(k + 1)] = f_p1;
+    // F(k+1) from the shared psi(k+1) (written last iteration) and the own psi(k+2) - psi(k)
+    double z_p1 = 0.0;
+    if (frole && k >= k0 - 2) {
+      double fx, fy;
+      F_of(sps + slot(k + 1), s_p2 - s_0, f_p1, s_p1, fx, fy, z_p1);
+      sfx[slot(k + 1)] = fx;
+      sfy[slot(k + 1)] = fy;
     }
-    __syncthreads();
-    if (own) {
-      u0 -= mu_;
-      uxp -= mu_;
-      v0 -= mv_;
-      vyp -= mv_;
-      w0 -= mw_;
-      wzp -= mw_;
-      const double* P0 = S.phi[slot7(k)];
-      const double p0 = P0[hq];
-      const double pxp = P0[hq + 1], pxm = P0[hq - 1], pyp = P0[hq + PHX], pym = P0[hq - PHX];
-      const double pzp = S.phi[slot7(k + 1)][hq], pzm = S.phi[slot7(k - 1)][hq];
+    // output plane k from the shared phi(k), Fx/Fy(k) and the own column
+    if (out) {
+      const double u_0 = u0 - mu_, u_x = uxp - mu_, v_0 = v0 - mv_, v_y = vyp - mv_;
+      const double w_0 = w0 - mw_, w_z = wzp - mw_;
+      const double* P0 = sph + slot(k);
+      const double p0 = f_0;
+      const double pxp = P0[1], pxm = P0[-1], pyp = P0[PHX], pym = P0[-PHX];
+      const double pzp = f_p1, pzm = f_m1;
       // multi/main.f90:551-557
-      double rhs = -((uxp * 0.5 * (pxp + p0) - u0 * 0.5 * (p0 + pxm)) * dxi) -
-                   (vyp * 0.5 * (pyp + p0) - v0 * 0.5 * (p0 + pym)) * dxi -
-                   (wzp * 0.5 * (pzp + p0) - w0 * 0.5 * (p0 + pzm)) * dxi +
+      double rhs = -((u_x * 0.5 * (pxp + p0) - u_0 * 0.5 * (p0 + pxm)) * dxi) -
+                   (v_y * 0.5 * (pyp + p0) - v_0 * 0.5 * (p0 + pym)) * dxi -
+                   (w_z * 0.5 * (pzp + p0) - w_0 * 0.5 * (p0 + pzm)) * dxi +
                    gamma * (eps * (pxp - 2.0 * p0 + pxm) * ddxi + eps * (pyp - 2.0 * p0 + pym) * ddxi +
                             eps * (pzp - 2.0 * p0 + pzm) * ddxi);
       // :609-614
-      const double* F0x = S.F[slot3(k)][0];
-      const double* F0y = S.F[slot3(k)][1];
-      rhs = rhs - gamma * ((F0x[fq + 1] - F0x[fq - 1]) * hdxi + (F0y[fq + PFX] - F0y[fq - PFX]) * hdxi +
-                           (S.F[slot3(k + 1)][2][fq] - S.F[slot3(k - 1)][2][fq]) * hdxi);
+      const double* Fx = sfx + slot(k);
+      const double* Fy = sfy + slot(k);
+      rhs = rhs - gamma * ((Fx[1] - Fx[-1]) * hdxi + (Fy[PHX] - Fy[-PHX]) * hdxi + (z_p1 - z_m1) * hdxi);
       // :625-626
-      *pphin = p0 + dt * (a.alpha * rhs - a.beta * ro);
-      *prphi = rhs;
+      a.phin[c] = p0 + dt * (alpha * rhs - beta * ro);
+      a.rphio[c] = rhs;
+      w0 = wzp;
+      c += plane;
     }
-    pu += plane;
-    pv += plane;
-    pw += plane;
-    pphin += plane;
-    prphi += plane;
+    __syncthreads();
+    f_m1 = f_0;
+    f_0 = f_p1;
+    f_p1 = f_p2;
+    f_p2 = f_p3;
+    s_0 = s_p1;
+    s_p1 = s_p2;
+    z_m1 = z_0;
+    z_0 = z_p1;
   }
-  __pipeline_wait_prior(0);
 }
 
 cudaError_t launch_phase(const PhaseArgs& a, cudaStream_t st) {
-  const size_t smem = sizeof(PhaseSmem);
-  static int attr_set[64] = {0};
+  constexpr size_t smem = 8 * sizeof(double) * PNT;  // psi, phi, Fx, Fy: two planes each
+  auto kern = a.clamp ? k_phase<true> : k_phase<false>;
+  static int attr_set[64][2] = {};
   int dev = 0;
   cudaGetDevice(&dev);
-  if (dev < 64 && !attr_set[dev]) {
-    cudaError_t e = cudaFuncSetAttribute(k_phase, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (dev >= 64 || !attr_set[dev][a.clamp ? 1 : 0]) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    attr_set[dev] = 1;
+    if (dev < 64) attr_set[dev][a.clamp ? 1 : 0] = 1;
   }
   const int zc = a.zchunk > 0 ? a.zchunk : PZC;
   dim3 grd((a.g.nx + PTX - 1) / PTX, (a.g.ny + PTY - 1) / PTY, (a.g.nz + zc - 1) / zc);
-  k_phase<<<grd, PNT, smem, st>>>(a);
+  kern<<<grd, PNT, smem, st>>>(a);
   return cudaGetLastError();
 }
 
