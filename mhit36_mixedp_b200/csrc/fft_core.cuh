@@ -197,4 +197,110 @@ __device__ __forceinline__ void fft_tile(Cx<T>* s, const Cx<T>* __restrict__ tw,
   }
 }
 
+
+// ---------------------------------------------------------------- stages with register I/O
+// Stage s of the transform in radix order REV (false: Radix<N>::r[0..ns-1], true: reversed).
+// Butterfly q = threadIdx.x + m NT works on column b = q % B, t = q / B: it reads elements
+// t + r N/R and writes elements (t/p) p R + t%p + r p, p the product of the earlier radices.
+// The first stage (p = 1) therefore reads, and the last stage (p = N/R) writes, the strided
+// set t + r N/R: those two stages can take their operands from, and leave their results in,
+// registers, so a tile loaded from (stored to) global memory skips a shared-memory pass.
+template <int N, bool REV> __host__ __device__ constexpr int rad(int s) {
+  return REV ? Radix<N>::r[Radix<N>::ns - 1 - s] : Radix<N>::r[s];
+}
+template <int N, bool REV> __host__ __device__ constexpr int pbefore(int s) {
+  int p = 1;
+  for (int i = 0; i < s; ++i) p *= rad<N, REV>(i);
+  return p;
+}
+template <int N, int B, int NT, int R> struct StageShape {
+  static constexpr int NB = N / R * B;
+  static constexpr int BPT = (NB + NT - 1) / NT;
+};
+template <int N, int B, int NT, int R> __device__ __forceinline__ bool st_valid(int m) {
+  constexpr int NB = StageShape<N, B, NT, R>::NB;
+  return NB % NT == 0 || (int)threadIdx.x + m * NT < NB;
+}
+
+template <typename T, int N, int B, int NT, int R>
+__device__ __forceinline__ void st_read(const Cx<T>* s, Cx<T> (&a)[StageShape<N, B, NT, R>::BPT][R]) {
+#pragma unroll
+  for (int m = 0; m < StageShape<N, B, NT, R>::BPT; ++m) {
+    if (st_valid<N, B, NT, R>(m)) {
+      const int q = threadIdx.x + m * NT, b = q % B, t = q / B;
+#pragma unroll
+      for (int r = 0; r < R; ++r) a[m][r] = s[sw<B>(t + r * (N / R), b)];
+    }
+  }
+}
+
+template <typename T, int N, int B, int NT, int R, bool INV>
+__device__ __forceinline__ void st_compute(Cx<T> (&a)[StageShape<N, B, NT, R>::BPT][R], const Cx<T>* __restrict__ tw,
+                                           int twstride, int p) {
+#pragma unroll
+  for (int m = 0; m < StageShape<N, B, NT, R>::BPT; ++m) {
+    if (st_valid<N, B, NT, R>(m)) {
+      const int q = threadIdx.x + m * NT, t = q / B, k = t % p;
+      if (p > 1) {
+        const int step = (N / (p * R)) * twstride;
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+          Cx<T> w = tw[r * k * step];
+          if (INV) w.y = -w.y;
+          a[m][r] = cmul(a[m][r], w);
+        }
+      }
+      dftR<T, INV, R>(a[m]);
+    }
+  }
+}
+
+template <typename T, int N, int B, int NT, int R>
+__device__ __forceinline__ void st_write(Cx<T>* s, const Cx<T> (&a)[StageShape<N, B, NT, R>::BPT][R], int p) {
+#pragma unroll
+  for (int m = 0; m < StageShape<N, B, NT, R>::BPT; ++m) {
+    if (st_valid<N, B, NT, R>(m)) {
+      const int q = threadIdx.x + m * NT, b = q % B, t = q / B, k = t % p;
+      const int j = (t / p) * p * R + k;
+#pragma unroll
+      for (int r = 0; r < R; ++r) s[sw<B>(j + r * p, b)] = a[m][r];
+    }
+  }
+}
+
+// Full transform in radix order REV: `in` holds the first stage's operands (elements
+// t + r N/R0), `out` receives the last stage's results (elements t + r N/R_last).  s is used
+// between stages; on entry no thread may still be reading s, and on return threads may still
+// be reading it (the caller synchronises before writing s again).
+template <typename T, int N, int B, int NT, bool INV, bool REV>
+__device__ __forceinline__ void fft_regs(
+    Cx<T>* s, const Cx<T>* __restrict__ tw, int twstride,
+    Cx<T> (&in)[StageShape<N, B, NT, rad<N, REV>(0)>::BPT][rad<N, REV>(0)],
+    Cx<T> (&out)[StageShape<N, B, NT, rad<N, REV>(Radix<N>::ns - 1)>::BPT][rad<N, REV>(Radix<N>::ns - 1)]) {
+  constexpr int NS = Radix<N>::ns;
+  constexpr int R0 = rad<N, REV>(0);
+  st_compute<T, N, B, NT, R0, INV>(in, tw, twstride, 1);
+  if constexpr (NS == 1) {
+#pragma unroll
+    for (int m = 0; m < StageShape<N, B, NT, R0>::BPT; ++m)
+#pragma unroll
+      for (int r = 0; r < R0; ++r) out[m][r] = in[m][r];
+  } else {
+    st_write<T, N, B, NT, R0>(s, in, 1);
+    __syncthreads();
+    if constexpr (NS == 3) {
+      constexpr int R1 = rad<N, REV>(1);
+      Cx<T> a1[StageShape<N, B, NT, R1>::BPT][R1];
+      st_read<T, N, B, NT, R1>(s, a1);
+      __syncthreads();
+      st_compute<T, N, B, NT, R1, INV>(a1, tw, twstride, pbefore<N, REV>(1));
+      st_write<T, N, B, NT, R1>(s, a1, pbefore<N, REV>(1));
+      __syncthreads();
+    }
+    constexpr int RL = rad<N, REV>(NS - 1);
+    st_read<T, N, B, NT, RL>(s, out);
+    st_compute<T, N, B, NT, RL, INV>(out, tw, twstride, pbefore<N, REV>(NS - 1));
+  }
+}
+
 }  // namespace mhit

@@ -178,13 +178,23 @@ k_fftx_inv(const Cx<T>* __restrict__ spec, T* __restrict__ p, const Cx<T>* __res
 
 // ------------------------------------------------------------------ y / z column passes
 // MODE 0: forward, 1: inverse, 2: forward + spectral divide + inverse (z only)
+// The first stage reads its operands straight from global memory and the last stage stores
+// its results straight to global memory; in MODE 2 the forward transform's last stage, the
+// divide and the inverse transform's first stage (radices in reversed order, so it works on the
+// same strided element set) stay in registers: 4 shared-memory passes over the tile per
+// transform of three stages instead of 8.  The z solve keeps two transforms' worth of
+// butterflies in registers and runs one block per SM without spills; the single transforms of
+// up to 512 points fit two blocks per SM.
 template <typename T, int N, int MODE>
-__global__ void __launch_bounds__(fft_threads<N, Tile<T>::B>())
+__global__ void __launch_bounds__(fft_threads<N, Tile<T>::B>(), (MODE == 2 || N >= 1024) ? 1 : 2)
 k_fft_cols(Cx<T>* __restrict__ spec, const Cx<T>* __restrict__ tw, Geo g, size_t stride_n,
            size_t stride_outer, const double* __restrict__ k2x, const double* __restrict__ k2y,
            const double* __restrict__ k2z, double ntot) {
   constexpr int B = Tile<T>::B;
   constexpr int NT = fft_threads<N, B>();
+  constexpr int NS = Radix<N>::ns;
+  constexpr int RA = rad<N, false>(0), RL = rad<N, false>(NS - 1);
+  constexpr int BA = StageShape<N, B, NT, RA>::BPT, BL = StageShape<N, B, NT, RL>::BPT;
   extern __shared__ __align__(16) unsigned char smraw[];
   Cx<T>* s = reinterpret_cast<Cx<T>*>(smraw);
   const int kx0 = blockIdx.x * B;
@@ -192,41 +202,66 @@ k_fft_cols(Cx<T>* __restrict__ spec, const Cx<T>* __restrict__ tw, Geo g, size_t
   const int nkx = g.nkx;
   Cx<T>* base = spec + (size_t)outer * stride_outer + kx0;
   // The row pitch is a multiple of 16 complex and the padding columns stay zero, so every
-  // B-wide tile is in bounds: all loads of the tile go out back to back as async copies.
-  for (int e = threadIdx.x; e < N * B; e += NT) {
-    const int n = e / B, b = e - n * B;
-    __pipeline_memcpy_async(&s[sw<B>(n, b)], &base[(size_t)n * stride_n + b], sizeof(Cx<T>));
+  // B-wide tile is in bounds.
+  Cx<T> a[BA][RA];
+#pragma unroll
+  for (int m = 0; m < BA; ++m) {
+    if (st_valid<N, B, NT, RA>(m)) {
+      const int q = threadIdx.x + m * NT, b = q % B, t = q / B;
+#pragma unroll
+      for (int r = 0; r < RA; ++r) a[m][r] = base[(size_t)(t + r * (N / RA)) * stride_n + b];
+    }
   }
-  __pipeline_commit();
-  __pipeline_wait_prior(0);
-  __syncthreads();
-  fft_tile<T, N, B, NT, MODE == 1>(s, tw, 1);
+  Cx<T> z[BL][RL];
+  fft_regs<T, N, B, NT, MODE == 1, false>(s, tw, 1, a, z);
   if constexpr (MODE == 2) {
     // multi/main.f90:889-895: phi3d = -phi3d/k2/(nx*ny*nz) in FP64, phi3d(1,1,1) = 0.
     // One reciprocal of k2*N per element (within 2 ulp of the reference's two divides).
     const double ky2 = k2y[outer];
-    for (int e = threadIdx.x; e < N * B; e += NT) {
-      const int n = e / B, b = e - n * B;
-      const int kx = kx0 + b;
-      if (kx < nkx) {
-        const double k2 = (k2x[kx] + ky2) + k2z[n];
-        const Cx<T> z = s[sw<B>(n, b)];
-        const double inv = 1.0 / (k2 * ntot);
-        double re = -(double)z.x * inv;
-        double im = -(double)z.y * inv;
-        if (kx == 0 && outer == 0 && n == 0) { re = 0.0; im = 0.0; }
-        s[sw<B>(n, b)] = cx<T>((T)re, (T)im);
+#pragma unroll
+    for (int m = 0; m < BL; ++m) {
+      if (st_valid<N, B, NT, RL>(m)) {
+        const int q = threadIdx.x + m * NT, b = q % B, t = q / B;
+        const int kx = kx0 + b;
+#pragma unroll
+        for (int r = 0; r < RL; ++r) {
+          const int n = t + r * (N / RL);
+          double re = 0.0, im = 0.0;
+          if (kx < nkx && !(kx == 0 && outer == 0 && n == 0)) {
+            const double k2 = (k2x[kx] + ky2) + k2z[n];
+            const double inv = 1.0 / (k2 * ntot);
+            re = -(double)z[m][r].x * inv;
+            im = -(double)z[m][r].y * inv;
+          }
+          z[m][r] = cx<T>((T)re, (T)im);
+        }
       }
     }
-    __syncthreads();
-    fft_tile<T, N, B, NT, true>(s, tw, 1);
-  }
-  for (int e = threadIdx.x; e < N * B; e += NT) {
-    const int n = e / B, b = e - n * B;
-    if (kx0 + b < nkx) base[(size_t)n * stride_n + b] = s[sw<B>(n, b)];
+    __syncthreads();  // every thread has read the forward transform's last stage
+    fft_regs<T, N, B, NT, true, true>(s, tw, 1, z, a);
+#pragma unroll
+    for (int m = 0; m < BA; ++m) {
+      if (st_valid<N, B, NT, RA>(m)) {
+        const int q = threadIdx.x + m * NT, b = q % B, t = q / B;
+        if (kx0 + b < nkx) {
+#pragma unroll
+          for (int r = 0; r < RA; ++r) base[(size_t)(t + r * (N / RA)) * stride_n + b] = a[m][r];
+        }
+      }
+    }
+  } else {
+#pragma unroll
+    for (int m = 0; m < BL; ++m) {
+      if (st_valid<N, B, NT, RL>(m)) {
+        const int q = threadIdx.x + m * NT, b = q % B, t = q / B;
+        if (kx0 + b < nkx) {
+#pragma unroll
+          for (int r = 0; r < RL; ++r) base[(size_t)(t + r * (N / RL)) * stride_n + b] = z[m][r];
+        }
+      }
+    }
   }
 }
-
 // ------------------------------------------------------------------ host launchers
 template <typename KernelT>
 static cudaError_t prep_smem(KernelT kern, size_t smem) {
