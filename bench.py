@@ -48,7 +48,7 @@ BYTES_PER_POINT = {
 # of one launch / cells): k_phase, k_mom from profiles/k_phase_k_mom_ns_acdi_256.md (256^3); the
 # Poisson and projection kernels from profiles/poisson_projection_fp32_512x512x256.md.  Traffic
 # scales with the cell count for these streaming kernels, so a launch at 512^3 moves 8x the bytes.
-TRAFFIC_PER_POINT = {"k_phase": 56.1, "k_mom": 104.5, "k_div_fftx": 28.4, "k_fft_cols_yfwd": 7.5,
+TRAFFIC_PER_POINT = {"k_phase": 55.1, "k_mom": 104.4, "k_div_fftx": 28.4, "k_fft_cols_yfwd": 7.5,
                      "k_fft_cols_zsolve": 7.5, "k_fft_cols_yinv": 7.5, "k_fftx_inv": 7.5,
                      "k_correct+k_finalize": 51.2}
 # the step-level model: NS+ACDI 256 B/pt (FP32 Poisson), 280 B/pt (FP64)

@@ -13,7 +13,7 @@ module mhit_gpu
 
   integer(c_int), parameter :: MHIT_OK = 0, MHIT_ERR_ARG = -1, MHIT_ERR_CUDA = -2, MHIT_ERR_NAN = -3
   integer(c_int), parameter :: MHIT_ERR_CFL = -4, MHIT_ERR_IO = -5, MHIT_ERR_STATE = -6
-  integer(c_int), parameter :: MHIT_POISSON_FP64 = 0, MHIT_POISSON_FP32 = 1
+  integer(c_int), parameter :: MHIT_POISSON_FP64 = 0, MHIT_POISSON_FP32 = 1, MHIT_POISSON_FP32_REFINED = 2
   integer(c_int), parameter :: MHIT_LAP_EXACT = 0, MHIT_LAP_MODIFIED = 1
   integer(c_int), parameter :: MHIT_INTERP_LINEAR1D = 0, MHIT_INTERP_TRILINEAR = 1
 
@@ -134,6 +134,40 @@ module mhit_gpu
       type(c_ptr), value :: ctx
       integer(c_int), value :: nsteps
       real(c_double), intent(out) :: ms
+    end function
+
+    ! ensemble of nbox independent boxes (params(1:nbox), any sizes) stepped together
+    integer(c_int) function mhit_ensemble_create(params, nbox, ens) bind(C, name="mhit_ensemble_create")
+      import :: c_int, c_ptr, mhit_params
+      type(mhit_params), intent(in) :: params(*)
+      integer(c_int), value :: nbox
+      type(c_ptr), intent(out) :: ens
+    end function
+
+    subroutine mhit_ensemble_destroy(ens) bind(C, name="mhit_ensemble_destroy")
+      import :: c_ptr
+      type(c_ptr), value :: ens
+    end subroutine
+
+    ! context of box b (0-based): upload, download, diagnostics and field files per box
+    integer(c_int) function mhit_ensemble_box(ens, b, ctx) bind(C, name="mhit_ensemble_box")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ens
+      integer(c_int), value :: b
+      type(c_ptr), intent(out) :: ctx
+    end function
+
+    integer(c_int) function mhit_ensemble_step(ens, nsteps) bind(C, name="mhit_ensemble_step")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ens
+      integer(c_int), value :: nsteps
+    end function
+
+    integer(c_int) function mhit_ensemble_autotune(ens, trials, nlanes) bind(C, name="mhit_ensemble_autotune")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ens
+      integer(c_int), value :: trials
+      integer(c_int), intent(out) :: nlanes
     end function
   end interface
 
