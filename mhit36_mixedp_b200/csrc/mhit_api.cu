@@ -62,6 +62,7 @@ struct mhit_ctx {
   void* P = nullptr;
   float* P2 = nullptr;    // refinement: residual, then the pressure correction (FP32)
   double* P64 = nullptr;  // refinement: corrected pressure (FP64)
+  double* Pw = nullptr;   // FP32 modes: the pressure widened to FP64 for a download (lazy)
   void* spec = nullptr;
   void *twx = nullptr, *twy = nullptr, *twz = nullptr;
   double *k2x = nullptr, *k2y = nullptr, *k2z = nullptr;
@@ -144,6 +145,12 @@ __global__ void k_apply_mean(double* u, double* v, double* w, size_t n, DevScala
     v[i] = v[i] - b;
     w[i] = w[i] - c;
   }
+}
+
+// FP32 pressure -> FP64 (exact) for a download
+__global__ void k_widen(const float* __restrict__ src, double* __restrict__ dst, size_t n) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    dst[i] = (double)src[i];
 }
 
 __global__ void k_clear_mean(DevScalars* sc) {
@@ -447,6 +454,7 @@ void mhit_destroy(mhit_ctx* c) {
   cudaFree(c->P);
   cudaFree(c->P2);
   cudaFree(c->P64);
+  cudaFree(c->Pw);
   cudaFree(c->spec);
   cudaFree(c->twx);
   cudaFree(c->twy);
@@ -715,40 +723,37 @@ int mhit_profile_step(mhit_ctx* c, double* ms, const char** names, int* nstages)
 int mhit_download_fields(mhit_ctx* c, double* u, double* v, double* w, double* p, double* phi) {
   int rc;
   if ((rc = check_ctx(c))) return rc;
-  if ((rc = fetch_scalars(c))) return rc;
+  if (phi && !c->prm.phiflag) return set_error(MHIT_ERR_STATE, "context was created with phiflag=0");
   const size_t n = c->n, fb = n * sizeof(double);
   double* outs[3] = {u, v, w};
   double* srcs[3] = {c->U[c->cur], c->V[c->cur], c->W[c->cur]};
+  if (u || v || w) {
+    // the lazily removed mean (multi/main.f90:977-981) is made explicit on the device: the
+    // stored value minus the mean, the same double every reader computes, so later steps are
+    // unchanged
+    k_apply_mean<<<148 * 4, 256, 0, c->st>>>(c->U[c->cur], c->V[c->cur], c->W[c->cur], n, c->sc);
+    MHIT_CUDA_TRY(cudaGetLastError());
+    k_clear_mean<<<1, 1, 0, c->st>>>(c->sc);
+    MHIT_CUDA_TRY(cudaGetLastError());
+  }
   for (int q = 0; q < 3; ++q) {
     if (!outs[q]) continue;
     MHIT_CUDA_TRY(cudaMemcpyAsync(outs[q], srcs[q], fb, cudaMemcpyDeviceToHost, c->st));
   }
-  if (phi) {
-    if (!c->prm.phiflag) return set_error(MHIT_ERR_STATE, "context was created with phiflag=0");
-    MHIT_CUDA_TRY(cudaMemcpyAsync(phi, c->PHI[c->cur], fb, cudaMemcpyDeviceToHost, c->st));
-  }
-  std::vector<float> pf;
-  if (p && c->P64) {
-    MHIT_CUDA_TRY(cudaMemcpyAsync(p, c->P64, fb, cudaMemcpyDeviceToHost, c->st));
-  } else if (p) {
-    if (tsize(c) == 4) {
-      pf.resize(n);
-      MHIT_CUDA_TRY(cudaMemcpyAsync(pf.data(), c->P, n * 4, cudaMemcpyDeviceToHost, c->st));
-    } else {
-      MHIT_CUDA_TRY(cudaMemcpyAsync(p, c->P, fb, cudaMemcpyDeviceToHost, c->st));
+  if (phi) MHIT_CUDA_TRY(cudaMemcpyAsync(phi, c->PHI[c->cur], fb, cudaMemcpyDeviceToHost, c->st));
+  if (p) {
+    const double* src = static_cast<const double*>(c->P);
+    if (c->P64) {
+      src = c->P64;
+    } else if (tsize(c) == 4) {
+      if (!c->Pw) MHIT_CUDA_TRY(cudaMalloc(&c->Pw, fb));
+      k_widen<<<148 * 4, 256, 0, c->st>>>(static_cast<const float*>(c->P), c->Pw, n);
+      MHIT_CUDA_TRY(cudaGetLastError());
+      src = c->Pw;
     }
+    MHIT_CUDA_TRY(cudaMemcpyAsync(p, src, fb, cudaMemcpyDeviceToHost, c->st));
   }
-  MHIT_CUDA_TRY(cudaStreamSynchronize(c->st));
-  // lazily removed mean (multi/main.f90:977-981)
-  for (int q = 0; q < 3; ++q) {
-    if (!outs[q]) continue;
-    const double m = c->sc_host->mean[q];
-    if (m != 0.0)
-      for (size_t i = 0; i < n; ++i) outs[q][i] = outs[q][i] - m;
-  }
-  if (p && !c->P64 && tsize(c) == 4)
-    for (size_t i = 0; i < n; ++i) p[i] = (double)pf[i];
-  return MHIT_OK;
+  return fetch_scalars(c);  // synchronises the stream: the copies are complete
 }
 
 int mhit_diagnostics(mhit_ctx* c, mhit_diag* d) {
