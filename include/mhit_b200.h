@@ -139,6 +139,18 @@ int mhit_diagnostics(mhit_ctx* ctx, mhit_diag* d);
 int mhit_write_field(mhit_ctx* ctx, const char* dir, int t, int fieldn);
 int mhit_read_field(mhit_ctx* ctx, const char* path, int fieldn);
 
+/* Exact-resume checkpoint (no reference counterpart: the reference restarts from the field
+ * files, multi/readwrite.f90:107-318, with an Euler step because rhs_o is not in them,
+ * multi/main.f90:440-441).  The file holds everything the next step reads: u, v, w as stored
+ * with the lazily removed mean, phi, rhs_o of u, v, w and phi, the pressure in the Poisson
+ * precision, the device scalars (mean, gumax of the previous projection), the step count and the
+ * tracer table; stepping a context that read it gives the same bits as never stopping.
+ * mhit_read_checkpoint needs a context created with the same nx, ny, nz, phiflag, partflag and
+ * Poisson mode (MHIT_ERR_ARG otherwise; MHIT_ERR_IO for a missing, short or foreign file).  A
+ * read that fails after the header leaves the context's fields undefined: upload or read again. */
+int mhit_write_checkpoint(mhit_ctx* ctx, const char* path);
+int mhit_read_checkpoint(mhit_ctx* ctx, const char* path);
+
 /* Measurement helpers (no reference counterpart; the reference times with cpu_time,
  * multi/main.f90:453,463,1009-1010).  mhit_time_steps runs nsteps on the context stream between
  * two CUDA events and returns the elapsed milliseconds.  mhit_profile_step runs one step with

@@ -68,6 +68,8 @@ SIGNATURES = {
     "mhit_diagnostics": (_c.c_int, [_c.c_void_p, _P(MhitDiag)]),
     "mhit_write_field": (_c.c_int, [_c.c_void_p, _c.c_char_p, _c.c_int, _c.c_int]),
     "mhit_read_field": (_c.c_int, [_c.c_void_p, _c.c_char_p, _c.c_int]),
+    "mhit_write_checkpoint": (_c.c_int, [_c.c_void_p, _c.c_char_p]),
+    "mhit_read_checkpoint": (_c.c_int, [_c.c_void_p, _c.c_char_p]),
     "mhit_time_steps": (_c.c_int, [_c.c_void_p, _c.c_int, _dp]),
     "mhit_profile_step": (_c.c_int, [_c.c_void_p, _dp, _P(_c.c_char_p), _P(_c.c_int)]),
     "mhit_ensemble_create": (_c.c_int, [_P(MhitParams), _c.c_int, _P(_c.c_void_p)]),

@@ -236,6 +236,20 @@ class Solver:
         """``readfield(fieldn)`` / ``readfield_restart`` (multi/readwrite.f90:107-318)."""
         _check(self._lib.mhit_read_field(self._ctx, path.encode(), int(fieldn)))
 
+    def write_checkpoint(self, path: str):
+        """Everything the next step reads (fields, AB2 history, device scalars, step count,
+        tracers): a run resumed with ``read_checkpoint`` continues bit for bit."""
+        _check(self._lib.mhit_write_checkpoint(self._ctx, path.encode()))
+
+    def read_checkpoint(self, path: str):
+        """Restore a ``write_checkpoint`` file into a context of the same size and mode."""
+        _check(self._lib.mhit_read_checkpoint(self._ctx, path.encode()))
+        if self.params.partflag:
+            import struct
+            with open(path, "rb") as f:
+                hdr = f.read(48)
+            self._np = struct.unpack_from("<i", hdr, 8 + 6 * 4)[0]
+
     # -------------------------------------------------------------- measurement
     def time_steps(self, nsteps: int) -> float:
         ms = ctypes.c_double()

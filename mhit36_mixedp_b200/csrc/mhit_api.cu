@@ -12,6 +12,7 @@
 // Steps after the first are replayed from two captured CUDA graphs (one per parity of the
 // velocity ping-pong buffers), so a step costs one graph launch on the host.
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <algorithm>
@@ -76,6 +77,7 @@ struct mhit_ctx {
   int cur = 0;
   long long nstep = 0;
   bool graph_built = false;
+  unsigned gen = 0;  // bumped whenever arguments baked into captured graphs change
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
   cudaEvent_t ev[2 * ST_COUNT] = {};
   int zchunk_phase = 0, zchunk_mom = 0;  // z planes per block of k_phase / k_mom (0: default)
@@ -641,18 +643,19 @@ int mhit_upload_particles(mhit_ctx* c, const double* part, int npart) {
     c->part = nullptr;
   }
   c->np = npart;
-  if (npart == 0) return MHIT_OK;
-  const size_t bytes = (size_t)npart * 12 * sizeof(double);
-  MHIT_CUDA_TRY(cudaMalloc(&c->part, bytes));
-  MHIT_CUDA_TRY(cudaMemcpyAsync(c->part, part, bytes, cudaMemcpyHostToDevice, c->st));
-  MHIT_CUDA_TRY(cudaStreamSynchronize(c->st));
-  // the tracer kernel's pointer is baked into captured graphs
+  c->gen++;
+  // the tracer kernel's pointer (and whether it runs at all) is baked into captured graphs
   for (int i = 0; i < 2; ++i)
     if (c->gexec[i]) {
       cudaGraphExecDestroy(c->gexec[i]);
       c->gexec[i] = nullptr;
     }
   c->graph_built = false;
+  if (npart == 0) return MHIT_OK;
+  const size_t bytes = (size_t)npart * 12 * sizeof(double);
+  MHIT_CUDA_TRY(cudaMalloc(&c->part, bytes));
+  MHIT_CUDA_TRY(cudaMemcpyAsync(c->part, part, bytes, cudaMemcpyHostToDevice, c->st));
+  MHIT_CUDA_TRY(cudaStreamSynchronize(c->st));
   return MHIT_OK;
 }
 
@@ -845,6 +848,117 @@ int mhit_read_field(mhit_ctx* c, const char* path, int fieldn) {
   return reset_history(c);
 }
 
+// ------------------------------------------------------------------ checkpoint
+// File layout (little-endian): CkptHeader, DevScalars, then the arrays in the order of
+// ckpt_arrays(), each raw and complete, then the tracer table (np x 12 float64).
+namespace {
+struct CkptHeader {
+  char magic[8];  // "MHITCKP1"
+  int32_t nx, ny, nz, phiflag, partflag, poisson, np, pbytes;
+  int64_t nstep;
+};
+constexpr char kCkptMagic[8] = {'M', 'H', 'I', 'T', 'C', 'K', 'P', '1'};
+
+struct CkptArray {
+  void* dev;
+  size_t bytes;
+};
+
+std::vector<CkptArray> ckpt_arrays(mhit_ctx* c) {
+  const size_t fb = c->n * sizeof(double);
+  const int k = c->cur;
+  std::vector<CkptArray> a = {{c->U[k], fb}, {c->V[k], fb}, {c->W[k], fb}, {c->RU, fb}, {c->RV, fb}, {c->RW, fb}};
+  if (c->prm.phiflag) {
+    a.push_back({c->PHI[k], fb});
+    a.push_back({c->RPHI, fb});
+  }
+  a.push_back({c->P, c->n * tsize(c)});
+  if (c->P64) a.push_back({c->P64, fb});
+  return a;
+}
+
+struct FileCloser {
+  FILE* f;
+  ~FileCloser() {
+    if (f) fclose(f);
+  }
+};
+}  // namespace
+
+int mhit_write_checkpoint(mhit_ctx* c, const char* path) {
+  int rc;
+  if ((rc = check_ctx(c))) return rc;
+  if (!path) return set_error(MHIT_ERR_ARG, "null path");
+  if ((rc = fetch_scalars(c))) return rc;
+  FileCloser fc{fopen(path, "wb")};
+  if (!fc.f) return set_error(MHIT_ERR_IO, std::string("cannot create ") + path);
+  CkptHeader h;
+  memcpy(h.magic, kCkptMagic, 8);
+  h.nx = c->prm.nx;
+  h.ny = c->prm.ny;
+  h.nz = c->prm.nz;
+  h.phiflag = c->prm.phiflag;
+  h.partflag = c->prm.partflag;
+  h.poisson = c->prm.poisson;
+  h.np = c->np;
+  h.pbytes = (int32_t)tsize(c);
+  h.nstep = c->nstep;
+  bool ok = fwrite(&h, sizeof(h), 1, fc.f) == 1 && fwrite(c->sc_host, sizeof(DevScalars), 1, fc.f) == 1;
+  std::vector<unsigned char> buf;
+  for (const CkptArray& a : ckpt_arrays(c)) {
+    buf.resize(a.bytes);
+    MHIT_CUDA_TRY(cudaMemcpy(buf.data(), a.dev, a.bytes, cudaMemcpyDeviceToHost));
+    ok = ok && fwrite(buf.data(), 1, a.bytes, fc.f) == a.bytes;
+  }
+  if (c->np > 0) {
+    const size_t pb = (size_t)c->np * 12 * sizeof(double);
+    buf.resize(pb);
+    MHIT_CUDA_TRY(cudaMemcpy(buf.data(), c->part, pb, cudaMemcpyDeviceToHost));
+    ok = ok && fwrite(buf.data(), 1, pb, fc.f) == pb;
+  }
+  const int cl = fclose(fc.f);
+  fc.f = nullptr;
+  if (!ok || cl != 0) return set_error(MHIT_ERR_IO, std::string("short write to ") + path);
+  return MHIT_OK;
+}
+
+int mhit_read_checkpoint(mhit_ctx* c, const char* path) {
+  int rc;
+  if ((rc = check_ctx(c))) return rc;
+  if (!path) return set_error(MHIT_ERR_ARG, "null path");
+  FileCloser fc{fopen(path, "rb")};
+  if (!fc.f) return set_error(MHIT_ERR_IO, std::string("cannot open ") + path);
+  CkptHeader h;
+  if (fread(&h, sizeof(h), 1, fc.f) != 1 || memcmp(h.magic, kCkptMagic, 8) != 0)
+    return set_error(MHIT_ERR_IO, std::string("not a checkpoint file: ") + path);
+  if (h.nx != c->prm.nx || h.ny != c->prm.ny || h.nz != c->prm.nz || h.phiflag != c->prm.phiflag ||
+      h.partflag != c->prm.partflag || h.poisson != c->prm.poisson || h.pbytes != (int32_t)tsize(c) ||
+      h.np < 0 || h.nstep < 0)
+    return set_error(MHIT_ERR_ARG, "checkpoint was written by a context of another size or mode");
+  DevScalars s;
+  if (fread(&s, sizeof(s), 1, fc.f) != 1) return set_error(MHIT_ERR_IO, std::string("short read from ") + path);
+  MHIT_CUDA_TRY(cudaStreamSynchronize(c->st));
+  c->cur = 0;
+  std::vector<unsigned char> buf;
+  for (const CkptArray& a : ckpt_arrays(c)) {
+    buf.resize(a.bytes);
+    if (fread(buf.data(), 1, a.bytes, fc.f) != a.bytes)
+      return set_error(MHIT_ERR_IO, std::string("short read from ") + path);
+    MHIT_CUDA_TRY(cudaMemcpy(a.dev, buf.data(), a.bytes, cudaMemcpyHostToDevice));
+  }
+  if (c->prm.partflag) {
+    const size_t pb = (size_t)h.np * 12 * sizeof(double);
+    buf.resize(pb);
+    if (fread(buf.data(), 1, pb, fc.f) != pb) return set_error(MHIT_ERR_IO, std::string("short read from ") + path);
+    rc = mhit_upload_particles(c, h.np ? reinterpret_cast<const double*>(buf.data()) : nullptr, h.np);
+    if (rc) return rc;
+  }
+  *c->sc_host = s;
+  MHIT_CUDA_TRY(cudaMemcpy(c->sc, c->sc_host, sizeof(DevScalars), cudaMemcpyHostToDevice));
+  c->nstep = h.nstep;
+  return MHIT_OK;
+}
+
 // ------------------------------------------------------------------ test hooks
 int mhit_debug_run_stage(mhit_ctx* c, int stage) {
   int rc;
@@ -926,6 +1040,7 @@ struct mhit_ensemble {
   std::vector<cudaEvent_t> join;
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
   bool built = false;
+  std::vector<unsigned> gen;  // the boxes' graph generations the ensemble graphs were built from
   cudaEvent_t ev[2] = {nullptr, nullptr};
 };
 
@@ -987,6 +1102,8 @@ static int ens_build(mhit_ensemble* e) {
     if (err != cudaSuccess) return set_cuda_error(err, "cudaGraphInstantiate (ensemble)", __FILE__, __LINE__);
   }
   e->built = true;
+  e->gen.clear();
+  for (mhit_ctx* c : e->box) e->gen.push_back(c->gen);
   return MHIT_OK;
 }
 
@@ -1001,6 +1118,9 @@ static int ens_enqueue_steps(mhit_ensemble* e, int nsteps) {
     if (n0 == 0) {
       rc = ens_enqueue(e, 1.0, 0.0, cur);  // Euler first step, multi/main.f90:440-441
     } else {
+      // a box whose captured arguments changed (tracers uploaded) invalidates the ensemble graphs
+      for (size_t b = 0; e->built && b < e->box.size(); ++b)
+        if (e->gen.size() != e->box.size() || e->gen[b] != e->box[b]->gen) ens_drop_graphs(e);
       if (!e->built && (rc = ens_build(e))) return rc;
       MHIT_CUDA_TRY(cudaGraphLaunch(e->gexec[cur], e->st));
       rc = MHIT_OK;

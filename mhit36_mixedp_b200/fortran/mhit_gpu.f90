@@ -129,6 +129,19 @@ module mhit_gpu
       integer(c_int), value :: fieldn
     end function
 
+    ! exact-resume checkpoint: fields, rhs_o history, device scalars, step count, tracers
+    integer(c_int) function mhit_write_checkpoint(ctx, path) bind(C, name="mhit_write_checkpoint")
+      import :: c_int, c_ptr, c_char
+      type(c_ptr), value :: ctx
+      character(kind=c_char), dimension(*), intent(in) :: path
+    end function
+
+    integer(c_int) function mhit_read_checkpoint(ctx, path) bind(C, name="mhit_read_checkpoint")
+      import :: c_int, c_ptr, c_char
+      type(c_ptr), value :: ctx
+      character(kind=c_char), dimension(*), intent(in) :: path
+    end function
+
     integer(c_int) function mhit_time_steps(ctx, nsteps, ms) bind(C, name="mhit_time_steps")
       import :: c_int, c_ptr, c_double
       type(c_ptr), value :: ctx

@@ -69,3 +69,34 @@ def test_ensemble_requires_boxes_in_step(gpu):
         ens.boxes[0].step(1)
         with pytest.raises(MhitStateError):
             ens.step(1)
+
+
+def test_ensemble_follows_a_tracer_reupload(gpu):
+    """Uploading a new tracer table to a box after the ensemble graphs were captured (they bake in
+    the tracer kernel and its table) must rebuild them: the box then matches a standalone box that
+    did the same."""
+    specs = [(16, 200), (32, 300)]
+    prms = [Params(nx=n, dt=5e-4, mu=0.005, partflag=1) for n, _ in specs]
+    fields = [synth.solenoidal_velocity(n, 10 + b) for b, (n, _) in enumerate(specs)]
+    first = [synth.uniform_particles(npart, 20 + b) for b, (_, npart) in enumerate(specs)]
+    second = synth.uniform_particles(150, 30)
+    with Ensemble(prms) as ens:
+        for box, (u, v, w), part in zip(ens.boxes, fields, first):
+            box.upload(u, v, w)
+            box.upload_particles(part)
+        ens.step(4)                       # Euler + graph-replayed steps
+        ens.boxes[0].upload_particles(second)
+        ens.step(3)
+        got = ens.boxes[0].download()
+        got_part = ens.boxes[0].download_particles()
+    with Solver(prms[0]) as s:
+        s.upload(*fields[0])
+        s.upload_particles(first[0])
+        s.step(4)
+        s.upload_particles(second)
+        s.step(3)
+        ref = s.download()
+        ref_part = s.download_particles()
+    for k in ref:
+        np.testing.assert_array_equal(got[k], ref[k])
+    np.testing.assert_array_equal(got_part, ref_part)
