@@ -151,6 +151,14 @@ def run_ours(args, rank, world, dev):
             s.step(0)  # flag check of the timed steps
             prof = [s.profile_step() for _ in range(3)]
             dg = s.diagnostics()
+            if mode == "fp32":
+                # droplet labelling of the current state (post/unionfind_periodic): host call,
+                # wall clock including its host<->device copies of the per-drop sums
+                s.label_drops(0.5, 6)
+                t0 = time.perf_counter()
+                drops = s.label_drops(0.5, 6)
+                res["drops"] = {"ms_per_call": (time.perf_counter() - t0) * 1e3, "ndrops": len(drops["cells"]),
+                                "connectivity": 6, "cells_in_drops": int(drops["cells"].sum())}
         stages = {k: statistics.mean(p[k] for p in prof) for k in prof[0]}
         res[mode] = {"ms": ms / args.steps, "stages": stages, "diag": dg, "clocks": clocks}
     # the discrete-Laplacian solve, where divergence after projection is round-off: FP64, plain
@@ -354,7 +362,7 @@ def main():
             "step_roofline_frac": step_roof, "stages_ms": {m: res[m]["stages"] for m in ("fp32", "fp64")},
             "roofline": roof, "cpu_baseline": cb, "e2e": e2e,
             "gpu_launches": 9 * args.steps, "clocks": clocks,
-            "modified_laplacian": res["modified"],
+            "modified_laplacian": res["modified"], "drop_labelling": res.get("drops"),
         }
         print(json.dumps(line), flush=True)
     if dist:

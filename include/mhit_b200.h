@@ -151,6 +151,22 @@ int mhit_read_field(mhit_ctx* ctx, const char* path, int fieldn);
 int mhit_write_checkpoint(mhit_ctx* ctx, const char* path);
 int mhit_read_checkpoint(mhit_ctx* ctx, const char* path);
 
+/* Droplet labelling (post/unionfind_periodic/main.f90): connected components of
+ * phi >= thresh (the reference uses 0.5) with periodic boundaries, connectivity 6 (faces) or 26
+ * (faces, edges, corners), and per drop the cell count, volume = cells dx^3, the centre as the
+ * circular mean of the cell centres per axis in [0, L) and the mean of the stored u, v, w over
+ * its cells (:276-336, :425-436).  Drops are numbered by their smallest cell index (k, j, i).
+ * Fills min(maxdrops, total) entries of drops and sets *ndrops = total; labels (may be NULL)
+ * receives the label field (0 background, 1..total), x fastest.  Needs phiflag = 1. */
+typedef struct {
+  long long cells;
+  double volume;
+  double x, y, z;
+  double u, v, w;
+} mhit_drop;
+int mhit_label_drops(mhit_ctx* ctx, double thresh, int connectivity, mhit_drop* drops, int maxdrops, int* ndrops,
+                     int* labels);
+
 /* Measurement helpers (no reference counterpart; the reference times with cpu_time,
  * multi/main.f90:453,463,1009-1010).  mhit_time_steps runs nsteps on the context stream between
  * two CUDA events and returns the elapsed milliseconds.  mhit_profile_step runs one step with

@@ -52,6 +52,11 @@ class MhitDiag(_c.Structure):
     ]
 
 
+class MhitDrop(_c.Structure):
+    _fields_ = [("cells", _c.c_longlong), ("volume", _c.c_double), ("x", _c.c_double), ("y", _c.c_double),
+                ("z", _c.c_double), ("u", _c.c_double), ("v", _c.c_double), ("w", _c.c_double)]
+
+
 _dp = _P(_c.c_double)
 SIGNATURES = {
     "mhit_abi_version": (_c.c_int, []),
@@ -70,6 +75,8 @@ SIGNATURES = {
     "mhit_read_field": (_c.c_int, [_c.c_void_p, _c.c_char_p, _c.c_int]),
     "mhit_write_checkpoint": (_c.c_int, [_c.c_void_p, _c.c_char_p]),
     "mhit_read_checkpoint": (_c.c_int, [_c.c_void_p, _c.c_char_p]),
+    "mhit_label_drops": (_c.c_int, [_c.c_void_p, _c.c_double, _c.c_int, _P(MhitDrop), _c.c_int, _P(_c.c_int),
+                                    _c.c_void_p]),
     "mhit_time_steps": (_c.c_int, [_c.c_void_p, _c.c_int, _dp]),
     "mhit_profile_step": (_c.c_int, [_c.c_void_p, _dp, _P(_c.c_char_p), _P(_c.c_int)]),
     "mhit_ensemble_create": (_c.c_int, [_P(MhitParams), _c.c_int, _P(_c.c_void_p)]),

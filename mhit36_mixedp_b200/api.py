@@ -17,7 +17,7 @@ import dataclasses
 import numpy as np
 
 from . import _lib
-from ._lib import MhitDiag, MhitParams, MhitRun
+from ._lib import MhitDiag, MhitDrop, MhitParams, MhitRun
 
 FIELD_U, FIELD_V, FIELD_W, FIELD_P, FIELD_PHI = 1, 2, 3, 4, 5
 
@@ -249,6 +249,30 @@ class Solver:
             with open(path, "rb") as f:
                 hdr = f.read(48)
             self._np = struct.unpack_from("<i", hdr, 8 + 6 * 4)[0]
+
+    # -------------------------------------------------------------- droplet labelling
+    def label_drops(self, thresh: float = 0.5, connectivity: int = 6, labels: bool = False, capacity: int = 4096):
+        """Connected components of phi >= thresh with periodic boundaries and their statistics
+        (post/unionfind_periodic/main.f90).  Returns a dict of arrays ordered by each drop's
+        smallest cell index: cells, volume, x, y, z (circular-mean centre), u, v, w (mean
+        velocity); with labels=True also the (nz, ny, nx) int32 label field (0 background)."""
+        cap = max(int(capacity), 1)
+        while True:
+            arr = (MhitDrop * cap)()
+            nd = ctypes.c_int()
+            lab = np.empty(self.params.shape, dtype=np.int32) if labels else None
+            lp = lab.ctypes.data_as(ctypes.c_void_p) if labels else None
+            _check(self._lib.mhit_label_drops(self._ctx, float(thresh), int(connectivity), arr, cap,
+                                              ctypes.byref(nd), lp))
+            if nd.value <= cap:
+                break
+            cap = nd.value
+        n = nd.value
+        out = {f: np.array([getattr(arr[i], f) for i in range(n)], dtype=np.int64 if f == "cells" else np.float64)
+               for f, _ in MhitDrop._fields_}
+        if labels:
+            out["labels"] = lab
+        return out
 
     # -------------------------------------------------------------- measurement
     def time_steps(self, nsteps: int) -> float:

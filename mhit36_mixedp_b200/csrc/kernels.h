@@ -105,4 +105,25 @@ cudaError_t launch_tracer(const TracerArgs& a, cudaStream_t st);
 // ---------------------------------------------------------------- utilities
 cudaError_t launch_fill(double* p, size_t n, double v, cudaStream_t st);
 
+// ---------------------------------------------------------------- droplet labelling
+struct LabelArgs {
+  int nx, ny, nz;
+  const double* phi;
+  double thresh;
+  int connectivity;             // 6 or 26
+  int* lab;                     // n ints of scratch: parents, then the drop encoding
+  int* counts;                  // roots per chunk of cells, then the chunks' first drop numbers
+  int* err;                     // set when a bounded union-find loop ran out
+  const double *u, *v, *w;      // stored velocity (lazy mean in sc)
+  const DevScalars* sc;
+  const double* trig;           // sin, cos of the cell centres per axis (x, y, z)
+  double* acc;                  // [ndrops][9]
+  unsigned long long* cells;    // [ndrops]
+  int* out;                     // label field (0 background, 1.. drop) or nullptr
+};
+int label_chunks(int n);
+cudaError_t launch_label_components(const LabelArgs& a, cudaStream_t st);  // init, merge, flatten, count
+cudaError_t launch_label_number(const LabelArgs& a, cudaStream_t st);      // counts must hold offsets
+cudaError_t launch_label_stats(const LabelArgs& a, cudaStream_t st);
+
 }  // namespace mhit

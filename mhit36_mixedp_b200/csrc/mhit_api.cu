@@ -959,6 +959,125 @@ int mhit_read_checkpoint(mhit_ctx* c, const char* path) {
   return MHIT_OK;
 }
 
+// ------------------------------------------------------------------ droplet labelling
+namespace {
+struct DevBuf {  // temporary device allocation freed on every return path
+  void* p = nullptr;
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+};
+}  // namespace
+
+int mhit_label_drops(mhit_ctx* c, double thresh, int connectivity, mhit_drop* drops, int maxdrops, int* ndrops,
+                     int* labels) {
+  int rc;
+  if ((rc = check_ctx(c))) return rc;
+  if (!c->prm.phiflag) return set_error(MHIT_ERR_STATE, "context was created with phiflag=0");
+  if (connectivity != 6 && connectivity != 26) return set_error(MHIT_ERR_ARG, "connectivity must be 6 or 26");
+  if (!ndrops || maxdrops < 0 || (maxdrops > 0 && !drops)) return set_error(MHIT_ERR_ARG, "bad drop buffer");
+  const int nx = c->prm.nx, ny = c->prm.ny, nz = c->prm.nz;
+  const int n = (int)c->n;
+  const int nch = label_chunks(n);
+  // scratch: the spectrum buffer (at least 4 bytes per cell, unused between steps) holds the
+  // parents; the chunk counts, the error flag and the trig tables share one allocation
+  const size_t trig_n = 2 * (size_t)(nx + ny + nz);
+  DevBuf small, accb, outb;
+  const size_t small_bytes = sizeof(double) * trig_n + sizeof(int) * (nch + 1);
+  MHIT_CUDA_TRY(cudaMalloc(&small.p, small_bytes));
+  double* trig = static_cast<double*>(small.p);
+  int* counts = reinterpret_cast<int*>(trig + trig_n);
+  int* err = counts + nch;
+  // cell centres x_i = dx/2 + (i-1) dx accumulated as post/unionfind_periodic/main.f90:294-298,
+  // sin/cos(2 pi x_i / L) with L the axis period (2 pi for the cubic box)
+  const double pi = 4.0 * atan(1.0), dx = 2.0 * pi / nx;
+  std::vector<double> th(trig_n);
+  {
+    size_t o = 0;
+    for (int axis = 0; axis < 3; ++axis) {
+      const int na = axis == 0 ? nx : (axis == 1 ? ny : nz);
+      const double L = na * dx;
+      double x = dx / 2.0;
+      for (int i = 0; i < na; ++i) {
+        if (i > 0) x = x + dx;
+        th[o + i] = sin(2.0 * pi * x / L);
+        th[o + na + i] = cos(2.0 * pi * x / L);
+      }
+      o += 2 * (size_t)na;
+    }
+  }
+  MHIT_CUDA_TRY(cudaMemcpyAsync(trig, th.data(), sizeof(double) * trig_n, cudaMemcpyHostToDevice, c->st));
+  MHIT_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int), c->st));
+  LabelArgs a;
+  a.nx = nx;
+  a.ny = ny;
+  a.nz = nz;
+  a.phi = c->PHI[c->cur];
+  a.thresh = thresh;
+  a.connectivity = connectivity;
+  a.lab = static_cast<int*>(c->spec);
+  a.counts = counts;
+  a.err = err;
+  a.u = c->U[c->cur];
+  a.v = c->V[c->cur];
+  a.w = c->W[c->cur];
+  a.sc = c->sc;
+  a.trig = trig;
+  a.acc = nullptr;
+  a.cells = nullptr;
+  a.out = nullptr;
+  MHIT_CUDA_TRY(launch_label_components(a, c->st));
+  std::vector<int> cnt(nch + 1);
+  MHIT_CUDA_TRY(cudaMemcpyAsync(cnt.data(), counts, sizeof(int) * (nch + 1), cudaMemcpyDeviceToHost, c->st));
+  MHIT_CUDA_TRY(cudaStreamSynchronize(c->st));
+  if (cnt[nch]) return set_error(MHIT_ERR_STATE, "droplet labelling: union-find bound exceeded");
+  int total = 0;
+  for (int b = 0; b < nch; ++b) {  // exclusive prefix sum: first drop number of each chunk
+    const int k = cnt[b];
+    cnt[b] = total;
+    total += k;
+  }
+  MHIT_CUDA_TRY(cudaMemcpyAsync(counts, cnt.data(), sizeof(int) * nch, cudaMemcpyHostToDevice, c->st));
+  MHIT_CUDA_TRY(launch_label_number(a, c->st));
+  const size_t nd = (size_t)std::max(total, 1);
+  MHIT_CUDA_TRY(cudaMalloc(&accb.p, nd * (9 * sizeof(double) + sizeof(unsigned long long))));
+  a.acc = static_cast<double*>(accb.p);
+  a.cells = reinterpret_cast<unsigned long long*>(a.acc + nd * 9);
+  MHIT_CUDA_TRY(cudaMemsetAsync(accb.p, 0, nd * (9 * sizeof(double) + sizeof(unsigned long long)), c->st));
+  if (labels) {
+    MHIT_CUDA_TRY(cudaMalloc(&outb.p, sizeof(int) * c->n));
+    a.out = static_cast<int*>(outb.p);
+  }
+  MHIT_CUDA_TRY(launch_label_stats(a, c->st));
+  std::vector<double> acc(nd * 9);
+  std::vector<unsigned long long> cells(nd);
+  MHIT_CUDA_TRY(cudaMemcpyAsync(acc.data(), a.acc, sizeof(double) * nd * 9, cudaMemcpyDeviceToHost, c->st));
+  MHIT_CUDA_TRY(cudaMemcpyAsync(cells.data(), a.cells, sizeof(unsigned long long) * nd, cudaMemcpyDeviceToHost, c->st));
+  if (labels) MHIT_CUDA_TRY(cudaMemcpyAsync(labels, a.out, sizeof(int) * c->n, cudaMemcpyDeviceToHost, c->st));
+  MHIT_CUDA_TRY(cudaStreamSynchronize(c->st));
+  // post/unionfind_periodic/main.f90:319-336 and the volume of :436
+  const double per[3] = {nx * dx, ny * dx, nz * dx};
+  for (int d = 0; d < total && d < maxdrops; ++d) {
+    const double* s = &acc[(size_t)d * 9];
+    mhit_drop& o = drops[d];
+    o.cells = (long long)cells[d];
+    o.volume = (double)cells[d] * dx * dx * dx;
+    double ctr[3];
+    for (int q = 0; q < 3; ++q) {
+      ctr[q] = per[q] * atan2(s[2 * q], s[2 * q + 1]) / (2.0 * pi);
+      if (ctr[q] < 0.0) ctr[q] = ctr[q] + per[q];
+    }
+    o.x = ctr[0];
+    o.y = ctr[1];
+    o.z = ctr[2];
+    o.u = s[6] / (double)cells[d];
+    o.v = s[7] / (double)cells[d];
+    o.w = s[8] / (double)cells[d];
+  }
+  *ndrops = total;
+  return MHIT_OK;
+}
+
 // ------------------------------------------------------------------ test hooks
 int mhit_debug_run_stage(mhit_ctx* c, int stage) {
   int rc;

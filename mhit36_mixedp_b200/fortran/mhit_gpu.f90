@@ -31,6 +31,14 @@ module mhit_gpu
     integer(c_int) :: restart, tstart, tfin, dump, inflow, inphi, inpart
   end type mhit_run
 
+  ! one drop of mhit_label_drops (post/unionfind_periodic/main.f90:425-436)
+  type, bind(C) :: mhit_drop
+    integer(c_long_long) :: cells
+    real(c_double) :: volume
+    real(c_double) :: x, y, z
+    real(c_double) :: u, v, w
+  end type mhit_drop
+
   type, bind(C) :: mhit_diag
     integer(c_long_long) :: nstep
     real(c_double) :: gumax, cfl
@@ -140,6 +148,19 @@ module mhit_gpu
       import :: c_int, c_ptr, c_char
       type(c_ptr), value :: ctx
       character(kind=c_char), dimension(*), intent(in) :: path
+    end function
+
+    ! connected components of phi >= thresh (connectivity 6 or 26), statistics per drop;
+    ! labels may be c_null_ptr or c_loc of an integer(c_int) array (nx, ny, nz)
+    integer(c_int) function mhit_label_drops(ctx, thresh, connectivity, drops, maxdrops, ndrops, labels) &
+        bind(C, name="mhit_label_drops")
+      import :: c_int, c_ptr, c_double, mhit_drop
+      type(c_ptr), value :: ctx
+      real(c_double), value :: thresh
+      integer(c_int), value :: connectivity, maxdrops
+      type(mhit_drop), intent(out) :: drops(*)
+      integer(c_int), intent(out) :: ndrops
+      type(c_ptr), value :: labels
     end function
 
     integer(c_int) function mhit_time_steps(ctx, nsteps, ms) bind(C, name="mhit_time_steps")

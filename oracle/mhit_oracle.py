@@ -560,3 +560,80 @@ def single_drop(p: Params):
     pos = ((X - lx / 2) ** 2.0)[None, None, :] + ((Y - lx / 2) ** 2.0)[None, :, None]
     pos = pos + ((Z - lx / 2) ** 2.0)[:, None, None]
     return 0.5 * (1.0 - np.tanh((np.sqrt(pos) - p.radius) / 2 / p.eps))
+
+
+# ---------------------------------------------------------------------- droplet labelling
+def neighbour_offsets(connectivity):
+    """(dz, dy, dx) of the 6 face or 26 face/edge/corner neighbours
+    (post/unionfind_periodic/main.f90:33-48)."""
+    if connectivity == 6:
+        return [(0, 0, 1), (0, 0, -1), (0, 1, 0), (0, -1, 0), (1, 0, 0), (-1, 0, 0)]
+    if connectivity == 26:
+        return [(a, b, c) for a in (-1, 0, 1) for b in (-1, 0, 1) for c in (-1, 0, 1) if (a, b, c) != (0, 0, 0)]
+    raise ValueError("connectivity must be 6 or 26")
+
+
+def label_components(phi, thresh=0.5, connectivity=6):
+    """Periodic connected components of phi >= thresh by min-label propagation, the algorithm of
+    post/unionfind_periodic/main.f90:137-258: every masked cell starts with its own index and
+    takes the minimum over itself and its masked neighbours (periodic wrap) until nothing changes.
+    Arrays are (nz, ny, nx), x fastest; the starting index is the flat cell index (the reference's
+    includes its halo planes), so each component ends labelled with its smallest cell index.
+    Returns the label array with -1 for background."""
+    n = phi.size
+    mask = phi >= thresh
+    big = np.int64(n)
+    lab = np.where(mask, np.arange(n, dtype=np.int64).reshape(phi.shape), big)
+    offs = neighbour_offsets(connectivity)
+    while True:
+        new = lab
+        for dz, dy, dx in offs:
+            # value at (k+dz, j+dy, i+dx), periodic
+            new = np.minimum(new, np.roll(lab, shift=(-dz, -dy, -dx), axis=(0, 1, 2)))
+        new = np.where(mask, new, big)
+        if np.array_equal(new, lab):
+            break
+        lab = new
+    return np.where(mask, lab, -1)
+
+
+def drop_statistics(lab, u, v, w, lx=2 * math.pi):
+    """Per component (ordered by label): cells, volume = cells dx^3, centre = circular mean of the
+    cell centres per axis, mean u, v, w (post/unionfind_periodic/main.f90:276-336, :425-436).
+    Cell centres accumulate x(1) = dx/2, x(i) = x(i-1) + dx as the reference does (:294-298);
+    sums are in float64 (the reference accumulates the velocities in default REAL)."""
+    nz, ny, nx = lab.shape
+    pi = 4.0 * math.atan(1.0)
+    dx = lx / nx
+    sel = lab >= 0
+    roots = np.unique(lab[sel])
+    ids = np.searchsorted(roots, lab[sel])
+    nd = len(roots)
+    kk, jj, ii = np.nonzero(sel)
+    cells = np.bincount(ids, minlength=nd)
+    out = {"label": roots, "cells": cells, "volume": cells.astype(np.float64) * dx * dx * dx}
+    for name, idx, na in (("x", ii, nx), ("y", jj, ny), ("z", kk, nz)):
+        per = na * dx
+        xs = np.empty(na)
+        x = dx / 2.0
+        for i in range(na):
+            if i > 0:
+                x = x + dx
+            xs[i] = x
+        s = np.bincount(ids, weights=np.sin(2.0 * pi * xs / per)[idx], minlength=nd)
+        c = np.bincount(ids, weights=np.cos(2.0 * pi * xs / per)[idx], minlength=nd)
+        ctr = per * np.arctan2(s, c) / (2.0 * pi)
+        out[name] = np.where(ctr < 0.0, ctr + per, ctr)
+    for name, f in (("u", u), ("v", v), ("w", w)):
+        out[name] = np.bincount(ids, weights=f[sel], minlength=nd) / cells
+    return out
+
+
+def reference_test_sphere(nx):
+    """The synthetic sphere of post/unionfind_periodic/main.f90:124-129 (readf = .false.):
+    phi = 1 at 1-based (i, j, k) with (i-cx)^2+(j-cy)^2+(k-cz)^2 <= r2, cx = nx/4, cy = nx/3,
+    cz = nx/2, r2 = (nx/10)^2 in integer arithmetic; phi = 0 elsewhere.  (nz, ny, nx) array."""
+    cx, cy, cz, r2 = nx // 4, nx // 3, nx // 2, (nx // 10) ** 2
+    i = np.arange(1, nx + 1)
+    d2 = (i[None, None, :] - cx) ** 2 + (i[None, :, None] - cy) ** 2 + (i[:, None, None] - cz) ** 2
+    return np.where(d2 <= r2, 1.0, 0.0), (cx, cy, cz, r2)
