@@ -116,3 +116,25 @@ def uniform_particles(npart, seed):
 def sigma_from_weber(rho, u_rms, radius, weber):
     """sigma = rho u_rms^2 (2R) / We (the reference has no Weber number; this is the choice)."""
     return rho * u_rms * u_rms * (2.0 * radius) / weber
+
+
+def abc_velocity(nx, modes=((1, 1.0), (3, 0.3)), ny=None, nz=None):
+    """Arnold-Beltrami-Childress flow summed over wavenumbers k with amplitude a:
+    u = a (sin kz + cos ky), v = a (sin kx + cos kz), w = a (sin ky + cos kx) at the staggered face
+    positions.  Each component is independent of its own coordinate, so the discrete divergence is
+    exactly zero; cheap to build at any size (outer sums of 1-D tables), used for large grids
+    where the Fourier-mode generator above would need tens of GB of host memory."""
+    ny = ny or nx
+    nz = nz or nx
+    dx = LX / nx
+    x = (np.arange(nx) + 0.5) * dx
+    y = (np.arange(ny) + 0.5) * dx
+    z = (np.arange(nz) + 0.5) * dx
+    u = np.zeros((nz, ny, nx))
+    v = np.zeros((nz, ny, nx))
+    w = np.zeros((nz, ny, nx))
+    for k, a in modes:
+        u += (a * np.sin(k * z))[:, None, None] + (a * np.cos(k * y))[None, :, None]
+        v += (a * np.sin(k * x))[None, None, :] + (a * np.cos(k * z))[:, None, None]
+        w += (a * np.sin(k * y))[None, :, None] + (a * np.cos(k * x))[None, None, :]
+    return u, v, w
