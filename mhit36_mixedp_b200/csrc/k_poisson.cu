@@ -182,15 +182,25 @@ k_fftx_inv(const Cx<T>* __restrict__ spec, T* __restrict__ p, const Cx<T>* __res
 // its results straight to global memory; in MODE 2 the forward transform's last stage, the
 // divide and the inverse transform's first stage (radices in reversed order, so it works on the
 // same strided element set) stay in registers: 4 shared-memory passes over the tile per
-// transform of three stages instead of 8.  The z solve keeps two transforms' worth of
-// butterflies in registers and runs one block per SM without spills; the single transforms of
-// up to 512 points fit two blocks per SM.
+// transform of three stages instead of 8.
+//
+// Tiles are 8 columns wide in both precisions (64-byte rows of float complex: whole DRAM
+// sectors, one butterfly per thread and stage for the 512-point transforms).  The FP64 z solve
+// keeps two transforms' worth of butterflies in registers and runs one block per SM without
+// spills, the FP32 one two blocks; the single transforms of up to 512 points fit two blocks per
+// SM.  Measured at 512^3 FP32: 16-column tiles 0.603 ms for the z solve, 8 columns 0.551 ms,
+// 4 columns 0.68 ms.
+template <typename T, int N, int MODE> struct ColTile {
+  static constexpr int B = 8;
+  static constexpr int MINB = (N >= 1024 || (MODE == 2 && sizeof(T) == 8)) ? 1 : 2;
+};
+
 template <typename T, int N, int MODE>
-__global__ void __launch_bounds__(fft_threads<N, Tile<T>::B>(), (MODE == 2 || N >= 1024) ? 1 : 2)
+__global__ void __launch_bounds__(fft_threads<N, ColTile<T, N, MODE>::B>(), ColTile<T, N, MODE>::MINB)
 k_fft_cols(Cx<T>* __restrict__ spec, const Cx<T>* __restrict__ tw, Geo g, size_t stride_n,
            size_t stride_outer, const double* __restrict__ k2x, const double* __restrict__ k2y,
            const double* __restrict__ k2z, double ntot) {
-  constexpr int B = Tile<T>::B;
+  constexpr int B = ColTile<T, N, MODE>::B;
   constexpr int NT = fft_threads<N, B>();
   constexpr int NS = Radix<N>::ns;
   constexpr int RA = rad<N, false>(0), RL = rad<N, false>(NS - 1);
@@ -296,7 +306,7 @@ static cudaError_t launch_xinv_m(const PoissonArgs& a, cudaStream_t st) {
 
 template <typename T, int N, int MODE>
 static cudaError_t launch_cols_n(const PoissonArgs& a, int axis, cudaStream_t st) {
-  constexpr int B = Tile<T>::B;
+  constexpr int B = ColTile<T, N, MODE>::B;
   constexpr int NT = fft_threads<N, B>();
   const size_t smem = (size_t)N * B * sizeof(Cx<T>);
   auto kern = k_fft_cols<T, N, MODE>;
