@@ -8,11 +8,17 @@
 //
 // Blocking: a block owns a MTX x MTY column of cells and marches up a chunk of z planes.
 // Rings of z planes live in shared memory, filled with cp.async one plane ahead of use:
-//   u, v, w   planes k-1..k+2 (slot k+2 in flight), x/y halo 1
-//   phi^{n+1} planes k-2..k+2, x halo [-2,+1], y halo [-2,+1]
-//   chempot   planes k-1, k over x [-1, MTX-1], y [-1, MTY-1]
+//   u, v, w   planes k-1..k+1 read, k+2 in flight (4 slots), y halo 1, x rows [-2, MTX+2)
+//   phi^{n+1} planes k-2..k+2 read, k+3 in flight (8 slots), y halo [-2,+1], x rows [-2, MTX+2)
+//   chempot   planes k-1, k read, k+1 written (4 slots) over x [-1, MTX-1], y [-1, MTY-1]
 // so every input byte crosses HBM once (plus the x/y halo re-read from L2) and the chemical
-// potential is evaluated once per cell.
+// potential is evaluated once per cell.  Iteration k computes the chemical potential of plane
+// k+1 and the output of plane k after a single barrier: every shared read of the iteration
+// reads what earlier iterations wrote or copied.  The rows start at x = -2, an even column because the
+// tile origin and nx are even, so they are copied as 16-byte pairs with cp.async.cg, which
+// bypasses L1: with 8-byte copies (which allocate in L1) the kernel was 3.06 ms at 512^3 and
+// 4.24 ms when the shared-memory carveout left L1 small; with 16-byte L2-only copies it is
+// 2.96 ms whatever the carveout.
 //
 // The velocity read here is the stored one minus the running mean of the previous
 // projection (DevScalars::mean); subtracting on read is exactly the reference's
@@ -26,14 +32,14 @@ namespace mhit {
 
 constexpr int MTX = 32, MTY = 8, MNT = MTX * MTY;
 constexpr int MZC = 32;                       // default z planes per block
-constexpr int UPX = MTX + 2, UPY = MTY + 2;   // u/v/w plane (halo 1)
+constexpr int UPX = MTX + 4, UPY = MTY + 2;   // u/v/w plane: x in [-2, T+2), y in [-1, T+1)
 constexpr int UPL = UPX * UPY;
-constexpr int PPX = MTX + 3, PPY = MTY + 3;   // phi plane: x,y in [-2, T+1)
+constexpr int PPX = MTX + 4, PPY = MTY + 3;   // phi plane: x in [-2, T+2), y in [-2, T+1)
 constexpr int PPL = PPX * PPY;
 constexpr int CPX = MTX + 1, CPY = MTY + 1;   // chempot plane: x,y in [-1, T)
 constexpr int CPL = CPX * CPY;
-constexpr int UCP = (UPL + MNT - 1) / MNT;    // copies per thread per u/v/w plane
-constexpr int PCP = (PPL + MNT - 1) / MNT;
+constexpr int UPAIRS = UPY * (UPX / 2), PPAIRS = PPY * (PPX / 2);  // 16-byte copies per plane
+static_assert(UPAIRS <= MNT && PPAIRS <= MNT, "one pair per thread and plane");
 
 template <bool PHI> struct MomSmem;
 template <> struct MomSmem<false> {
@@ -41,9 +47,15 @@ template <> struct MomSmem<false> {
 };
 template <> struct MomSmem<true> {
   double u[4][UPL], v[4][UPL], w[4][UPL];
-  double phi[5][PPL];
-  double cp[2][CPL];
+  double phi[8][PPL];
+  double cp[4][CPL];
 };
+
+// 16-byte global -> shared copy through L2 only (cp.async.cg)
+__device__ __forceinline__ void cp16(void* dst, const void* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
 
 __device__ __forceinline__ int pmod_int(int x, int n) {
   x %= n;
@@ -63,67 +75,35 @@ __global__ void __launch_bounds__(MNT, 3) k_mom(MomArgs a) {
   const int k1 = min(k0 + zc, nz);
   const int tid = threadIdx.x;
 
-  // per-thread in-plane source offsets of the elements this thread copies
-  int uoff[UCP], poff[PCP];
-#pragma unroll
-  for (int c = 0; c < UCP; ++c) {
-    const int e = tid + c * MNT;
-    uoff[c] = -1;
-    if (e < UPL) {
-      const int y = e / UPX, x = e - y * UPX;
-      uoff[c] = pmod_int(j0 - 1 + y, ny) * nx + pmod_int(i0 - 1 + x, nx);
-    }
+  // this thread's 16-byte pair of a u/v/w plane and of a phi plane: source offset in the
+  // plane, destination index in the ring plane (-1: no pair)
+  int up_src = -1, up_dst = 0, pp_src = -1, pp_dst = 0;
+  if (tid < UPAIRS) {
+    const int y = tid / (UPX / 2), xp = tid - y * (UPX / 2);
+    up_src = pmod_int(j0 - 1 + y, ny) * nx + pmod_int(i0 - 2 + 2 * xp, nx);
+    up_dst = y * UPX + 2 * xp;
   }
-#pragma unroll
-  for (int c = 0; c < PCP; ++c) {
-    const int e = tid + c * MNT;
-    poff[c] = -1;
-    if (PHI && e < PPL) {
-      const int y = e / PPX, x = e - y * PPX;
-      poff[c] = pmod_int(j0 - 2 + y, ny) * nx + pmod_int(i0 - 2 + x, nx);
-    }
+  if (PHI && tid < PPAIRS) {
+    const int y = tid / (PPX / 2), xp = tid - y * (PPX / 2);
+    pp_src = pmod_int(j0 - 2 + y, ny) * nx + pmod_int(i0 - 2 + 2 * xp, nx);
+    pp_dst = y * PPX + 2 * xp;
   }
-  auto issue_plane = [&](int m) {
-    const int kw = pmod_int(m, nz);
-    const size_t base = (size_t)kw * plane;
-    const int su = (m - k0 + 8) & 3;
-#pragma unroll
-    for (int c = 0; c < UCP; ++c) {
-      if (uoff[c] >= 0) {
-        const int e = tid + c * MNT;
-        __pipeline_memcpy_async(&S.u[su][e], a.u + base + uoff[c], 8);
-        __pipeline_memcpy_async(&S.v[su][e], a.v + base + uoff[c], 8);
-        __pipeline_memcpy_async(&S.w[su][e], a.w + base + uoff[c], 8);
-      }
-    }
+  auto copy_phi = [&](int m, size_t base) {
     if constexpr (PHI) {
-      const int sp = (m - k0 + 10) % 5;
-#pragma unroll
-      for (int c = 0; c < PCP; ++c) {
-        if (poff[c] >= 0) {
-          const int e = tid + c * MNT;
-          __pipeline_memcpy_async(&reinterpret_cast<MomSmem<true>&>(S).phi[sp][e], a.phi + base + poff[c], 8);
-        }
-      }
+      if (pp_src >= 0)
+        cp16(&reinterpret_cast<MomSmem<true>&>(S).phi[(m - k0 + 16) & 7][pp_dst], a.phi + base + pp_src);
     }
-    __pipeline_commit();
   };
-  // phi ring only (planes k0-2 .. k0-1 before the u ring starts)
-  auto issue_phi = [&](int m) {
-    if constexpr (PHI) {
-      const int kw = pmod_int(m, nz);
-      const size_t base = (size_t)kw * plane;
-      const int sp = (m - k0 + 10) % 5;
-#pragma unroll
-      for (int c = 0; c < PCP; ++c) {
-        if (poff[c] >= 0) {
-          const int e = tid + c * MNT;
-          __pipeline_memcpy_async(&reinterpret_cast<MomSmem<true>&>(S).phi[sp][e], a.phi + base + poff[c], 8);
-        }
-      }
+  auto issue_uvw = [&](int m) {
+    const size_t base = (size_t)pmod_int(m, nz) * plane;
+    const int su = (m - k0 + 16) & 3;
+    if (up_src >= 0) {
+      cp16(&S.u[su][up_dst], a.u + base + up_src);
+      cp16(&S.v[su][up_dst], a.v + base + up_src);
+      cp16(&S.w[su][up_dst], a.w + base + up_src);
     }
-    __pipeline_commit();
   };
+  auto issue_phi = [&](int m) { copy_phi(m, (size_t)pmod_int(m, nz) * plane); };
 
   const double eps = g.eps, epsi = g.epsi, ddxi = g.ddxi, dxi = g.dxi;
   const double s6 = 6.0 * g.sigma;
@@ -131,8 +111,8 @@ __global__ void __launch_bounds__(MNT, 3) k_mom(MomArgs a) {
   auto chempot_plane = [&](int m) {
     if constexpr (PHI) {
       auto& P = reinterpret_cast<MomSmem<true>&>(S).phi;
-      const int pm = (m - k0 + 9) % 5, p0 = (m - k0 + 10) % 5, pp = (m - k0 + 11) % 5;
-      const int sc = (m - k0 + 4) & 1;
+      const int pm = (m - k0 + 15) & 7, p0 = (m - k0 + 16) & 7, pp = (m - k0 + 17) & 7;
+      const int sc = (m - k0 + 16) & 3;
       for (int e = tid; e < CPL; e += MNT) {
         const int y = e / CPX, x = e - y * CPX;
         const int q = (y + 1) * PPX + (x + 1);  // phi index of (i0-1+x, j0-1+y)
@@ -145,14 +125,22 @@ __global__ void __launch_bounds__(MNT, 3) k_mom(MomArgs a) {
 
   const double mu_ = a.sc->mean[0], mv_ = a.sc->mean[1], mw_ = a.sc->mean[2];
 
-  // prologue: phi k0-2, k0-1; u/v/w + phi k0-1, k0, k0+1
-  issue_phi(k0 - 2);
-  issue_plane(k0 - 1);
-  issue_plane(k0);
-  issue_plane(k0 + 1);
-  __pipeline_wait_prior(0);
-  __syncthreads();
-  chempot_plane(k0 - 1);
+  // Iteration k computes the chemical potential of plane k+1 and the output of plane k after
+  // one barrier; the copies it waits for (u, v, w(k+1), phi(k+2)) were issued one iteration
+  // earlier.  With the phase field the loop starts at k0-2 (k0-2, k0-1 only fill the chemical
+  // potential of k0-1 and k0), so every chemical potential comes from the loop body.
+  const int ks = PHI ? k0 - 2 : k0;
+  if constexpr (PHI) {
+    issue_phi(k0 - 2);
+    issue_phi(k0 - 1);
+    issue_phi(k0);
+    issue_uvw(k0 - 1);
+  } else {
+    issue_uvw(k0 - 1);
+    issue_uvw(k0);
+    issue_uvw(k0 + 1);
+  }
+  __pipeline_commit();
 
   const int tx = tid % MTX, ty = tid / MTX;
   const int i = i0 + tx, j = j0 + ty;
@@ -163,26 +151,31 @@ __global__ void __launch_bounds__(MNT, 3) k_mom(MomArgs a) {
   const double mu = g.mu, rhoi = g.rhoi, dt = g.dt, al = a.alpha, be = a.beta;
   // (h*0.25)*dxi == h*(0.25*dxi) exactly: scaling by 0.25 does not round
   const double q4 = 0.25 * dxi;
-  const int uq = (ty + 1) * UPX + (tx + 1);   // own cell in the u/v/w plane
+  const int uq = (ty + 1) * UPX + (tx + 2);   // own cell in the u/v/w plane
   const int pq = (ty + 2) * PPX + (tx + 2);   // own cell in the phi plane
   const int cq = (ty + 1) * CPX + (tx + 1);   // own cell in the chempot plane
 
-  for (int k = k0; k < k1; ++k) {
-    const size_t c = (size_t)k * plane + (size_t)(own ? j : 0) * nx + (own ? i : 0);
+  for (int k = ks; k < k1; ++k) {
+    const bool out = own && k >= k0;
+    const size_t c = (size_t)(k >= k0 ? k : k0) * plane + (size_t)(own ? j : 0) * nx + (own ? i : 0);
     double ruo = 0.0, rvo = 0.0, rwo = 0.0;
-    if (own) {
+    if (out) {
       ruo = a.ru[c];
       rvo = a.rv[c];
       rwo = a.rw[c];
     }
-    // plane k+1 landed (issued one iteration ago); everyone is done with iteration k-1
+    // this thread's copies landed; after the barrier everyone's have, and everyone is done
+    // with iteration k-1
     __pipeline_wait_prior(0);
     __syncthreads();
-    issue_plane(k + 2);
-    chempot_plane(k);
-    __syncthreads();
-    if (own) {
-      const int sm = (k - k0 + 7) & 3, s0 = (k - k0 + 8) & 3, sp = (k - k0 + 9) & 3;
+    if (k + 1 < k1) {
+      issue_uvw(k + 2);
+      issue_phi(k + 3);
+    }
+    __pipeline_commit();
+    if (k + 1 < k1) chempot_plane(k + 1);
+    if (out) {
+      const int sm = (k - k0 + 15) & 3, s0 = (k - k0 + 16) & 3, sp = (k - k0 + 17) & 3;
       const double* U0 = S.u[s0];
       const double* V0 = S.v[s0];
       const double* W0 = S.w[s0];
@@ -223,8 +216,8 @@ __global__ void __launch_bounds__(MNT, 3) k_mom(MomArgs a) {
       if constexpr (PHI) {
         // :737-739 at the cell and at its -x/-y/-z neighbours, :768-770 face average
         auto& SP = reinterpret_cast<MomSmem<true>&>(S);
-        const int pmm = (k - k0 + 8) % 5, pm = (k - k0 + 9) % 5, p0 = (k - k0 + 10) % 5, pp = (k - k0 + 11) % 5;
-        const int c0s = (k - k0 + 4) & 1, cms = (k - k0 + 3) & 1;
+        const int pmm = (k - k0 + 14) & 7, pm = (k - k0 + 15) & 7, p0 = (k - k0 + 16) & 7, pp = (k - k0 + 17) & 7;
+        const int c0s = (k - k0 + 16) & 3, cms = (k - k0 + 15) & 3;
         const double* P0 = SP.phi[p0];
         const double pc = P0[pq];
         const double c0 = SP.cp[c0s][cq];
