@@ -71,7 +71,28 @@ def build(verbose: bool = False, force: bool = False, extra_flags=None) -> str:
             sys.stderr.write(" ".join(cmd) + "\n" + r.stdout + r.stderr)
         if r.returncode != 0:
             raise RuntimeError("link of libmhit_b200.so failed")
+    build_host(verbose, force)
     return LIB
+
+
+HOST_SRC = os.path.join(HERE, "host", "mhit_main.cpp")
+HOST_BIN = os.path.join(HERE, "mhit_main")
+
+
+def build_host(verbose: bool = False, force: bool = False) -> str:
+    """The C++ host driver (host/mhit_main.cpp) linked against the library, rpath $ORIGIN."""
+    deps = [HOST_SRC, LIB, os.path.join(ROOT, "include", "mhit_b200.h")]
+    if not force and os.path.exists(HOST_BIN) and os.path.getmtime(HOST_BIN) >= max(os.path.getmtime(d) for d in deps):
+        return HOST_BIN
+    cxx = shutil.which("g++") or "g++"
+    cmd = [cxx, "-O2", "-std=c++17", "-Wall", HOST_SRC, "-o", HOST_BIN, "-L", HERE, "-lmhit_b200",
+           "-Wl,-rpath,$ORIGIN"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if verbose or r.returncode != 0:
+        sys.stderr.write(" ".join(cmd) + "\n" + r.stdout + r.stderr)
+    if r.returncode != 0:
+        raise RuntimeError("build of the host driver failed")
+    return HOST_BIN
 
 
 if __name__ == "__main__":
