@@ -136,6 +136,14 @@ def workload(n, seed_drops=1, seed_vel=2):
     return prm, u, v, w, phi
 
 
+def max_over_ranks(values, dist, device):
+    """Element-wise maximum of per-rank timings over the process group (every rank gets it)."""
+    import torch
+    t = torch.tensor([float(x) for x in values], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t]
+
+
 def run_ours(args, rank, world, dev):
     from mhit36_mixedp_b200 import Params, Solver
     n = args.n
@@ -386,10 +394,7 @@ def main():
     res, e2e = run_ours(args, rank, world, dev)
     ms32, ms64 = res["fp32"]["ms"], res["fp64"]["ms"]
     if dist:
-        import torch
-        t = torch.tensor([ms32, ms64], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms32, ms64 = float(t[0]), float(t[1])
+        ms32, ms64 = max_over_ranks([ms32, ms64], dist, f"cuda:{local}")
         dist.barrier()
     if rank == 0:
         n = args.n
