@@ -237,17 +237,20 @@ def cpu_sample(n_sample=256, steps=3, n_target=512):
                       f"{steps} steps, best AB2 step x (512/{n_sample})^3 = {scale:g}"}
 
 
-def ensemble_workload():
+def ensemble_workload(indices=None):
     """32 NS+ACDI boxes: 16 x 64^3, 10 x 128^3, 6 x 192^3; per-box seeds 100+b; nu ~ U[0.002,0.01],
-    We ~ U[0.5,5], 32-256 drops of radius 0.3 (eps = dx), FP32 Poisson, dt = 2e-4."""
+    We ~ U[0.5,5], 32-256 drops of radius 0.3 (eps = dx), FP32 Poisson, dt = 2e-4.  With indices,
+    only those boxes' fields are built (the parameters of every box come from one seeded stream)."""
     from mhit36_mixedp_b200 import Params, synth
     rng = np.random.default_rng(99)
-    sizes = [64] * 16 + [128] * 10 + [192] * 6
+    sizes = ENSEMBLE_SIZES
     boxes = []
     for b, n in enumerate(sizes):
         nu = float(rng.uniform(0.002, 0.01))
         we = float(rng.uniform(0.5, 5.0))
         ndrops = int(rng.integers(32, 257))
+        if indices is not None and b not in indices:
+            continue
         u, v, w = synth.solenoidal_velocity(n, 100 + b)
         phi = synth.drops_phi(n, synth.drop_centres(ndrops, 100 + b), 0.3, 2 * math.pi / n)
         prm = Params(nx=n, dt=2e-4, mu=nu, rho=1.0, radius=0.3, sigma=synth.sigma_from_weber(1.0, 1.0, 0.3, we),
@@ -256,84 +259,74 @@ def ensemble_workload():
     return boxes
 
 
+ENSEMBLE_SIZES = [64] * 16 + [128] * 10 + [192] * 6
+
+
+def partition_boxes(sizes, nranks):
+    """Boxes onto ranks by greedy longest-first bin packing on the cell count (the step cost is
+    proportional to it): the box indices of each rank, sorted."""
+    order = sorted(range(len(sizes)), key=lambda b: (-sizes[b] ** 3, b))
+    load = [0] * nranks
+    parts = [[] for _ in range(nranks)]
+    for b in order:
+        r = min(range(nranks), key=lambda q: (load[q], q))
+        parts[r].append(b)
+        load[r] += sizes[b] ** 3
+    return [sorted(p) for p in parts]
+
+
 def run_ensemble(args):
+    """The 32-box ensemble; under torchrun the boxes are shared out over the ranks (strong
+    scaling: the same 32 boxes whatever N), each rank steps its share as one ensemble, and the
+    step time is the max over ranks."""
     from mhit36_mixedp_b200 import Ensemble
-    boxes = ensemble_workload()
-    with Ensemble([b[0] for b in boxes]) as ens:
-        tuning = ens.autotune(trials=2)
-        for box, (prm, u, v, w, phi) in zip(ens.boxes, boxes):
-            box.upload(u, v, w, phi)
-        ens.step(max(args.warmup, 3))
-        with Clocks(0) as clk:
-            ms = ens.time_steps(args.steps)
-        ens.step(0)
-    npts = sum(b[0].nx ** 3 for b in boxes)
-    peak, kind = peaks()
-    frac = STEP_BYTES["fp32"] * npts / (ms / args.steps * 1e-3) / 1e9 / peak
-    line = {"metric": "ms per ensemble step, 32 NS+ACDI boxes (16x64^3, 10x128^3, 6x192^3), FP32 Poisson",
-            "value": ms / args.steps, "unit": "ms/timestep", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-            "higher_is_better": False, "data": "synthetic", "dtype": "f64+f32",
-            "config": {"workload": "ensemble", "boxes": len(boxes), "points": npts, "one_graph_launch_per_step": True},
-            "tuning": tuning, "step_roofline_frac": frac, "peak_kind": kind, "clocks": clk.summary()}
-    print(json.dumps(line), flush=True)
-    return 0
-
-
-def run_large_ns(args):
-    """1024^3 NS (no phase field), FP32 against FP64 Poisson, ABC velocity, nu = 8e-4."""
-    from mhit36_mixedp_b200 import Params, Solver, synth
-    n = 1024 if args.n == 512 else args.n
-    u, v, w = synth.abc_velocity(n)
-    prm = dict(nx=n, dt=2e-4, mu=8e-4, rho=1.0, f1=1.0, f2=1.0, f3=1.0, k0=2.0)
-    res = {}
-    for mode in ("fp32", "fp64"):
-        with Solver(Params(poisson=mode, **prm)) as s:
-            s.upload(u, v, w)
-            s.step(max(args.warmup, 3))
-            with Clocks(0) as clk:
-                ms = s.time_steps(args.steps)
-            s.step(0)
-            prof = s.profile_step()
-            dg = s.diagnostics()
-        res[mode] = {"ms_per_step": ms / args.steps, "stages_ms": prof, "maxdiv": dg["maxdiv"], "clocks": clk.summary()}
-    peak, kind = peaks()
-    npts = n ** 3
-    ns_bytes = {"fp32": 192, "fp64": 216}  # NS step model: 192 / 216 B per point
-    for mode in res:
-        res[mode]["step_roofline_frac"] = ns_bytes[mode] * npts / (res[mode]["ms_per_step"] * 1e-3) / 1e9 / peak
-    line = {"metric": f"ms/timestep {n}^3 NS, 1 B200, FP32 vs FP64 Poisson", "value": res["fp32"]["ms_per_step"],
-            "unit": "ms/timestep", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
-            "data": "synthetic (ABC flow k=1,3)", "dtype": "f64+f32",
-            "config": {"workload": f"NS {n}^3, nu=8e-4, dt=2e-4", "l2": "inputs larger than L2"},
-            "fp64_ms_per_step": res["fp64"]["ms_per_step"], "detail": res, "peak_kind": kind}
-    print(json.dumps(line), flush=True)
-    return 0
-
-
-def run_tracers(args):
-    """512^3 NS+ACDI with 1e6 tracers, FP64 Poisson, both interpolation modes."""
-    from mhit36_mixedp_b200 import Params, Solver, synth
-    n = args.n
-    prm, u, v, w, phi = workload(n)
-    npart = 1_000_000
-    part = synth.uniform_particles(npart, 3)
-    prm = dict(prm, partflag=1, npart=npart)
-    res = {}
-    for interp in ("linear1d", "trilinear"):
-        with Solver(Params(poisson="fp64", interp=interp, **prm)) as s:
-            s.upload(u, v, w, phi)
-            s.upload_particles(part)
-            s.step(max(args.warmup, 3))
-            ms = s.time_steps(args.steps)
-            s.step(0)
-            prof = [s.profile_step() for _ in range(3)]
-        tr = statistics.mean(p["k_tracer"] for p in prof if "k_tracer" in p) if "k_tracer" in prof[0] else None
-        res[interp] = {"ms_per_step": ms / args.steps, "tracer_stage_ms": tr}
-    line = {"metric": f"ms/timestep {n}^3 NS+ACDI + 1e6 tracers, 1 B200, FP64 Poisson",
-            "value": res["linear1d"]["ms_per_step"], "unit": "ms/timestep", "n_gpus": 1, "steps": args.steps,
-            "warmup": args.warmup, "higher_is_better": False, "data": "synthetic", "dtype": "f64",
-            "config": {"workload": f"NS+ACDI {n}^3 + 1e6 uniform tracers (seed 3)"}, "detail": res}
-    print(json.dumps(line), flush=True)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(local)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist = tdist
+    mine = partition_boxes(ENSEMBLE_SIZES, world)[rank]
+    ms, tuning, clocks = 0.0, None, None
+    if mine:
+        boxes = ensemble_workload(set(mine))
+        for b in boxes:
+            b[0].device = local
+        with Ensemble([b[0] for b in boxes]) as ens:
+            tuning = ens.autotune(trials=2)
+            for box, (prm, u, v, w, phi) in zip(ens.boxes, boxes):
+                box.upload(u, v, w, phi)
+            ens.step(max(args.warmup, 3))
+            if dist:
+                dist.barrier()
+            with Clocks(local) as clk:
+                ms = ens.time_steps(args.steps)
+            ens.step(0)
+            clocks = clk.summary()
+    elif dist:
+        dist.barrier()
+    if dist:
+        ms = max_over_ranks([ms], dist, f"cuda:{local}")[0]
+        dist.barrier()
+    if rank == 0:
+        npts = sum(n ** 3 for n in ENSEMBLE_SIZES)
+        peak, kind = peaks()
+        frac = STEP_BYTES["fp32"] * npts / (ms / args.steps * 1e-3) / 1e9 / peak / world
+        line = {"metric": "ms per ensemble step, 32 NS+ACDI boxes (16x64^3, 10x128^3, 6x192^3), FP32 Poisson",
+                "value": ms / args.steps, "unit": "ms/timestep", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "higher_is_better": False, "scaling": "strong", "data": "synthetic",
+                "dtype": "f64+f32",
+                "config": {"workload": "ensemble", "boxes": len(ENSEMBLE_SIZES), "points": npts,
+                           "one_graph_launch_per_step": True, "boxes_per_rank": [len(p) for p in partition_boxes(ENSEMBLE_SIZES, world)]},
+                "tuning_rank0": tuning, "step_roofline_frac": frac, "peak_kind": kind, "clocks": clocks}
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
     return 0
 
 
