@@ -24,12 +24,18 @@ __constant__ int8_t c_fwd[13][3] = {{0, 0, 1},  {0, 1, 0},  {1, 0, 0},  {0, 1, 1
                                     {1, 0, 1},  {1, 0, -1}, {1, 1, 0},  {1, -1, 0}, {1, 1, 1},
                                     {1, 1, -1}, {1, -1, 1}, {1, -1, -1}};
 
-__device__ __forceinline__ int find_root(const int* lab, int x, long long bound, int* err) {
-  const volatile int* vl = lab;  // parents change under concurrent links: read them from L2
+// Root of x with path halving: each visited node is re-pointed at its grandparent.  A node's
+// ancestors stay its ancestors (roots are only ever hung under smaller roots) and parents only
+// decrease, so a plain store of the grandparent is safe under concurrent links and halvings.
+__device__ __forceinline__ int find_root(int* lab, int x, long long bound, int* err) {
+  volatile int* vl = lab;  // parents change under concurrent links: read them from L2
   for (long long it = 0; it < bound; ++it) {
     const int y = vl[x];
     if (y == x) return x;
-    x = y;
+    const int z = vl[y];
+    if (z == y) return y;
+    vl[x] = z;
+    x = z;
   }
   atomicExch(err, 1);
   return x;
@@ -129,7 +135,11 @@ __device__ __forceinline__ int drop_of(const int* lab, int c) {
 }
 
 // per drop: cells, sums of sin/cos of the cell centre per axis, sums of u, v, w
-// (post/unionfind_periodic/main.f90:302-315); acc is [ndrops][LACC]
+// (post/unionfind_periodic/main.f90:302-315); acc is [ndrops][9].  Cells of one drop are
+// contiguous along x, so the 32 cells a warp visits mostly belong to one or two drops: the
+// lanes of each drop are grouped (match_any), sum their values with shuffles, and one lane per
+// group does the atomics -- a drop of 10^5 cells would otherwise serialise 10^6 atomics on nine
+// addresses.
 __global__ void k_lab_stats(const int* __restrict__ lab, int nx, int ny, int nz, const double* __restrict__ u,
                             const double* __restrict__ v, const double* __restrict__ w,
                             const double* __restrict__ trig, const DevScalars* __restrict__ sc,
@@ -143,21 +153,45 @@ __global__ void k_lab_stats(const int* __restrict__ lab, int nx, int ny, int nz,
   const double* cys = sy + ny;
   const double* sz = cys + ny;
   const double* czs = sz + nz;
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
-    const int d = drop_of(lab, c);
-    if (d < 0) continue;
-    const int i = c % nx, j = (c / nx) % ny, k = c / (nx * ny);
-    double* a = acc + (size_t)d * 9;
-    atomicAdd(&cells[d], 1ull);
-    atomicAdd(a + 0, sx[i]);
-    atomicAdd(a + 1, cxs[i]);
-    atomicAdd(a + 2, sy[j]);
-    atomicAdd(a + 3, cys[j]);
-    atomicAdd(a + 4, sz[k]);
-    atomicAdd(a + 5, czs[k]);
-    atomicAdd(a + 6, u[c] - mu_);
-    atomicAdd(a + 7, v[c] - mv_);
-    atomicAdd(a + 8, w[c] - mw_);
+  const int lane = threadIdx.x & 31;
+  const int warps = gridDim.x * (blockDim.x >> 5);
+  // warp-uniform loop: all 32 lanes take part in every match and shuffle
+  for (int base = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32; base < n; base += warps * 32) {
+    const int c = base + lane;
+    const int d = c < n ? drop_of(lab, c) : -1;
+    if (__all_sync(0xffffffffu, d < 0)) continue;  // the whole warp is background (most warps)
+    double val[9];
+    if (d >= 0) {
+      const int i = c % nx, j = (c / nx) % ny, k = c / (nx * ny);
+      val[0] = sx[i];
+      val[1] = cxs[i];
+      val[2] = sy[j];
+      val[3] = cys[j];
+      val[4] = sz[k];
+      val[5] = czs[k];
+      val[6] = u[c] - mu_;
+      val[7] = v[c] - mv_;
+      val[8] = w[c] - mw_;
+    } else {
+#pragma unroll
+      for (int q = 0; q < 9; ++q) val[q] = 0.0;
+    }
+    const unsigned grp = __match_any_sync(0xffffffffu, d);
+    double sum[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) sum[q] = 0.0;
+    // every lane of a group walks the same lanes in the same order: the sums are identical
+    for (unsigned m = grp; m; m &= m - 1) {
+      const int l = __ffs(m) - 1;
+#pragma unroll
+      for (int q = 0; q < 9; ++q) sum[q] += __shfl_sync(grp, val[q], l);
+    }
+    if (d >= 0 && lane == __ffs(grp) - 1) {
+      double* a = acc + (size_t)d * 9;
+      atomicAdd(&cells[d], (unsigned long long)__popc(grp));
+#pragma unroll
+      for (int q = 0; q < 9; ++q) atomicAdd(a + q, sum[q]);
+    }
   }
 }
 

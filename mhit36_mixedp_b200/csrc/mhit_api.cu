@@ -64,6 +64,10 @@ struct mhit_ctx {
   float* P2 = nullptr;    // refinement: residual, then the pressure correction (FP32)
   double* P64 = nullptr;  // refinement: corrected pressure (FP64)
   double* Pw = nullptr;   // FP32 modes: the pressure widened to FP64 for a download (lazy)
+  void* lab_small = nullptr;  // droplet labelling scratch (trig tables, chunk counts), grown lazily
+  size_t lab_small_bytes = 0;
+  void* lab_acc = nullptr;    // droplet labelling per-drop sums, grown lazily
+  size_t lab_acc_bytes = 0;
   void* spec = nullptr;
   void *twx = nullptr, *twy = nullptr, *twz = nullptr;
   double *k2x = nullptr, *k2y = nullptr, *k2z = nullptr;
@@ -457,6 +461,8 @@ void mhit_destroy(mhit_ctx* c) {
   cudaFree(c->P2);
   cudaFree(c->P64);
   cudaFree(c->Pw);
+  cudaFree(c->lab_small);
+  cudaFree(c->lab_acc);
   cudaFree(c->spec);
   cudaFree(c->twx);
   cudaFree(c->twy);
@@ -961,6 +967,17 @@ int mhit_read_checkpoint(mhit_ctx* c, const char* path) {
 
 // ------------------------------------------------------------------ droplet labelling
 namespace {
+// device buffer that only grows (kept by the context across calls)
+int grow_buffer(void** p, size_t* have, size_t need) {
+  if (*have >= need) return MHIT_OK;
+  cudaFree(*p);
+  *p = nullptr;
+  *have = 0;
+  MHIT_CUDA_TRY(cudaMalloc(p, need));
+  *have = need;
+  return MHIT_OK;
+}
+
 struct DevBuf {  // temporary device allocation freed on every return path
   void* p = nullptr;
   ~DevBuf() {
@@ -982,10 +999,10 @@ int mhit_label_drops(mhit_ctx* c, double thresh, int connectivity, mhit_drop* dr
   // scratch: the spectrum buffer (at least 4 bytes per cell, unused between steps) holds the
   // parents; the chunk counts, the error flag and the trig tables share one allocation
   const size_t trig_n = 2 * (size_t)(nx + ny + nz);
-  DevBuf small, accb, outb;
+  DevBuf outb;
   const size_t small_bytes = sizeof(double) * trig_n + sizeof(int) * (nch + 1);
-  MHIT_CUDA_TRY(cudaMalloc(&small.p, small_bytes));
-  double* trig = static_cast<double*>(small.p);
+  if ((rc = grow_buffer(&c->lab_small, &c->lab_small_bytes, small_bytes))) return rc;
+  double* trig = static_cast<double*>(c->lab_small);
   int* counts = reinterpret_cast<int*>(trig + trig_n);
   int* err = counts + nch;
   // cell centres x_i = dx/2 + (i-1) dx accumulated as post/unionfind_periodic/main.f90:294-298,
@@ -1040,10 +1057,11 @@ int mhit_label_drops(mhit_ctx* c, double thresh, int connectivity, mhit_drop* dr
   MHIT_CUDA_TRY(cudaMemcpyAsync(counts, cnt.data(), sizeof(int) * nch, cudaMemcpyHostToDevice, c->st));
   MHIT_CUDA_TRY(launch_label_number(a, c->st));
   const size_t nd = (size_t)std::max(total, 1);
-  MHIT_CUDA_TRY(cudaMalloc(&accb.p, nd * (9 * sizeof(double) + sizeof(unsigned long long))));
-  a.acc = static_cast<double*>(accb.p);
+  const size_t acc_bytes = nd * (9 * sizeof(double) + sizeof(unsigned long long));
+  if ((rc = grow_buffer(&c->lab_acc, &c->lab_acc_bytes, acc_bytes))) return rc;
+  a.acc = static_cast<double*>(c->lab_acc);
   a.cells = reinterpret_cast<unsigned long long*>(a.acc + nd * 9);
-  MHIT_CUDA_TRY(cudaMemsetAsync(accb.p, 0, nd * (9 * sizeof(double) + sizeof(unsigned long long)), c->st));
+  MHIT_CUDA_TRY(cudaMemsetAsync(c->lab_acc, 0, acc_bytes, c->st));
   if (labels) {
     MHIT_CUDA_TRY(cudaMalloc(&outb.p, sizeof(int) * c->n));
     a.out = static_cast<int*>(outb.p);
