@@ -171,3 +171,29 @@ def test_fp32_refined_needs_modified_laplacian(gpu):
     from mhit36_mixedp_b200 import MhitArgError
     with pytest.raises(MhitArgError, match="MODIFIED"):
         Solver(Params(nx=32, poisson="fp32_refined"))
+
+
+@pytest.mark.parametrize("poisson,tol", [("fp64", TOL64), ("fp32", 1e-5)])
+def test_noncubic_box(gpu, poisson, tol):
+    """nx != ny != nz (32 x 16 x 64, spacing 2 pi/nx in every direction): every kernel's y and
+    z wraps, the 16- and 64-point column transforms and the tracers on a non-cubic box."""
+    nx, ny, nz = 32, 16, 64
+    dx = 2 * np.pi / nx
+    u, v, w = synth.solenoidal_velocity(nx, 4, ny=ny, nz=nz)
+    x = (np.arange(nx) + 0.5) * dx
+    y = (np.arange(ny) + 0.5) * dx
+    z = (np.arange(nz) + 0.5) * dx
+    r = np.sqrt((x[None, None, :] - np.pi) ** 2 + (y[None, :, None] - ny * dx / 2) ** 2
+                + (z[:, None, None] - nz * dx / 2) ** 2)
+    phi = 0.5 * (1.0 - np.tanh((r - 0.8) / (2 * dx)))
+    part = synth.uniform_particles(300, 9)
+    part[:, 2] *= ny / nx  # positions inside the y and z extents
+    part[:, 3] *= nz / nx
+    prm = dict(nx=nx, ny=ny, nz=nz, dt=5e-4, mu=0.006, rho=1.0, f1=1.0, f2=1.0, f3=1.0, k0=2.0, radius=0.8,
+               sigma=0.5, epsr=1.0, phiflag=1, partflag=1, poisson=poisson)
+    st, out, dg, gpart = run_both(prm, u, v, w, phi, part, 4)
+    for f in ("u", "v", "w", "phi"):
+        e = relerr(out[f], getattr(st, f))
+        assert e < tol, (f, e)
+    # positions integrate the velocity: dt * steps * (velocity difference) bounds them
+    assert np.max(np.abs(gpart[:, 1:4] - st.part[:, 1:4])) < (1e-10 if poisson == "fp64" else 1e-7)
