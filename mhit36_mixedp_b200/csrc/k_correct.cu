@@ -17,24 +17,40 @@ constexpr int CNT = 256;
 
 constexpr int CTX = 32, CTY = 16, CZC = 16;  // x-y tile and z chunk of k_correct
 
-template <typename T> struct Pair;
-template <> struct Pair<double> {
-  using V = double2;
+// Pressure sources of the projection: a pair of x-adjacent values and a single value, widened
+// to FP64.  PSum is the refinement's p = p32 + delta, formed on the fly exactly as a stored
+// (double)p32 + (double)delta would be.
+struct PDouble {
+  const double* p;
+  __device__ __forceinline__ double2 pair(size_t o) const { return *reinterpret_cast<const double2*>(p + o); }
+  __device__ __forceinline__ double one(size_t o) const { return p[o]; }
 };
-template <> struct Pair<float> {
-  using V = float2;
+struct PFloat {
+  const float* p;
+  __device__ __forceinline__ double2 pair(size_t o) const {
+    const float2 v = *reinterpret_cast<const float2*>(p + o);
+    return make_double2((double)v.x, (double)v.y);
+  }
+  __device__ __forceinline__ double one(size_t o) const { return (double)p[o]; }
+};
+struct PSum {
+  const float* p;
+  const float* d;
+  __device__ __forceinline__ double2 pair(size_t o) const {
+    const float2 a = *reinterpret_cast<const float2*>(p + o), b = *reinterpret_cast<const float2*>(d + o);
+    return make_double2((double)a.x + (double)b.x, (double)a.y + (double)b.y);
+  }
+  __device__ __forceinline__ double one(size_t o) const { return (double)p[o] + (double)d[o]; }
 };
 
 // Each thread owns two adjacent x cells (16-byte loads of u, v, w) of one tile row and marches
 // up CZC planes two at a time: p(k-1) is carried in registers from the previous plane,
 // p(i-1) comes from the neighbouring lane of the 16-lane row, p(j-1) from L1.
-template <typename T>
-__global__ void __launch_bounds__(CNT) k_correct(CorrectArgs a) {
-  using PV = typename Pair<T>::V;
+template <typename S>
+__global__ void __launch_bounds__(CNT) k_correct(CorrectArgs a, S ps) {
   const Geo& g = a.g;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const size_t plane = (size_t)nx * ny;
-  const T* __restrict__ p = static_cast<const T*>(a.p);
   double* __restrict__ U = a.u;
   double* __restrict__ V = a.v;
   double* __restrict__ W = a.w;
@@ -50,16 +66,16 @@ __global__ void __launch_bounds__(CNT) k_correct(CorrectArgs a) {
   double mu = -INFINITY, mv = -INFINITY, mw = -INFINITY;
   const size_t r0 = (size_t)jc * nx + ic;
   const ptrdiff_t dym = ((ptrdiff_t)jm - jc) * nx;
-  PV pk = *reinterpret_cast<const PV*>(p + (size_t)wrapm(k0, nz) * plane + r0);
-  double pkm0 = (double)pk.x, pkm1 = (double)pk.y;
-  auto plane_step = [&](size_t c, const PV pc2, const PV py2, const T pxm_edge, const double2 uo, const double2 vo,
-                        const double2 wo) {
-    const double pc0 = (double)pc2.x, pc1 = (double)pc2.y;
+  const double2 pk = ps.pair((size_t)wrapm(k0, nz) * plane + r0);
+  double pkm0 = pk.x, pkm1 = pk.y;
+  auto plane_step = [&](size_t c, const double2 pc2, const double2 py2, const double pxm_edge, const double2 uo,
+                        const double2 vo, const double2 wo) {
+    const double pc0 = pc2.x, pc1 = pc2.y;
     double pxm0 = __shfl_up_sync(0xffffffffu, pc1, 1, 16);
-    if (edge) pxm0 = (double)pxm_edge;
+    if (edge) pxm0 = pxm_edge;
     // multi/main.f90:953-955
     const double u0 = uo.x - cc * (pc0 - pxm0) * dxi, u1 = uo.y - cc * (pc1 - pc0) * dxi;
-    const double v0 = vo.x - cc * (pc0 - (double)py2.x) * dxi, v1 = vo.y - cc * (pc1 - (double)py2.y) * dxi;
+    const double v0 = vo.x - cc * (pc0 - py2.x) * dxi, v1 = vo.y - cc * (pc1 - py2.y) * dxi;
     const double w0 = wo.x - cc * (pc0 - pkm0) * dxi, w1 = wo.y - cc * (pc1 - pkm1) * dxi;
     pkm0 = pc0;
     pkm1 = pc1;
@@ -78,9 +94,9 @@ __global__ void __launch_bounds__(CNT) k_correct(CorrectArgs a) {
   int k = k0;
   for (; k + 1 < k1; k += 2) {
     const size_t ca = (size_t)k * plane + r0, cb = ca + plane;
-    const PV pa = *reinterpret_cast<const PV*>(p + ca), pb = *reinterpret_cast<const PV*>(p + cb);
-    const PV ya = *reinterpret_cast<const PV*>(p + ca + dym), yb = *reinterpret_cast<const PV*>(p + cb + dym);
-    const T xa = edge ? p[ca - ic + im] : (T)0, xb = edge ? p[cb - ic + im] : (T)0;
+    const double2 pa = ps.pair(ca), pb = ps.pair(cb);
+    const double2 ya = ps.pair(ca + dym), yb = ps.pair(cb + dym);
+    const double xa = edge ? ps.one(ca - ic + im) : 0.0, xb = edge ? ps.one(cb - ic + im) : 0.0;
     const double2 ua = *reinterpret_cast<const double2*>(U + ca), ub = *reinterpret_cast<const double2*>(U + cb);
     const double2 va = *reinterpret_cast<const double2*>(V + ca), vb = *reinterpret_cast<const double2*>(V + cb);
     const double2 wa = *reinterpret_cast<const double2*>(W + ca), wb = *reinterpret_cast<const double2*>(W + cb);
@@ -89,9 +105,9 @@ __global__ void __launch_bounds__(CNT) k_correct(CorrectArgs a) {
   }
   if (k < k1) {
     const size_t ca = (size_t)k * plane + r0;
-    const PV pa = *reinterpret_cast<const PV*>(p + ca);
-    const PV ya = *reinterpret_cast<const PV*>(p + ca + dym);
-    const T xa = edge ? p[ca - ic + im] : (T)0;
+    const double2 pa = ps.pair(ca);
+    const double2 ya = ps.pair(ca + dym);
+    const double xa = edge ? ps.one(ca - ic + im) : 0.0;
     plane_step(ca, pa, ya, xa, *reinterpret_cast<const double2*>(U + ca), *reinterpret_cast<const double2*>(V + ca),
                *reinterpret_cast<const double2*>(W + ca));
   }
@@ -176,8 +192,9 @@ int correct_blocks(const Geo& g) {
 
 cudaError_t launch_correct(const CorrectArgs& a, cudaStream_t st) {
   const dim3 grd = correct_grid(a.g), blk(CNT);
-  if (a.fp32) k_correct<float><<<grd, blk, 0, st>>>(a);
-  else k_correct<double><<<grd, blk, 0, st>>>(a);
+  if (a.pd) k_correct<<<grd, blk, 0, st>>>(a, PSum{static_cast<const float*>(a.p), a.pd});
+  else if (a.fp32) k_correct<<<grd, blk, 0, st>>>(a, PFloat{static_cast<const float*>(a.p)});
+  else k_correct<<<grd, blk, 0, st>>>(a, PDouble{static_cast<const double*>(a.p)});
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   k_finalize<<<1, 1024, 0, st>>>(a.partials, a.nblocks, a.g, a.sc);

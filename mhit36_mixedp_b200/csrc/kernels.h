@@ -71,6 +71,7 @@ struct CorrectArgs {
   double *u, *v, *w;  // u* in, u** out (in place)
   const void* p;      // float or double pressure
   bool fp32;
+  const float* pd = nullptr;  // refinement: the FP32 correction; the pressure is p + pd
   double* partials;   // [nblocks][6]
   int nblocks;
   DevScalars* sc;

@@ -49,7 +49,7 @@ enum {
 };
 static const char* kStageNames[ST_COUNT] = {"k_tracer", "k_phase", "k_mom", "k_div_fftx", "k_fft_cols_yfwd",
                                             "k_fft_cols_zsolve", "k_fft_cols_yinv", "k_fftx_inv",
-                                            "refine(k_residual+5 passes+k_combine)", "k_correct+k_finalize"};
+                                            "refine(k_residual+5 passes)", "k_correct+k_finalize"};
 
 struct mhit_ctx {
   mhit_params prm;
@@ -261,7 +261,8 @@ static int enqueue_stage(mhit_ctx* c, int stage, double alpha, double beta, int 
         MHIT_CUDA_TRY(poisson_stage(a, stage - ST_XFWD, c->st));
         return MHIT_OK;
       }
-      // one FP64 residual sweep: r -> P2, L_h delta = r in FP32 (delta -> P2), P64 = P + P2
+      // one FP64 residual sweep: r -> P2, L_h delta = r in FP32 (delta -> P2); the projection
+      // reads p = P + P2
       ResidArgs r;
       r.g = c->g;
       r.u = c->U[nxt];
@@ -274,7 +275,6 @@ static int enqueue_stage(mhit_ctx* c, int stage, double alpha, double beta, int 
       a.rreal = c->P2;
       a.p = c->P2;
       for (int s = 0; s < PSTAGE_COUNT; ++s) MHIT_CUDA_TRY(poisson_stage(a, s, c->st));
-      MHIT_CUDA_TRY(launch_combine(static_cast<const float*>(c->P), c->P2, c->P64, c->n, c->st));
       return MHIT_OK;
     }
     case ST_CORRECT: {
@@ -283,9 +283,9 @@ static int enqueue_stage(mhit_ctx* c, int stage, double alpha, double beta, int 
       a.u = c->U[nxt];
       a.v = c->V[nxt];
       a.w = c->W[nxt];
-      const bool refined = p.poisson == MHIT_POISSON_FP32_REFINED;
-      a.p = refined ? static_cast<const void*>(c->P64) : c->P;
-      a.fp32 = p.poisson == MHIT_POISSON_FP32;
+      a.p = c->P;
+      a.fp32 = p.poisson != MHIT_POISSON_FP64;
+      a.pd = p.poisson == MHIT_POISSON_FP32_REFINED ? c->P2 : nullptr;
       a.partials = c->partials;
       a.nblocks = c->nblk;
       a.sc = c->sc;
@@ -752,7 +752,8 @@ int mhit_download_fields(mhit_ctx* c, double* u, double* v, double* w, double* p
   if (phi) MHIT_CUDA_TRY(cudaMemcpyAsync(phi, c->PHI[c->cur], fb, cudaMemcpyDeviceToHost, c->st));
   if (p) {
     const double* src = static_cast<const double*>(c->P);
-    if (c->P64) {
+    if (c->P64) {  // refinement: materialise p = P + P2 in FP64
+      MHIT_CUDA_TRY(launch_combine(static_cast<const float*>(c->P), c->P2, c->P64, c->n, c->st));
       src = c->P64;
     } else if (tsize(c) == 4) {
       if (!c->Pw) MHIT_CUDA_TRY(cudaMalloc(&c->Pw, fb));
@@ -879,7 +880,7 @@ std::vector<CkptArray> ckpt_arrays(mhit_ctx* c) {
     a.push_back({c->RPHI, fb});
   }
   a.push_back({c->P, c->n * tsize(c)});
-  if (c->P64) a.push_back({c->P64, fb});
+  if (c->P2) a.push_back({c->P2, c->n * sizeof(float)});  // refinement: the correction
   return a;
 }
 
