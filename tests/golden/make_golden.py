@@ -1,7 +1,8 @@
 """Generate the golden fixtures under tests/golden (run in a checkout that has the reference).
 
-1. tg128_d2z.json -- the reference's own published Taylor-Green Re=1600 dissipation curve at
-   128^3 (val/cudec_128_d2z.txt of aroccon/MHIT36_mixedp: t, epsilon; nu = 6.25e-4, dt = 2e-4,
+1. tg128_d2z.json, tg512_d2z.json -- the reference's own published Taylor-Green Re=1600
+   dissipation curves at 128^3 and 512^3 (val/cudec_128_d2z.txt and val/cudec_512_d2z.txt of
+   aroccon/MHIT36_mixedp: t, epsilon; nu = 6.25e-4, dt = 2e-4,
    val/comparison_diss.m:5,10), plus how epsilon was computed by the reference's
    post-processor (post/compute_diss/main.f90:7-11,72-117: central differences with
    dx = lx/(nx-1), lx = 2*pi where pi=3.14159265358979 is a default-REAL literal, i.e. the
@@ -23,20 +24,20 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
 
-def tg_curve(ref):
+def tg_curve(ref, n):
     rows = []
-    with open(os.path.join(ref, "val", "cudec_128_d2z.txt")) as f:
+    with open(os.path.join(ref, "val", f"cudec_{n}_d2z.txt")) as f:
         for line in f:
             parts = line.split()
             if len(parts) >= 2:
                 rows.append([float(parts[0]), float(parts[1])])
     out = {
-        "source": "val/cudec_128_d2z.txt (aroccon/MHIT36_mixedp)",
-        "nx": 128, "nu": 6.25e-4, "dt": 2e-4, "forcing": 0.0,
+        "source": f"val/cudec_{n}_d2z.txt (aroccon/MHIT36_mixedp)",
+        "nx": n, "nu": 6.25e-4, "dt": 2e-4, "forcing": 0.0,
         "postproc_dx": "lx/(nx-1) with lx = 2*float32(pi)",
         "t_eps": rows,
     }
-    with open(os.path.join(HERE, "tg128_d2z.json"), "w") as f:
+    with open(os.path.join(HERE, f"tg{n}_d2z.json"), "w") as f:
         json.dump(out, f, indent=1)
 
 
@@ -80,6 +81,7 @@ def oracle_fixtures():
 
 if __name__ == "__main__":
     ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
-    tg_curve(ref)
+    tg_curve(ref, 128)
+    tg_curve(ref, 512)
     oracle_fixtures()
     print("written", os.listdir(HERE))
