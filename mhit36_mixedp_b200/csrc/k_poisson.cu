@@ -184,15 +184,18 @@ k_fftx_inv(const Cx<T>* __restrict__ spec, T* __restrict__ p, const Cx<T>* __res
 // same strided element set) stay in registers: 4 shared-memory passes over the tile per
 // transform of three stages instead of 8.
 //
-// Tiles are 8 columns wide in both precisions (64-byte rows of float complex: whole DRAM
-// sectors, one butterfly per thread and stage for the 512-point transforms).  The FP64 z solve
-// keeps two transforms' worth of butterflies in registers and runs one block per SM without
-// spills, the FP32 one two blocks; the single transforms of up to 512 points fit two blocks per
-// SM.  Measured at 512^3 FP32: 16-column tiles 0.603 ms for the z solve, 8 columns 0.551 ms,
-// 4 columns 0.68 ms.
+// Tiles are 8 columns wide (64-byte rows of float complex: whole DRAM sectors, one butterfly
+// per thread and stage for the 512-point transforms), except for the FP64 512-point z solve.
+// The z solve keeps two transforms' worth of butterflies in registers (128 per thread in FP64);
+// the FP32 one runs two blocks per SM, the single transforms of up to 512 points fit two blocks
+// per SM.  Measured at 512^3 FP32: 16-column tiles 0.603 ms for the z solve, 8 columns
+// 0.551 ms, 4 columns 0.68 ms.  The FP64 512-point z solve runs 4-column tiles (64-byte rows)
+// of 256 threads, two blocks per SM, so one block's loads overlap the other's butterflies:
+// 0.865 ms against 0.97 ms for one 8-column block of 512 threads per SM (2 columns: 1.24 ms).
 template <typename T, int N, int MODE> struct ColTile {
-  static constexpr int B = 8;
-  static constexpr int MINB = (N >= 1024 || (MODE == 2 && sizeof(T) == 8)) ? 1 : 2;
+  static constexpr bool Z64 = MODE == 2 && N == 512 && sizeof(T) == 8;
+  static constexpr int B = Z64 ? 4 : 8;
+  static constexpr int MINB = Z64 ? 2 : ((N >= 1024 || (MODE == 2 && sizeof(T) == 8)) ? 1 : 2);
 };
 
 template <typename T, int N, int MODE>
