@@ -330,6 +330,66 @@ def run_ensemble(args):
     return 0
 
 
+def run_large_ns(args):
+    """1024^3 NS (no phase field), FP32 against FP64 Poisson, nu = 8e-4: the seeded random
+    solenoidal velocity (seed 4, 0 < |k| <= 4, unit rms) synthesised on the device (its host
+    version would need tens of GB of host memory at this size), ABC forcing on."""
+    from mhit36_mixedp_b200 import Params, Solver
+    n = 1024 if args.n == 512 else args.n
+    prm = dict(nx=n, dt=2e-4, mu=8e-4, rho=1.0, f1=1.0, f2=1.0, f3=1.0, k0=2.0)
+    res = {}
+    for mode in ("fp32", "fp64"):
+        with Solver(Params(poisson=mode, **prm)) as s:
+            s.init_solenoidal(seed=4, kmax=4)
+            s.step(max(args.warmup, 3))
+            with Clocks(0) as clk:
+                ms = s.time_steps(args.steps)
+            s.step(0)
+            prof = s.profile_step()
+            dg = s.diagnostics()
+        res[mode] = {"ms_per_step": ms / args.steps, "stages_ms": prof, "maxdiv": dg["maxdiv"], "ke": dg["ke"],
+                     "clocks": clk.summary()}
+    peak, kind = peaks()
+    npts = n ** 3
+    ns_bytes = {"fp32": 192, "fp64": 216}  # NS step model: 192 / 216 B per point
+    for mode in res:
+        res[mode]["step_roofline_frac"] = ns_bytes[mode] * npts / (res[mode]["ms_per_step"] * 1e-3) / 1e9 / peak
+    line = {"metric": f"ms/timestep {n}^3 NS, 1 B200, FP32 vs FP64 Poisson", "value": res["fp32"]["ms_per_step"],
+            "unit": "ms/timestep", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
+            "data": "synthetic (seeded solenoidal modes 0<|k|<=4, seed 4, built on the device)", "dtype": "f64+f32",
+            "config": {"workload": f"NS {n}^3, nu=8e-4, dt=2e-4", "l2": "inputs larger than L2"},
+            "fp64_ms_per_step": res["fp64"]["ms_per_step"], "detail": res, "peak_kind": kind}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_tracers(args):
+    """512^3 NS+ACDI with 1e6 tracers, FP64 Poisson, both interpolation modes."""
+    from mhit36_mixedp_b200 import Params, Solver, synth
+    n = args.n
+    prm, u, v, w, phi = workload(n)
+    npart = 1_000_000
+    part = synth.uniform_particles(npart, 3)
+    prm = dict(prm, partflag=1, npart=npart)
+    res = {}
+    for interp in ("linear1d", "trilinear"):
+        with Solver(Params(poisson="fp64", interp=interp, **prm)) as s:
+            s.upload(u, v, w, phi)
+            s.upload_particles(part)
+            s.step(max(args.warmup, 3))
+            ms = s.time_steps(args.steps)
+            s.step(0)
+            prof = [s.profile_step() for _ in range(3)]
+        tr = statistics.mean(p["k_tracer"] for p in prof if "k_tracer" in p) if "k_tracer" in prof[0] else None
+        res[interp] = {"ms_per_step": ms / args.steps, "tracer_stage_ms": tr}
+    line = {"metric": f"ms/timestep {n}^3 NS+ACDI + 1e6 tracers, 1 B200, FP64 Poisson",
+            "value": res["linear1d"]["ms_per_step"], "unit": "ms/timestep", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": False, "data": "synthetic", "dtype": "f64",
+            "config": {"workload": f"NS+ACDI {n}^3 + 1e6 uniform tracers (seed 3)"}, "detail": res}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)

@@ -115,6 +115,30 @@ void mhit_destroy(mhit_ctx* ctx);
  * the Euler first step. */
 int mhit_upload_fields(mhit_ctx* ctx, const double* u, const double* v, const double* w, const double* phi);
 
+/* Initial conditions built on the device (the O(N^3) work of multi/main.f90:322-415 and of the
+ * seeded benchmark fields; the one-dimensional tables are computed on the host).
+ *
+ * mhit_init_taylor_green: u = sin(x - dx/2) cos(y) cos(z), v = -cos(x) sin(y - dx/2) cos(z),
+ *   w = 0 on the accumulated coordinates x(i) = x(i-1) + dx with the y/z labelling of
+ *   yz_shift (multi/main.f90:210-214, 324-337).  Replaces u, v, w.
+ * mhit_init_velocity_modes: u = Re sum_m c_m exp(i (m_x tx + m_y ty + m_z tz)) over the index
+ *   wavenumbers -kmax..kmax per axis (kmax 1..16), with the index phases tx = i 2pi/nx,
+ *   ty = (j + yz_shift) 2pi/ny, tz = (k + yz_shift) 2pi/nz and each component's own phase half a
+ *   cell back (its face position: u at tx - pi/nx, ...), then scaled to the given rms.  In a
+ *   cube the phases are the coordinates; in a box of nx dx by ny dx by nz dx the index
+ *   wavenumber m_y is the physical m_y nx/ny.  modes holds 3 (2kmax+1)^3 complex amplitudes as
+ *   (re, im) pairs, ordered [component][kz][ky][kx] with m from -kmax; the caller draws them (a
+ *   seeded random solenoidal field: Gaussian amplitudes with k.c = 0).  Replaces u, v, w.
+ * mhit_init_drops: phi = 0.5 (1 - tanh((r - radius)/(2 eps))), eps = epsr dx, r the periodic
+ *   minimum-image distance in the box nx dx by ny dx by nz dx to the nearest of ndrops centres
+ *   (x, y, z triples), cells at x = i dx, y = (j + yz_shift) dx, z = (k + yz_shift) dx; one
+ *   centre at (pi, pi, pi) is the centred drop of multi/main.f90:370-382.  Replaces phi (needs
+ *   phiflag = 1); the velocity keeps its values.
+ * Each resets rhs_o, rhsphi_o, gumax = 1 and the Euler first step like mhit_upload_fields. */
+int mhit_init_taylor_green(mhit_ctx* ctx);
+int mhit_init_velocity_modes(mhit_ctx* ctx, int kmax, const double* modes, double rms);
+int mhit_init_drops(mhit_ctx* ctx, int ndrops, const double* centres, double radius);
+
 /* Tracer table, column-major (npart, 12) as the reference's part(nplocmax,12)
  * (multi/particles.f90:11-22): tag, x, y, z, u, v, w, phi, u1, v1, w1, phi1. */
 int mhit_upload_particles(mhit_ctx* ctx, const double* part, int npart);
@@ -138,6 +162,16 @@ int mhit_diagnostics(mhit_ctx* ctx, mhit_diag* d);
  * the file at path into field fieldn (readfield/readfield_restart, :107-318). */
 int mhit_write_field(mhit_ctx* ctx, const char* dir, int t, int fieldn);
 int mhit_read_field(mhit_ctx* ctx, const char* path, int fieldn);
+
+/* Shell-summed kinetic-energy spectrum of the current velocity (no reference counterpart; the
+ * reference's post-processing has dissipation and 1-D profiles only):
+ *   E[k] = 1/2 sum over |kappa| in [k - 1/2, k + 1/2) of |u_kappa|^2 + |v_kappa|^2 + |w_kappa|^2,
+ * u_kappa the FFT of the stored velocity (mean removed) divided by nx ny nz, kappa in units of
+ * 2 pi / Lx (kappa_y = m_y nx/ny, kappa_z = m_z nx/nz), for k = 0..nbins-1 (nbins 1..4096).
+ * Shells beyond nbins are dropped; with all shells, sum E = KE of mhit_diagnostics (Parseval).
+ * Uses the FP64 transform passes of the Poisson solver (in the FP32 modes on an FP64 buffer
+ * allocated on first use); the last bits depend on the order of shared-memory atomics. */
+int mhit_energy_spectrum(mhit_ctx* ctx, double* E, int nbins);
 
 /* Exact-resume checkpoint (no reference counterpart: the reference restarts from the field
  * files, multi/readwrite.f90:107-318, with an Euler step because rhs_o is not in them,

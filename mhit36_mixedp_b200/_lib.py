@@ -66,6 +66,10 @@ SIGNATURES = {
     "mhit_init": (_c.c_int, [_P(MhitParams), _P(_c.c_void_p)]),
     "mhit_destroy": (None, [_c.c_void_p]),
     "mhit_upload_fields": (_c.c_int, [_c.c_void_p, _dp, _dp, _dp, _dp]),
+    "mhit_init_taylor_green": (_c.c_int, [_c.c_void_p]),
+    "mhit_init_velocity_modes": (_c.c_int, [_c.c_void_p, _c.c_int, _dp, _c.c_double]),
+    "mhit_init_drops": (_c.c_int, [_c.c_void_p, _c.c_int, _dp, _c.c_double]),
+    "mhit_energy_spectrum": (_c.c_int, [_c.c_void_p, _dp, _c.c_int]),
     "mhit_upload_particles": (_c.c_int, [_c.c_void_p, _dp, _c.c_int]),
     "mhit_download_particles": (_c.c_int, [_c.c_void_p, _dp, _c.c_int]),
     "mhit_step": (_c.c_int, [_c.c_void_p, _c.c_int]),

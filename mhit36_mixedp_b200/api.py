@@ -12,6 +12,7 @@ library's status code (the reference ``stop``s on CFL > 7, multi/main.f90:1006 -
 from __future__ import annotations
 
 import ctypes
+import math
 import dataclasses
 
 import numpy as np
@@ -188,6 +189,35 @@ class Solver:
             phi = self._field(phi, "phi")
         _check(self._lib.mhit_upload_fields(self._ctx, _dptr(u), _dptr(v), _dptr(w), _dptr(phi)))
 
+    # ------------------------------------------------ initial conditions built on the device
+    def init_taylor_green(self):
+        """Taylor-Green velocity of multi/main.f90:324-337, synthesised on the device."""
+        _check(self._lib.mhit_init_taylor_green(self._ctx))
+
+    def init_velocity_modes(self, modes, rms: float = 1.0):
+        """u, v, w = Re sum_k c_k exp(i k.x) over the (2 kmax + 1)^3 integer wavenumbers of
+        ``modes`` (complex, shape (3, K, K, K) ordered [component][kz][ky][kx], k from -kmax),
+        each component at its face position and scaled to ``rms``; synthesised on the device."""
+        m = np.asarray(modes, dtype=np.complex128)
+        if m.ndim != 4 or m.shape[0] != 3 or not (m.shape[1] == m.shape[2] == m.shape[3]) or m.shape[1] % 2 == 0:
+            raise MhitArgError(_lib.MHIT_ERR_ARG, "modes must be complex (3, K, K, K) with K odd")
+        kmax = (m.shape[1] - 1) // 2
+        flat = np.ascontiguousarray(m).view(np.float64).ravel()
+        _check(self._lib.mhit_init_velocity_modes(self._ctx, kmax, _dptr(flat), float(rms)))
+
+    def init_solenoidal(self, seed: int, kmax: int = 4, rms: float = 1.0):
+        """The seeded random solenoidal velocity of ``synth.solenoidal_velocity`` (same seed, same
+        amplitudes), synthesised on the device instead of the host."""
+        from . import synth
+        p = self.params
+        self.init_velocity_modes(synth.solenoidal_modes(seed, kmax, (1.0, p.nx / p.ny, p.nx / p.nz)), rms)
+
+    def init_drops(self, centres, radius: float):
+        """phi of drops of radius ``radius`` at ``centres`` ((n, 3) x, y, z): the nearest centre by
+        minimum image, eps = epsr dx (``synth.drops_phi`` / multi/main.f90:370-382), on the device."""
+        c = np.ascontiguousarray(np.asarray(centres, dtype=np.float64).reshape(-1, 3))
+        _check(self._lib.mhit_init_drops(self._ctx, c.shape[0], _dptr(c), float(radius)))
+
     def upload_particles(self, part):
         """Tracer table (npart, 12): tag, x, y, z, u, v, w, phi, u1, v1, w1, phi1."""
         part = np.asfortranarray(part, dtype=np.float64)
@@ -226,6 +256,16 @@ class Solver:
             "nstep": d.nstep, "gumax": d.gumax, "cfl": d.cfl, "mean": tuple(d.mean),
             "maxdiv": d.maxdiv, "ke": d.ke, "dissipation": d.dissipation, "flags": d.flags,
         }
+
+    def energy_spectrum(self, nbins: int | None = None) -> np.ndarray:
+        """E(k), k = 0..nbins-1: shell sums of 1/2 |u_k|^2 over the FP64 FFT of the velocity
+        (mean removed, normalised by nx ny nz; sum E = KE).  Default: every shell of the box."""
+        if nbins is None:
+            nx, ny, nz = self.params.nx, self.params.ny, self.params.nz
+            nbins = int(math.ceil(math.sqrt(3.0) * max(nx, ny, nz) / 2)) + 2
+        out = np.zeros(int(nbins), dtype=np.float64)
+        _check(self._lib.mhit_energy_spectrum(self._ctx, _dptr(out), int(nbins)))
+        return out
 
     # -------------------------------------------------------------- field files
     def writefield(self, outdir: str, t: int, fieldn: int):

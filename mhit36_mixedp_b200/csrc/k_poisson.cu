@@ -36,9 +36,9 @@ template <> __device__ __forceinline__ void store2<float>(float* p, float a, flo
 template <typename T, int M> __host__ __device__ constexpr int xpass_threads() { return fft_threads<M, Tile<T>::B>(); }
 
 // ------------------------------------------------------------------ forward x + divergence
-// RESID: transform the real FP32 field `rr` (the residual of the refinement sweep) instead of
-// the divergence of u*.
-template <typename T, int M, bool RESID>
+// SRC 0: the divergence of u*; SRC 1: the real FP32 field `rr` (the residual of the refinement
+// sweep); SRC 2: the real FP64 field `u` (the energy spectrum of a velocity component).
+template <typename T, int M, int SRC>
 __global__ void __launch_bounds__(xpass_threads<T, M>())
 k_div_fftx(const double* __restrict__ u, const double* __restrict__ v, const double* __restrict__ w,
            const float* __restrict__ rr, Cx<T>* __restrict__ spec, const Cx<T>* __restrict__ twx, Geo g,
@@ -55,8 +55,12 @@ k_div_fftx(const double* __restrict__ u, const double* __restrict__ v, const dou
     const int b = e / M, n = e - b * M;
     const int line = min(line0 + b, nlines - 1);  // a tail tile repeats the last line
     Cx<T> z;
-    if constexpr (RESID) {
+    if constexpr (SRC == 1) {
       const float2 r2 = __ldg(reinterpret_cast<const float2*>(rr + (size_t)line * nx + 2 * n));
+      z.x = (T)r2.x;
+      z.y = (T)r2.y;
+    } else if constexpr (SRC == 2) {
+      const double2 r2 = __ldg(reinterpret_cast<const double2*>(u + (size_t)line * nx + 2 * n));
       z.x = (T)r2.x;
       z.y = (T)r2.y;
     } else {
@@ -338,7 +342,7 @@ template <typename T, int M>
 static cudaError_t launch_xfwd_m(const PoissonArgs& a, cudaStream_t st) {
   constexpr int B = Tile<T>::B;
   const size_t smem = (size_t)(M + 1) * B * sizeof(Cx<T>);
-  auto kern = a.rreal ? k_div_fftx<T, M, true> : k_div_fftx<T, M, false>;
+  auto kern = a.rreal ? k_div_fftx<T, M, 1> : (a.real64 ? k_div_fftx<T, M, 2> : k_div_fftx<T, M, 0>);
   cudaError_t e = prep_smem(kern, smem);
   if (e != cudaSuccess) return e;
   const int nlines = a.g.ny * a.g.nz;
@@ -440,6 +444,7 @@ static cudaError_t poisson_stage_t(const PoissonArgs& a, int stage, cudaStream_t
     case PSTAGE_ZSOLVE: return launch_cols<T, 2>(a, 2, st);
     case PSTAGE_YINV: return launch_cols<T, 1>(a, 1, st);
     case PSTAGE_XINV: return launch_xinv<T>(a, st);
+    case PSTAGE_ZFWD: return launch_cols<T, 0>(a, 2, st);
   }
   return cudaErrorInvalidValue;
 }

@@ -9,6 +9,7 @@ int set_cuda_error(cudaError_t e, const char* expr, const char* file, int line);
 
 // ---------------------------------------------------------------- Poisson
 enum { PSTAGE_XFWD = 0, PSTAGE_YFWD, PSTAGE_ZSOLVE, PSTAGE_YINV, PSTAGE_XINV, PSTAGE_COUNT };
+constexpr int PSTAGE_ZFWD = PSTAGE_COUNT + 1;  // forward z transform alone (energy spectrum), not a step stage
 
 struct PoissonArgs {
   Geo g;
@@ -21,6 +22,7 @@ struct PoissonArgs {
   double cdiv;  // rho*dxi/dt
   double ntot;  // nx*ny*nz
   const float* rreal = nullptr;  // non-null: x-forward transforms this FP32 field (refinement)
+  bool real64 = false;           // x-forward transforms the FP64 field u (energy spectrum)
 };
 
 // FP64 residual of the FP32 solve: r = rho/dt div(u*) - L_h p (7-point Laplacian), stored as
@@ -126,5 +128,37 @@ int label_chunks(int n);
 cudaError_t launch_label_components(const LabelArgs& a, cudaStream_t st);  // init, merge, flatten, count
 cudaError_t launch_label_number(const LabelArgs& a, cudaStream_t st);      // counts must hold offsets
 cudaError_t launch_label_stats(const LabelArgs& a, cudaStream_t st);
+
+// ---------------------------------------------------------------- initial conditions
+cudaError_t launch_init_tg(double* u, double* v, double* w, const double* tab, int nx, int ny, int nz,
+                           cudaStream_t st);
+struct ModeArgs {
+  int nx, ny, nz, K;             // K = 2 kmax + 1 wavenumbers per axis
+  const Cx<double>* cm;          // mode amplitudes [kz][ky][kx] of one component
+  const Cx<double>* ex;          // exp(i k x) tables [nx][K], [ny][K], [nz][K]
+  const Cx<double>* ey;
+  const Cx<double>* ez;
+  Cx<double>* A;                 // scratch [K][K][nx]
+  Cx<double>* Bt;                // scratch [K][ny][nx]
+  double* f;                     // output field
+  double* partials;              // modes_partials(nx, ny) sums of f^2
+};
+int modes_partials(int nx, int ny);
+cudaError_t launch_init_modes(const ModeArgs& a, cudaStream_t st);
+cudaError_t launch_scale(double* f, size_t n, double s, cudaStream_t st);
+struct DropInitArgs {
+  double* phi;
+  const double* centres;  // [nd][3]
+  int nd, nx, ny, nz, s;
+  double dx, lx, ly, lz, radius, eps;
+};
+cudaError_t launch_init_drops(const DropInitArgs& a, cudaStream_t st);
+
+// ---------------------------------------------------------------- energy spectrum
+int spectrum_blocks(const Geo& g);
+// adds the shell energies of one component's FP64 half spectrum to E[0..nbins) (device);
+// partials holds spectrum_blocks(g) * nbins doubles
+cudaError_t launch_spectrum_bin(const Cx<double>* spec, const Geo& g, const DevScalars* sc, int comp, int nbins,
+                                double* partials, double* E, cudaStream_t st);
 
 }  // namespace mhit

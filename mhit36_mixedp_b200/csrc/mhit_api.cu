@@ -70,6 +70,9 @@ struct mhit_ctx {
   size_t lab_acc_bytes = 0;
   void* spec = nullptr;
   void *twx = nullptr, *twy = nullptr, *twz = nullptr;
+  void* spec64 = nullptr;  // energy spectrum in the FP32 modes: an FP64 half spectrum, grown lazily
+  size_t spec64_bytes = 0;
+  void* tw64[3] = {};      // ... and FP64 twiddles
   double *k2x = nullptr, *k2y = nullptr, *k2z = nullptr;
   double* tabs = nullptr;
   double* partials = nullptr;
@@ -464,6 +467,8 @@ void mhit_destroy(mhit_ctx* c) {
   cudaFree(c->lab_small);
   cudaFree(c->lab_acc);
   cudaFree(c->spec);
+  cudaFree(c->spec64);
+  for (void* t : c->tw64) cudaFree(t);
   cudaFree(c->twx);
   cudaFree(c->twy);
   cudaFree(c->twz);
@@ -1098,6 +1103,197 @@ int mhit_label_drops(mhit_ctx* c, double thresh, int connectivity, mhit_drop* dr
 }
 
 // ------------------------------------------------------------------ test hooks
+// ------------------------------------------------------------------ initial conditions on the device
+namespace {
+int to_device(DevBuf& b, const std::vector<double>& v, cudaStream_t st) {
+  MHIT_CUDA_TRY(cudaMalloc(&b.p, v.size() * sizeof(double)));
+  MHIT_CUDA_TRY(cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+  return MHIT_OK;
+}
+}  // namespace
+
+int mhit_init_taylor_green(mhit_ctx* c) {
+  int rc;
+  if ((rc = check_ctx(c))) return rc;
+  const int nx = c->prm.nx, ny = c->prm.ny, nz = c->prm.nz, s = c->prm.yz_shift;
+  const double dx = c->g.dx;
+  // multi/main.f90:324-337 on the accumulated coordinates x(i) = x(i-1) + dx (:210-214), y and z
+  // read s entries on (the halo-shifted labelling)
+  const std::vector<double> xa = grid_coords(std::max(nx, std::max(ny, nz)) + 1, dx);
+  std::vector<double> tab;
+  tab.reserve(2 * (size_t)nx + 2 * (size_t)ny + nz);
+  for (int i = 0; i < nx; ++i) tab.push_back(std::sin(xa[i] - dx / 2));
+  for (int i = 0; i < nx; ++i) tab.push_back(std::cos(xa[i]));
+  for (int j = 0; j < ny; ++j) tab.push_back(std::sin(xa[j + s] - dx / 2));
+  for (int j = 0; j < ny; ++j) tab.push_back(std::cos(xa[j + s]));
+  for (int k = 0; k < nz; ++k) tab.push_back(std::cos(xa[k + s]));
+  DevBuf dt;
+  if ((rc = to_device(dt, tab, c->st))) return rc;
+  c->cur = 0;
+  MHIT_CUDA_TRY(launch_init_tg(c->U[0], c->V[0], c->W[0], static_cast<const double*>(dt.p), nx, ny, nz, c->st));
+  MHIT_CUDA_TRY(cudaStreamSynchronize(c->st));
+  return reset_history(c);
+}
+
+int mhit_init_velocity_modes(mhit_ctx* c, int kmax, const double* modes, double rms) {
+  int rc;
+  if ((rc = check_ctx(c))) return rc;
+  if (kmax < 1 || kmax > 16 || !modes) return set_error(MHIT_ERR_ARG, "kmax must be 1..16 and modes non-null");
+  if (!(rms > 0.0)) return set_error(MHIT_ERR_ARG, "rms must be positive");
+  const int nx = c->prm.nx, ny = c->prm.ny, nz = c->prm.nz, s = c->prm.yz_shift;
+  const int K = 2 * kmax + 1;
+  const size_t k3 = (size_t)K * K * K;
+  const double lx = 8.0 * std::atan(1.0);
+  // scratch: the three components' modes, the exp(i k x) tables, A, B and the partial sums
+  std::vector<double> cm(modes, modes + 2 * 3 * k3);
+  DevBuf dcm, dA, dB, dpart;
+  if ((rc = to_device(dcm, cm, c->st))) return rc;
+  MHIT_CUDA_TRY(cudaMalloc(&dA.p, (size_t)K * K * nx * sizeof(Cx<double>)));
+  MHIT_CUDA_TRY(cudaMalloc(&dB.p, (size_t)K * ny * nx * sizeof(Cx<double>)));
+  const int npart = modes_partials(nx, ny);
+  MHIT_CUDA_TRY(cudaMalloc(&dpart.p, (size_t)npart * sizeof(double)));
+  std::vector<double> part(npart);
+  double* dst[3] = {c->U[0], c->V[0], c->W[0]};
+  c->cur = 0;
+  for (int comp = 0; comp < 3; ++comp) {
+    // index phases theta = (i + shift) 2 pi/n per axis (x: shift 0, y and z: yz_shift), the
+    // component's own axis half a cell back (its face position, multi/main.f90:331); for a box of
+    // nx dx by ny dx by nz dx the index wavenumber m_y is the physical m_y nx/ny
+    auto table = [&](int n, int shift, bool face) {
+      const double h = lx / n;
+      std::vector<double> t(2 * (size_t)n * K);
+      for (int i = 0; i < n; ++i) {
+        double x = (double)(i + shift) * h;
+        if (face) x = x - h / 2;
+        for (int q = 0; q < K; ++q) {
+          const double a = x * (double)(q - kmax);
+          t[2 * ((size_t)i * K + q)] = std::cos(a);
+          t[2 * ((size_t)i * K + q) + 1] = std::sin(a);
+        }
+      }
+      return t;
+    };
+    DevBuf dex, dey, dez;
+    if ((rc = to_device(dex, table(nx, 0, comp == 0), c->st))) return rc;
+    if ((rc = to_device(dey, table(ny, s, comp == 1), c->st))) return rc;
+    if ((rc = to_device(dez, table(nz, s, comp == 2), c->st))) return rc;
+    ModeArgs a;
+    a.nx = nx;
+    a.ny = ny;
+    a.nz = nz;
+    a.K = K;
+    a.cm = static_cast<const Cx<double>*>(dcm.p) + (size_t)comp * k3;
+    a.ex = static_cast<const Cx<double>*>(dex.p);
+    a.ey = static_cast<const Cx<double>*>(dey.p);
+    a.ez = static_cast<const Cx<double>*>(dez.p);
+    a.A = static_cast<Cx<double>*>(dA.p);
+    a.Bt = static_cast<Cx<double>*>(dB.p);
+    a.f = dst[comp];
+    a.partials = static_cast<double*>(dpart.p);
+    MHIT_CUDA_TRY(launch_init_modes(a, c->st));
+    MHIT_CUDA_TRY(cudaMemcpyAsync(part.data(), dpart.p, part.size() * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    MHIT_CUDA_TRY(cudaStreamSynchronize(c->st));  // the tables are freed at the end of this iteration
+    double ss = 0.0;
+    for (double v : part) ss += v;
+    const double mean2 = ss / (double)c->n;
+    if (!(mean2 > 0.0)) return set_error(MHIT_ERR_ARG, "the modes give a zero field");
+    MHIT_CUDA_TRY(launch_scale(dst[comp], c->n, rms / std::sqrt(mean2), c->st));
+  }
+  MHIT_CUDA_TRY(cudaStreamSynchronize(c->st));
+  return reset_history(c);
+}
+
+int mhit_init_drops(mhit_ctx* c, int ndrops, const double* centres, double radius) {
+  int rc;
+  if ((rc = check_ctx(c))) return rc;
+  if (!c->prm.phiflag) return set_error(MHIT_ERR_STATE, "context was created with phiflag=0");
+  if (ndrops < 1 || !centres || !(radius > 0.0)) return set_error(MHIT_ERR_ARG, "need ndrops >= 1, centres, radius > 0");
+  const int nx = c->prm.nx, ny = c->prm.ny, nz = c->prm.nz;
+  const double lx = 8.0 * std::atan(1.0);
+  std::vector<double> cen(centres, centres + 3 * (size_t)ndrops);
+  DevBuf dc;
+  if ((rc = to_device(dc, cen, c->st))) return rc;
+  // the velocity keeps its values: make its lazily removed mean explicit first
+  k_apply_mean<<<148 * 4, 256, 0, c->st>>>(c->U[c->cur], c->V[c->cur], c->W[c->cur], c->n, c->sc);
+  MHIT_CUDA_TRY(cudaGetLastError());
+  k_clear_mean<<<1, 1, 0, c->st>>>(c->sc);
+  MHIT_CUDA_TRY(cudaGetLastError());
+  DropInitArgs a;
+  a.phi = c->PHI[c->cur];
+  a.centres = static_cast<const double*>(dc.p);
+  a.nd = ndrops;
+  a.nx = nx;
+  a.ny = ny;
+  a.nz = nz;
+  a.s = c->prm.yz_shift;
+  a.dx = c->g.dx;
+  a.lx = lx;  // the box is 2 pi along x and n dx along y and z
+  a.ly = ny == nx ? lx : a.dx * ny;
+  a.lz = nz == nx ? lx : a.dx * nz;
+  a.radius = radius;
+  a.eps = c->g.eps;  // epsr dx
+  MHIT_CUDA_TRY(launch_init_drops(a, c->st));
+  MHIT_CUDA_TRY(cudaStreamSynchronize(c->st));
+  return reset_history(c);
+}
+
+// ------------------------------------------------------------------ energy spectrum
+int mhit_energy_spectrum(mhit_ctx* c, double* E, int nbins) {
+  int rc;
+  if ((rc = check_ctx(c))) return rc;
+  if (!E || nbins < 1 || nbins > 4096) return set_error(MHIT_ERR_ARG, "nbins must be 1..4096 and E non-null");
+  const Geo& g = c->g;
+  void* spec;
+  const void *tx, *ty, *tz;
+  if (c->prm.poisson == MHIT_POISSON_FP64) {  // the Poisson spectrum is scratch between steps
+    spec = c->spec;
+    tx = c->twx;
+    ty = c->twy;
+    tz = c->twz;
+  } else {
+    if ((rc = grow_buffer(&c->spec64, &c->spec64_bytes, (size_t)g.pitch * g.ny * g.nz * sizeof(Cx<double>))))
+      return rc;
+    if (!c->tw64[0]) {
+      const int ns[3] = {g.nx, g.ny, g.nz};
+      for (int q = 0; q < 3; ++q)
+        if ((rc = upload_vec(&c->tw64[q], twiddles<double>(ns[q])))) return rc;
+    }
+    spec = c->spec64;
+    tx = c->tw64[0];
+    ty = c->tw64[1];
+    tz = c->tw64[2];
+  }
+  DevBuf dpart, dE;
+  MHIT_CUDA_TRY(cudaMalloc(&dpart.p, (size_t)spectrum_blocks(g) * nbins * sizeof(double)));
+  MHIT_CUDA_TRY(cudaMalloc(&dE.p, (size_t)nbins * sizeof(double)));
+  MHIT_CUDA_TRY(cudaMemsetAsync(dE.p, 0, (size_t)nbins * sizeof(double), c->st));
+  const double* fields[3] = {c->U[c->cur], c->V[c->cur], c->W[c->cur]};
+  for (int comp = 0; comp < 3; ++comp) {
+    PoissonArgs a;
+    a.g = g;
+    a.fp32 = false;
+    a.u = fields[comp];
+    a.v = a.w = nullptr;
+    a.real64 = true;
+    a.spec = spec;
+    a.p = nullptr;
+    a.twx = tx;
+    a.twy = ty;
+    a.twz = tz;
+    a.k2x = a.k2y = a.k2z = nullptr;
+    a.cdiv = 0.0;
+    a.ntot = (double)c->n;
+    MHIT_CUDA_TRY(poisson_stage(a, PSTAGE_XFWD, c->st));
+    MHIT_CUDA_TRY(poisson_stage(a, PSTAGE_YFWD, c->st));
+    MHIT_CUDA_TRY(poisson_stage(a, PSTAGE_ZFWD, c->st));
+    MHIT_CUDA_TRY(launch_spectrum_bin(static_cast<const Cx<double>*>(spec), g, c->sc, comp, nbins,
+                                      static_cast<double*>(dpart.p), static_cast<double*>(dE.p), c->st));
+  }
+  MHIT_CUDA_TRY(cudaMemcpyAsync(E, dE.p, (size_t)nbins * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  MHIT_CUDA_TRY(cudaStreamSynchronize(c->st));
+  return MHIT_OK;
+}
+
 int mhit_debug_run_stage(mhit_ctx* c, int stage) {
   int rc;
   if ((rc = check_ctx(c))) return rc;

@@ -88,6 +88,30 @@ module mhit_gpu
       type(c_ptr), value :: phi
     end function
 
+    ! initial conditions built on the device (multi/main.f90:322-415 and the seeded fields)
+    integer(c_int) function mhit_init_taylor_green(ctx) bind(C, name="mhit_init_taylor_green")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ctx
+    end function
+
+    ! modes: 3*(2*kmax+1)**3 complex amplitudes, [component][kz][ky][kx] with k from -kmax
+    integer(c_int) function mhit_init_velocity_modes(ctx, kmax, modes, rms) bind(C, name="mhit_init_velocity_modes")
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: kmax
+      real(c_double), dimension(*), intent(in) :: modes
+      real(c_double), value :: rms
+    end function
+
+    ! centres(3,ndrops): x, y, z of each drop
+    integer(c_int) function mhit_init_drops(ctx, ndrops, centres, radius) bind(C, name="mhit_init_drops")
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: ndrops
+      real(c_double), dimension(*), intent(in) :: centres
+      real(c_double), value :: radius
+    end function
+
     ! part(npart,12): tag, x, y, z, u, v, w, phi, u1, v1, w1, phi1 (multi/particles.f90:15-22)
     integer(c_int) function mhit_upload_particles(ctx, part, npart) bind(C, name="mhit_upload_particles")
       import :: c_int, c_ptr, c_double

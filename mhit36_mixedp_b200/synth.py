@@ -31,29 +31,40 @@ def _coords(n, s):
     return (np.arange(n) + s) * dx
 
 
-def solenoidal_velocity(nx, seed, kmax=4, rms=1.0, yz_shift=1, ny=None, nz=None):
-    ny = ny or nx
-    nz = nz or nx
+def solenoidal_modes(seed, kmax=4, scale=(1.0, 1.0, 1.0)):
+    """The complex amplitudes c[component][kz][ky][kx] (index wavenumbers m from -kmax) of
+    ``solenoidal_velocity``: Gaussian on 0 < |m| <= kmax, Leray-projected (k . c = 0) with the
+    physical wavenumbers k = (m_x, m_y, m_z) * scale; scale = (1, nx/ny, nx/nz) for a box of
+    nx dx by ny dx by nz dx (all ones for a cube)."""
     rng = np.random.default_rng(seed)
     ks = np.arange(-kmax, kmax + 1)
     KZ, KY, KX = np.meshgrid(ks, ks, ks, indexing="ij")
-    k2 = KX ** 2 + KY ** 2 + KZ ** 2
-    mask = (k2 > 0) & (k2 <= kmax * kmax)
+    m2 = KX ** 2 + KY ** 2 + KZ ** 2
+    mask = (m2 > 0) & (m2 <= kmax * kmax)
     c = (rng.standard_normal((3,) + KX.shape) + 1j * rng.standard_normal((3,) + KX.shape)) * mask
-    kv = np.stack([KX, KY, KZ]).astype(np.float64)
+    kv = np.stack([KX * float(scale[0]), KY * float(scale[1]), KZ * float(scale[2])])
+    k2 = (kv * kv).sum(axis=0)
     with np.errstate(invalid="ignore", divide="ignore"):
-        kdotc = (kv * c).sum(axis=0) / np.where(k2 > 0, k2, 1)
+        kdotc = (kv * c).sum(axis=0) / np.where(m2 > 0, k2, 1)
     c = c - kv * kdotc[None]
-    c = c * mask
-    dx = LX / nx
+    return c * mask
+
+
+def solenoidal_velocity(nx, seed, kmax=4, rms=1.0, yz_shift=1, ny=None, nz=None):
+    ny = ny or nx
+    nz = nz or nx
+    ks = np.arange(-kmax, kmax + 1)
+    c = solenoidal_modes(seed, kmax, (1.0, nx / ny, nx / nz))
+    # index phase theta = (i + s) 2 pi / n per axis (the physical coordinate times the lowest
+    # wavenumber of that axis); the component's own axis is sampled half a cell back
     x = _coords(nx, 0)
     y = _coords(ny, yz_shift)
     z = _coords(nz, yz_shift)
     out = []
     for comp in range(3):
-        xs = x - dx / 2 if comp == 0 else x
-        ys = y - dx / 2 if comp == 1 else y
-        zs = z - dx / 2 if comp == 2 else z
+        xs = x - (LX / nx) / 2 if comp == 0 else x
+        ys = y - (LX / ny) / 2 if comp == 1 else y
+        zs = z - (LX / nz) / 2 if comp == 2 else z
         ex = np.exp(1j * np.outer(xs, ks))   # (nx, K)
         ey = np.exp(1j * np.outer(ys, ks))   # (ny, K)
         ez = np.exp(1j * np.outer(zs, ks))   # (nz, K)

@@ -532,6 +532,27 @@ def kinetic_energy(u, v, w):
     return 0.5 * float(np.mean(u * u + v * v + w * w))
 
 
+def energy_spectrum(u, v, w, nbins):
+    """Shell-summed kinetic-energy spectrum E(k) = 1/2 sum_{round|kappa| = k} |u_kappa|^2 (+ v, w),
+    u_kappa = rfftn(u)/N over the x-half spectrum (weight 2 for 0 < kx < nx/2), kappa in units of
+    2 pi/Lx: kappa_y = m_y nx/ny, kappa_z = m_z nx/nz.  The reference has no 3-D spectrum tool;
+    this is the definition the library's mhit_energy_spectrum restates (sum E = KE, Parseval)."""
+    nz, ny, nx = u.shape
+    ntot = float(u.size)
+    kx = np.arange(nx // 2 + 1, dtype=np.float64)
+    ky = np.fft.fftfreq(ny, 1.0 / ny) * (nx / ny)
+    kz = np.fft.fftfreq(nz, 1.0 / nz) * (nx / nz)
+    kk = np.sqrt(kx[None, None, :] ** 2 + (ky[None, :, None] ** 2 + kz[:, None, None] ** 2))
+    shell = np.rint(kk).astype(np.int64)
+    wgt = np.where((kx == 0) | (2 * kx == nx), 0.5, 1.0)[None, None, :]
+    e = np.zeros(shell.shape)
+    for f in (u, v, w):
+        c = np.fft.rfftn(f) / ntot
+        e += wgt * (c.real ** 2 + c.imag ** 2)
+    keep = shell < nbins
+    return np.bincount(shell[keep].ravel(), weights=e[keep].ravel(), minlength=nbins)[:nbins]
+
+
 def taylor_green(p: Params):
     """Taylor-Green start, multi/main.f90:324-337 (u at x(i)-dx/2, reference y/z labelling)."""
     xs = grid_coords(p.nx, p.dx)
