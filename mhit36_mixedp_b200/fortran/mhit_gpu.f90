@@ -112,6 +112,14 @@ module mhit_gpu
       real(c_double), value :: radius
     end function
 
+    ! E(0:nbins-1): shell-summed kinetic-energy spectrum of the current velocity
+    integer(c_int) function mhit_energy_spectrum(ctx, E, nbins) bind(C, name="mhit_energy_spectrum")
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: ctx
+      real(c_double), dimension(*), intent(out) :: E
+      integer(c_int), value :: nbins
+    end function
+
     ! part(npart,12): tag, x, y, z, u, v, w, phi, u1, v1, w1, phi1 (multi/particles.f90:15-22)
     integer(c_int) function mhit_upload_particles(ctx, part, npart) bind(C, name="mhit_upload_particles")
       import :: c_int, c_ptr, c_double
