@@ -138,6 +138,13 @@ int mhit_upload_fields(mhit_ctx* ctx, const double* u, const double* v, const do
 int mhit_init_taylor_green(mhit_ctx* ctx);
 int mhit_init_velocity_modes(mhit_ctx* ctx, int kmax, const double* modes, double rms);
 int mhit_init_drops(mhit_ctx* ctx, int ndrops, const double* centres, double radius);
+/* The tracer table of particlegenerator (multi/particles.f90:37-76, inflag = 1) built on the
+ * device: tags 1..npart, positions uniform in the box (2 pi by ny dx by nz dx), all velocities
+ * and histories zero.  The reference draws from an unseeded RANDOM_NUMBER; here coordinate a
+ * (0 x, 1 y, 2 z) of tracer i (0-based) is L_a * (top 53 bits of
+ * splitmix64(seed + (3 i + a + 1) * 0x9E3779B97F4A7C15)) / 2^53, reproducible from the seed.
+ * Replaces the table like mhit_upload_particles (needs partflag = 1). */
+int mhit_init_particles(mhit_ctx* ctx, int npart, unsigned long long seed);
 
 /* Tracer table, column-major (npart, 12) as the reference's part(nplocmax,12)
  * (multi/particles.f90:11-22): tag, x, y, z, u, v, w, phi, u1, v1, w1, phi1. */

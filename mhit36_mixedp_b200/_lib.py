@@ -70,6 +70,7 @@ SIGNATURES = {
     "mhit_init_velocity_modes": (_c.c_int, [_c.c_void_p, _c.c_int, _dp, _c.c_double]),
     "mhit_init_drops": (_c.c_int, [_c.c_void_p, _c.c_int, _dp, _c.c_double]),
     "mhit_energy_spectrum": (_c.c_int, [_c.c_void_p, _dp, _c.c_int]),
+    "mhit_init_particles": (_c.c_int, [_c.c_void_p, _c.c_int, _c.c_ulonglong]),
     "mhit_upload_particles": (_c.c_int, [_c.c_void_p, _dp, _c.c_int]),
     "mhit_download_particles": (_c.c_int, [_c.c_void_p, _dp, _c.c_int]),
     "mhit_step": (_c.c_int, [_c.c_void_p, _c.c_int]),

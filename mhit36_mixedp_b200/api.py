@@ -218,6 +218,12 @@ class Solver:
         c = np.ascontiguousarray(np.asarray(centres, dtype=np.float64).reshape(-1, 3))
         _check(self._lib.mhit_init_drops(self._ctx, c.shape[0], _dptr(c), float(radius)))
 
+    def init_particles(self, npart: int, seed: int):
+        """Tracer table built on the device: tags 1..npart, seeded uniform positions
+        (``synth.seeded_particles`` restates the generator), zero velocities and histories."""
+        _check(self._lib.mhit_init_particles(self._ctx, int(npart), int(seed) & 0xFFFFFFFFFFFFFFFF))
+        self._np = int(npart)
+
     def upload_particles(self, part):
         """Tracer table (npart, 12): tag, x, y, z, u, v, w, phi, u1, v1, w1, phi1."""
         part = np.asfortranarray(part, dtype=np.float64)

@@ -12,6 +12,7 @@
 //   k_drops     phi = 0.5 (1 - tanh((r - R)/(2 eps))) with r the periodic minimum-image distance
 //               to the nearest of n centres: the centred drop of multi/main.f90:370-382
 //               generalised to many drops.
+//   k_particles the tracer table of multi/particles.f90:37-76 from a counter-based generator.
 // Every product and sum is written with explicit IEEE operations (no contraction), so the
 // device fields equal a host evaluation in the same order except where CUDA's tanh differs
 // from the host's by an ulp.
@@ -139,6 +140,31 @@ __global__ void k_drops(double* __restrict__ phi, const double* __restrict__ cen
   }
 }
 
+// Tracer table of multi/particles.f90:37-76 (particlegenerator with inflag = 1): tag i, position
+// uniform in the box, everything else zero.  The reference draws from an unseeded
+// RANDOM_NUMBER; here position a of tracer i is splitmix64(seed + (3 i + a + 1) G) (Steele, Lea
+// and Flood, "Fast splittable pseudorandom number generators", OOPSLA 2014; G the golden-ratio
+// increment 0x9E3779B97F4A7C15) mapped to [0, 1) by its top 53 bits, times the box length.
+__device__ __forceinline__ unsigned long long splitmix64(unsigned long long z) {
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+__global__ void k_particles(double* __restrict__ part, int np, unsigned long long seed, double lx, double ly,
+                            double lz) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np; i += gridDim.x * blockDim.x) {
+    const double len[3] = {lx, ly, lz};
+    part[i] = (double)(i + 1);  // Itag
+    for (int a = 0; a < 3; ++a) {
+      const unsigned long long r = splitmix64(seed + (3ull * (unsigned long long)i + a + 1) * 0x9E3779B97F4A7C15ull);
+      const double u01 = (double)(r >> 11) * 0x1.0p-53;
+      part[(size_t)(1 + a) * np + i] = __dmul_rn(u01, len[a]);
+    }
+    for (int c = 4; c < 12; ++c) part[(size_t)c * np + i] = 0.0;
+  }
+}
+
 static int grid_for(size_t n) {
   const size_t b = (n + ITHREADS - 1) / ITHREADS;
   return (int)(b < 148 * 16 ? (b ? b : 1) : 148 * 16);
@@ -161,6 +187,12 @@ cudaError_t launch_init_modes(const ModeArgs& a, cudaStream_t st) {
 
 cudaError_t launch_scale(double* f, size_t n, double s, cudaStream_t st) {
   k_scale<<<grid_for(n), ITHREADS, 0, st>>>(f, n, s);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_init_particles(double* part, int np, unsigned long long seed, double lx, double ly, double lz,
+                                  cudaStream_t st) {
+  k_particles<<<grid_for((size_t)np), ITHREADS, 0, st>>>(part, np, seed, lx, ly, lz);
   return cudaGetLastError();
 }
 

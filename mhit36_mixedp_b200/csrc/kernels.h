@@ -153,6 +153,8 @@ struct DropInitArgs {
   double dx, lx, ly, lz, radius, eps;
 };
 cudaError_t launch_init_drops(const DropInitArgs& a, cudaStream_t st);
+cudaError_t launch_init_particles(double* part, int np, unsigned long long seed, double lx, double ly, double lz,
+                                  cudaStream_t st);
 
 // ---------------------------------------------------------------- energy spectrum
 int spectrum_blocks(const Geo& g);

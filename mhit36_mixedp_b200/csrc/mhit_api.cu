@@ -643,11 +643,8 @@ int mhit_upload_fields(mhit_ctx* c, const double* u, const double* v, const doub
   return reset_history(c);
 }
 
-int mhit_upload_particles(mhit_ctx* c, const double* part, int npart) {
-  int rc;
-  if ((rc = check_ctx(c))) return rc;
-  if (!c->prm.partflag) return set_error(MHIT_ERR_STATE, "context was created with partflag=0");
-  if (npart < 0 || (npart > 0 && !part)) return set_error(MHIT_ERR_ARG, "bad particle table");
+// Replace the tracer table by an allocated, unfilled one of npart rows (none for 0).
+static int reset_particles(mhit_ctx* c, int npart) {
   if (c->part) {
     MHIT_CUDA_TRY(cudaStreamSynchronize(c->st));
     cudaFree(c->part);
@@ -662,10 +659,31 @@ int mhit_upload_particles(mhit_ctx* c, const double* part, int npart) {
       c->gexec[i] = nullptr;
     }
   c->graph_built = false;
+  if (npart > 0) MHIT_CUDA_TRY(cudaMalloc(&c->part, (size_t)npart * 12 * sizeof(double)));
+  return MHIT_OK;
+}
+
+int mhit_upload_particles(mhit_ctx* c, const double* part, int npart) {
+  int rc;
+  if ((rc = check_ctx(c))) return rc;
+  if (!c->prm.partflag) return set_error(MHIT_ERR_STATE, "context was created with partflag=0");
+  if (npart < 0 || (npart > 0 && !part)) return set_error(MHIT_ERR_ARG, "bad particle table");
+  if ((rc = reset_particles(c, npart))) return rc;
   if (npart == 0) return MHIT_OK;
-  const size_t bytes = (size_t)npart * 12 * sizeof(double);
-  MHIT_CUDA_TRY(cudaMalloc(&c->part, bytes));
-  MHIT_CUDA_TRY(cudaMemcpyAsync(c->part, part, bytes, cudaMemcpyHostToDevice, c->st));
+  MHIT_CUDA_TRY(cudaMemcpyAsync(c->part, part, (size_t)npart * 12 * sizeof(double), cudaMemcpyHostToDevice, c->st));
+  MHIT_CUDA_TRY(cudaStreamSynchronize(c->st));
+  return MHIT_OK;
+}
+
+int mhit_init_particles(mhit_ctx* c, int npart, unsigned long long seed) {
+  int rc;
+  if ((rc = check_ctx(c))) return rc;
+  if (!c->prm.partflag) return set_error(MHIT_ERR_STATE, "context was created with partflag=0");
+  if (npart < 1) return set_error(MHIT_ERR_ARG, "npart must be positive");
+  if ((rc = reset_particles(c, npart))) return rc;
+  const double lx = 8.0 * std::atan(1.0);
+  MHIT_CUDA_TRY(launch_init_particles(c->part, npart, seed, lx, c->prm.ny == c->prm.nx ? lx : c->g.dx * c->prm.ny,
+                                      c->prm.nz == c->prm.nx ? lx : c->g.dx * c->prm.nz, c->st));
   MHIT_CUDA_TRY(cudaStreamSynchronize(c->st));
   return MHIT_OK;
 }

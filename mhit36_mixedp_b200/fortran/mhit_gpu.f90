@@ -112,6 +112,14 @@ module mhit_gpu
       real(c_double), value :: radius
     end function
 
+    ! tracer table built on the device: tags, seeded uniform positions, zero velocities
+    integer(c_int) function mhit_init_particles(ctx, npart, seed) bind(C, name="mhit_init_particles")
+      import :: c_int, c_ptr, c_long_long
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: npart
+      integer(c_long_long), value :: seed
+    end function
+
     ! E(0:nbins-1): shell-summed kinetic-energy spectrum of the current velocity
     integer(c_int) function mhit_energy_spectrum(ctx, E, nbins) bind(C, name="mhit_energy_spectrum")
       import :: c_int, c_ptr, c_double

@@ -2,15 +2,17 @@
 // `program main` (multi/main.f90) on one GPU, for hosts without a Fortran compiler.
 //
 //   input.inp          read by mhit_read_input (subroutine readinput, multi/readinput.f90:4-81)
-//   initial condition  inflow = 0: Taylor-Green on the staggered grid (multi/main.f90:322-337);
+//   initial condition  inflow = 0: Taylor-Green on the staggered grid (multi/main.f90:322-337),
+//                      built on the device by mhit_init_taylor_green;
 //                      inflow = 1: u, v, w from <indir>/{u,v,w}.dat (readfield, :339-350);
-//                      phiflag: inphi = 0 a centred drop (:370-382), inphi = 1 <indir>/phi.dat
+//                      phiflag: inphi = 0 a centred drop (:370-382, mhit_init_drops with one
+//                      centre at (pi, pi, pi)), inphi = 1 <indir>/phi.dat
 //   time loop          do t = tstart+1, tfin: one mhit_step per step (:456-1007), the CFL print
 //                      of :1003-1007 and its stop at CFL > 7 (:1006), field files every `dump`
 //                      steps (:1023-1034, writefield of multi/readwrite.f90)
 //
-// The grid coordinates follow the reference: x(i) accumulated as x(i-1) + dx (:225-231), and
-// the y/z planes read one entry on (the halo-shifted labelling, yz_shift = 1).
+// Fields read from files are uploaded with mhit_upload_fields; a mixed start (velocity from
+// files, centred drop) uploads the files first and then builds phi on the device.
 #include <sys/stat.h>
 
 #include <chrono>
@@ -111,17 +113,6 @@ bool read_raw(const std::string& path, std::vector<double>& a) {
   return got == a.size();
 }
 
-// x(0) = 0, x(i) = x(i-1) + dx: the accumulated coordinates of multi/main.f90:225-231
-std::vector<double> accumulated(int n, double dx) {
-  std::vector<double> x(n + 1, 0.0);
-  double acc = 0.0;
-  for (int i = 1; i <= n; ++i) {
-    acc = acc + dx;
-    x[i] = acc;
-  }
-  return x;
-}
-
 }  // namespace
 
 int main(int argc, char** argv) {
@@ -155,59 +146,41 @@ int main(int argc, char** argv) {
     return 0;
   }
 
-  const int nx = p.nx, ny = p.ny, nz = p.nz;
-  const size_t n = (size_t)nx * ny * nz;
-  const double lx = 8.0 * std::atan(1.0), dx = lx / nx;
-  const int s = p.yz_shift;
-  std::vector<double> u(n), v(n), w(n), phi;
+  const size_t n = (size_t)p.nx * p.ny * p.nz;
+  mhit_ctx* ctx = nullptr;
+  if ((rc = mhit_init(&p, &ctx))) return fail("mhit_init", rc);
+  auto bail = [&](const char* what, int r) {
+    mhit_destroy(ctx);
+    return fail(what, r);
+  };
   if (run.inflow == 1) {
+    std::vector<double> u(n), v(n), w(n), phi(p.phiflag ? n : 0);
     for (auto [name, a] : {std::pair<const char*, std::vector<double>*>{"u", &u}, {"v", &v}, {"w", &w}}) {
       const std::string path = o.indir + "/" + name + ".dat";
       if (!read_raw(path, *a)) {
         std::fprintf(stderr, "cannot read %s\n", path.c_str());
+        mhit_destroy(ctx);
         return 1;
       }
     }
+    // phi from the file when inphi = 1; otherwise a placeholder replaced by the drop below
+    if (p.phiflag && run.inphi == 1 && !read_raw(o.indir + "/phi.dat", phi)) {
+      std::fprintf(stderr, "cannot read %s/phi.dat\n", o.indir.c_str());
+      mhit_destroy(ctx);
+      return 1;
+    }
+    if ((rc = mhit_upload_fields(ctx, u.data(), v.data(), w.data(), p.phiflag ? phi.data() : nullptr)))
+      return bail("mhit_upload_fields", rc);
   } else {
-    // Taylor-Green, multi/main.f90:324-337: u = sin(x - dx/2) cos(y) cos(z),
-    // v = -cos(x) sin(y - dx/2) cos(z), w = 0, y and z read one entry on (yz_shift)
-    const std::vector<double> xa = accumulated(std::max(nx, std::max(ny, nz)) + 1, dx);
-    for (int k = 0; k < nz; ++k)
-      for (int j = 0; j < ny; ++j)
-        for (int i = 0; i < nx; ++i) {
-          const size_t c = ((size_t)k * ny + j) * nx + i;
-          const double X = xa[i], Y = xa[j + s], Z = xa[k + s];
-          u[c] = std::sin(X - dx / 2) * std::cos(Y) * std::cos(Z);
-          v[c] = -std::cos(X) * std::sin(Y - dx / 2) * std::cos(Z);
-          w[c] = 0.0;
-        }
-  }
-  if (p.phiflag) {
-    phi.resize(n);
-    if (run.inphi == 1) {
-      const std::string path = o.indir + "/phi.dat";
-      if (!read_raw(path, phi)) {
-        std::fprintf(stderr, "cannot read %s\n", path.c_str());
-        return 1;
-      }
-    } else {
-      // centred drop, multi/main.f90:370-382: phi = (1 - tanh((r - R)/(2 eps)))/2, eps = epsr dx
-      const double eps = p.epsr * dx;
-      for (int k = 0; k < nz; ++k)
-        for (int j = 0; j < ny; ++j)
-          for (int i = 0; i < nx; ++i) {
-            const double x = i * dx, y = (j + s) * dx, z = (k + s) * dx;
-            const double pos = (x - lx / 2) * (x - lx / 2) + (y - lx / 2) * (y - lx / 2) + (z - lx / 2) * (z - lx / 2);
-            phi[((size_t)k * ny + j) * nx + i] = 0.5 * (1.0 - std::tanh((std::sqrt(pos) - p.radius) / 2 / eps));
-          }
+    if ((rc = mhit_init_taylor_green(ctx))) return bail("mhit_init_taylor_green", rc);
+    if (p.phiflag && run.inphi == 1) {
+      if ((rc = mhit_read_field(ctx, (o.indir + "/phi.dat").c_str(), 5))) return bail("mhit_read_field", rc);
     }
   }
-
-  mhit_ctx* ctx = nullptr;
-  if ((rc = mhit_init(&p, &ctx))) return fail("mhit_init", rc);
-  if ((rc = mhit_upload_fields(ctx, u.data(), v.data(), w.data(), p.phiflag ? phi.data() : nullptr))) {
-    mhit_destroy(ctx);
-    return fail("mhit_upload_fields", rc);
+  if (p.phiflag && run.inphi != 1) {
+    const double pi = 4.0 * std::atan(1.0);
+    const double centre[3] = {pi, pi, pi};
+    if ((rc = mhit_init_drops(ctx, 1, centre, p.radius))) return bail("mhit_init_drops", rc);
   }
   const int nfields = p.phiflag ? 5 : 4;
   auto dump = [&](int t) -> int {

@@ -12,7 +12,8 @@ configurations with explicit seeds (``numpy.random.default_rng``):
 * ``drops_phi``: phi = 0.5 (1 - tanh((r - R)/(2 eps))) with r the minimum-image distance to the
   nearest of ``ndrops`` uniformly placed centres (the max over spheres of the single-drop
   profile of multi/main.f90:377-378; distances are capped at R + 40 eps, where phi < 1e-17).
-* ``uniform_particles``: the tracer table of multi/particles.f90:46-72 with seeded positions.
+* ``uniform_particles``: the tracer table of multi/particles.f90:46-72 with seeded positions;
+  ``seeded_particles``: the same table from the counter-based generator of mhit_init_particles.
 
 Grid coordinates use the reference labelling: x = i dx, y = (j + s) dx, z = (k + s) dx with
 s = yz_shift (1 for the reference, see multi/main.f90:327-331).
@@ -121,6 +122,31 @@ def uniform_particles(npart, seed):
     part = np.zeros((npart, 12), dtype=np.float64, order="F")
     part[:, 0] = np.arange(1, npart + 1)
     part[:, 1:4] = rng.uniform(0.0, LX, size=(npart, 3))
+    return part
+
+
+_GOLDEN = np.uint64(0x9E3779B97F4A7C15)
+
+
+def _splitmix64(z):
+    """The splitmix64 finaliser (Steele, Lea and Flood, OOPSLA 2014) on a uint64 array."""
+    with np.errstate(over="ignore"):
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+    return z ^ (z >> np.uint64(31))
+
+
+def seeded_particles(npart, seed, lengths=(LX, LX, LX)):
+    """The tracer table that mhit_init_particles builds on the device (multi/particles.f90:37-76
+    with a reproducible generator): coordinate a of tracer i is
+    lengths[a] * (top 53 bits of splitmix64(seed + (3 i + a + 1) G)) / 2^53."""
+    part = np.zeros((npart, 12), dtype=np.float64, order="F")
+    part[:, 0] = np.arange(1, npart + 1)
+    i = np.arange(npart, dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        for a in range(3):
+            r = _splitmix64(np.uint64(seed) + (np.uint64(3) * i + np.uint64(a + 1)) * _GOLDEN)
+            part[:, 1 + a] = (r >> np.uint64(11)).astype(np.float64) * 2.0 ** -53 * lengths[a]
     return part
 
 

@@ -63,7 +63,7 @@ def test_fortran_module_matches_header():
                "mhit_write_field", "mhit_read_field", "mhit_diagnostics", "mhit_destroy",
                "mhit_ensemble_create", "mhit_ensemble_box", "mhit_ensemble_step", "mhit_ensemble_autotune",
                "mhit_ensemble_destroy", "mhit_init_taylor_green", "mhit_init_velocity_modes", "mhit_init_drops",
-               "mhit_energy_spectrum"):
+               "mhit_energy_spectrum", "mhit_init_particles"):
         assert f'name="{fn}"' in f90, fn
     # the Poisson-mode constants agree with the C side
     for name, val in (("MHIT_POISSON_FP64", 0), ("MHIT_POISSON_FP32", 1), ("MHIT_POISSON_FP32_REFINED", 2)):

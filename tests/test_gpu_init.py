@@ -108,3 +108,30 @@ def test_init_drops_keeps_the_velocity(gpu):
         after = s.download(("u", "v", "w"))
     for f in "uvw":
         assert np.max(np.abs(after[f] - before[f])) <= 1e-15 * np.max(np.abs(before[f])), f
+
+
+@pytest.mark.parametrize("shape", SHAPES)
+def test_particles_match_host_twin(gpu, shape):
+    nx, ny, nz = shape
+    dx = 2 * math.pi / nx
+    lengths = (synth.LX, synth.LX if ny == nx else dx * ny, synth.LX if nz == nx else dx * nz)
+    with Solver(Params(nx=nx, ny=ny, nz=nz, partflag=1)) as s:
+        s.init_particles(1000, 77)
+        got = s.download_particles()
+    assert np.array_equal(got, synth.seeded_particles(1000, 77, lengths))
+
+
+def test_device_tracers_step_like_uploaded_ones(gpu):
+    n = 32
+    prm = Params(nx=n, partflag=1, mu=0.01, dt=5e-4)
+    res = []
+    for device_table in (True, False):
+        with Solver(prm) as s:
+            s.init_solenoidal(seed=2)
+            if device_table:
+                s.init_particles(500, 9)
+            else:
+                s.upload_particles(synth.seeded_particles(500, 9))
+            s.step(4)
+            res.append(s.download_particles())
+    assert np.array_equal(res[0], res[1])

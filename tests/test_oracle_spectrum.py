@@ -26,3 +26,26 @@ def test_single_mode_including_nyquist():
     E = orc.energy_spectrum(u, z, z, 20)
     assert abs(E[3] - 0.25) < 1e-15 and abs(E[8] - 0.5) < 1e-15
     assert abs(E.sum() - orc.kinetic_energy(u, z, z)) < 1e-15
+
+
+def test_seeded_particles_follow_splitmix64():
+    """synth.seeded_particles (the numpy twin of mhit_init_particles) against a pure-integer
+    restatement of splitmix64."""
+    M = (1 << 64) - 1
+    G = 0x9E3779B97F4A7C15
+
+    def mix(z):
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & M
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & M
+        return z ^ (z >> 31)
+
+    seed = 12345
+    lengths = (2 * np.pi, np.pi, 4 * np.pi)
+    part = synth.seeded_particles(50, seed, lengths)
+    for i in (0, 1, 17, 49):
+        for a in range(3):
+            r = mix((seed + (3 * i + a + 1) * G) & M)
+            assert part[i, 1 + a] == (r >> 11) * 2.0 ** -53 * lengths[a]
+    assert np.array_equal(part[:, 0], np.arange(1, 51)) and not part[:, 4:].any()
+    for a in range(3):
+        assert (part[:, 1 + a] >= 0).all() and (part[:, 1 + a] < lengths[a]).all()
