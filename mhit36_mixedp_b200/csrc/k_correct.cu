@@ -15,7 +15,7 @@ namespace mhit {
 
 constexpr int CNT = 256;
 
-constexpr int CTX = 32, CTY = 16, CZC = 16;  // x-y tile and z chunk of k_correct
+constexpr int CTX = 32, CTY = 16, CZC = 16;  // x-y tile and default z chunk of k_correct
 
 // Pressure sources of the projection: a pair of x-adjacent values and a single value, widened
 // to FP64.  PSum is the refinement's p = p32 + delta, formed on the fly exactly as a stored
@@ -44,10 +44,10 @@ struct PSum {
 };
 
 // Each thread owns two adjacent x cells (16-byte loads of u, v, w) of one tile row and marches
-// up CZC planes two at a time: p(k-1) is carried in registers from the previous plane,
+// up zc planes two at a time: p(k-1) is carried in registers from the previous plane,
 // p(i-1) comes from the neighbouring lane of the 16-lane row, p(j-1) from L1.
 template <typename S>
-__global__ void __launch_bounds__(CNT) k_correct(CorrectArgs a, S ps) {
+__global__ void __launch_bounds__(CNT) k_correct(CorrectArgs a, S ps, int zc) {
   const Geo& g = a.g;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const size_t plane = (size_t)nx * ny;
@@ -57,7 +57,7 @@ __global__ void __launch_bounds__(CNT) k_correct(CorrectArgs a, S ps) {
   const double cc = g.dt / g.rho, dxi = g.dxi;
   const int lx = threadIdx.x & 15, ty = threadIdx.x >> 4;  // 16 lanes x 16 rows
   const int i = blockIdx.x * CTX + 2 * lx, j = blockIdx.y * CTY + ty;
-  const int k0 = blockIdx.z * CZC, k1 = min(k0 + CZC, nz);
+  const int k0 = blockIdx.z * zc, k1 = min(k0 + zc, nz);
   const bool own = i < nx && j < ny;
   const int ic = own ? i : 0, jc = own ? j : 0;
   const int im = wrapm(ic, nx), jm = wrapm(jc, ny);
@@ -181,8 +181,17 @@ __global__ void __launch_bounds__(1024) k_finalize(const double* __restrict__ pa
   }
 }
 
+// z planes per block: 64 where that still leaves eight waves of two blocks on each of the 148
+// SMs (each chunk re-reads the p plane below it: 1.106 against 1.135 ms FP32, 1.209 against
+// 1.250 ms FP64 at 512^3), otherwise CZC
+static int correct_chunk(const Geo& g) {
+  const long long cols = (long long)((g.nx + CTX - 1) / CTX) * ((g.ny + CTY - 1) / CTY);
+  return cols * ((g.nz + 63) / 64) >= 8 * 148 * 2 ? 64 : CZC;
+}
+
 static dim3 correct_grid(const Geo& g) {
-  return dim3((g.nx + CTX - 1) / CTX, (g.ny + CTY - 1) / CTY, (g.nz + CZC - 1) / CZC);
+  const int zc = correct_chunk(g);
+  return dim3((g.nx + CTX - 1) / CTX, (g.ny + CTY - 1) / CTY, (g.nz + zc - 1) / zc);
 }
 
 int correct_blocks(const Geo& g) {
@@ -192,9 +201,10 @@ int correct_blocks(const Geo& g) {
 
 cudaError_t launch_correct(const CorrectArgs& a, cudaStream_t st) {
   const dim3 grd = correct_grid(a.g), blk(CNT);
-  if (a.pd) k_correct<<<grd, blk, 0, st>>>(a, PSum{static_cast<const float*>(a.p), a.pd});
-  else if (a.fp32) k_correct<<<grd, blk, 0, st>>>(a, PFloat{static_cast<const float*>(a.p)});
-  else k_correct<<<grd, blk, 0, st>>>(a, PDouble{static_cast<const double*>(a.p)});
+  const int zc = correct_chunk(a.g);
+  if (a.pd) k_correct<<<grd, blk, 0, st>>>(a, PSum{static_cast<const float*>(a.p), a.pd}, zc);
+  else if (a.fp32) k_correct<<<grd, blk, 0, st>>>(a, PFloat{static_cast<const float*>(a.p)}, zc);
+  else k_correct<<<grd, blk, 0, st>>>(a, PDouble{static_cast<const double*>(a.p)}, zc);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   k_finalize<<<1, 1024, 0, st>>>(a.partials, a.nblocks, a.g, a.sc);

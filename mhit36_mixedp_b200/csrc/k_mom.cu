@@ -253,9 +253,16 @@ static cudaError_t launch_mom_t(const MomArgs& a, cudaStream_t st) {
     if (e != cudaSuccess) return e;
     attr_set[dev] = 1;
   }
-  const int zc = a.zchunk > 0 ? a.zchunk : MZC;
+  // Default chunk: 64 planes where that still leaves eight waves of three blocks on each of the
+  // 148 SMs (2.896 against 2.928 ms at 512^3), otherwise MZC.  Results do not depend on it.
+  MomArgs b = a;
+  if (b.zchunk <= 0) {
+    const long long cols = (long long)((a.g.nx + MTX - 1) / MTX) * ((a.g.ny + MTY - 1) / MTY);
+    b.zchunk = cols * ((a.g.nz + 63) / 64) >= 8 * 148 * 3 ? 64 : MZC;
+  }
+  const int zc = b.zchunk;
   dim3 grd((a.g.nx + MTX - 1) / MTX, (a.g.ny + MTY - 1) / MTY, (a.g.nz + zc - 1) / zc);
-  k_mom<PHI><<<grd, MNT, smem, st>>>(a);
+  k_mom<PHI><<<grd, MNT, smem, st>>>(b);
   return cudaGetLastError();
 }
 

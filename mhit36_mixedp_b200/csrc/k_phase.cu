@@ -218,9 +218,17 @@ cudaError_t launch_phase(const PhaseArgs& a, cudaStream_t st) {
     if (e != cudaSuccess) return e;
     if (dev < 64) attr_set[dev][a.clamp ? 1 : 0] = 1;
   }
-  const int zc = a.zchunk > 0 ? a.zchunk : PZC;
+  // Default chunk: 128 planes where that still leaves eight waves of one block on each of the
+  // 148 SMs (the four planes of warm-up below a chunk cost 3% instead of 6%: 2.667 against
+  // 2.723 ms at 512^3), otherwise PZC.  Results do not depend on the chunk.
+  PhaseArgs b = a;
+  if (b.zchunk <= 0) {
+    const long long cols = (long long)((a.g.nx + PTX - 1) / PTX) * ((a.g.ny + PTY - 1) / PTY);
+    b.zchunk = cols * ((a.g.nz + 127) / 128) >= 8 * 148 ? 128 : PZC;
+  }
+  const int zc = b.zchunk;
   dim3 grd((a.g.nx + PTX - 1) / PTX, (a.g.ny + PTY - 1) / PTY, (a.g.nz + zc - 1) / zc);
-  kern<<<grd, PNT, smem, st>>>(a);
+  kern<<<grd, PNT, smem, st>>>(b);
   return cudaGetLastError();
 }
 

@@ -6,7 +6,8 @@ cannot step 512^3 in seconds, so these check what holds at any size.
   divergence error.
 * FP32 Poisson + one FP64 residual sweep reproduces that FP64 step to 1e-12.
 * FP32 and FP64 Poisson with the reference's exact k^2 agree to FP32 rounding (1e-5 of u_max)
-  and leave the same O(dx^2) divergence to 1e-5.
+  and leave the same O(dx^2) divergence up to FP32 rounding of the divergence scale
+  u_max n/2pi (two FP32 ulp: 1.2e-7 of it).
 * The downloaded velocity has zero mean (the mean removal of multi/main.f90:977-981).
 """
 import numpy as np
@@ -57,5 +58,5 @@ def test_512_fp32_poisson_matches_fp64(gpu, fields):
     for f in "uvw":
         e = np.abs(out32[f] - out64[f]).max() / umax
         assert e < 1e-5, (f, e)
-    assert abs(dg32["maxdiv"] - dg64["maxdiv"]) <= 1e-5 * dg64["maxdiv"]
+    assert abs(dg32["maxdiv"] - dg64["maxdiv"]) <= 1.2e-7 * umax * N / (2 * np.pi)
     assert abs(dg32["ke"] - dg64["ke"]) <= 1e-6 * dg64["ke"]
