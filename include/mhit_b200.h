@@ -134,7 +134,9 @@ int mhit_upload_fields(mhit_ctx* ctx, const double* u, const double* v, const do
  *   (x, y, z triples), cells at x = i dx, y = (j + yz_shift) dx, z = (k + yz_shift) dx; one
  *   centre at (pi, pi, pi) is the centred drop of multi/main.f90:370-382.  Replaces phi (needs
  *   phiflag = 1); the velocity keeps its values.
- * Each resets rhs_o, rhsphi_o, gumax = 1 and the Euler first step like mhit_upload_fields. */
+ * Each resets rhs_o, rhsphi_o, gumax = 1 and the Euler first step like mhit_upload_fields and
+ * keeps the fields it does not replace; after an error return the fields it would have replaced
+ * are undefined (upload or initialise them again). */
 int mhit_init_taylor_green(mhit_ctx* ctx);
 int mhit_init_velocity_modes(mhit_ctx* ctx, int kmax, const double* modes, double rms);
 int mhit_init_drops(mhit_ctx* ctx, int ndrops, const double* centres, double radius);

@@ -1147,8 +1147,9 @@ int mhit_init_taylor_green(mhit_ctx* c) {
   for (int k = 0; k < nz; ++k) tab.push_back(std::cos(xa[k + s]));
   DevBuf dt;
   if ((rc = to_device(dt, tab, c->st))) return rc;
-  c->cur = 0;
-  MHIT_CUDA_TRY(launch_init_tg(c->U[0], c->V[0], c->W[0], static_cast<const double*>(dt.p), nx, ny, nz, c->st));
+  // into the current ping-pong slot: phi (when present) stays where it is
+  const int k = c->cur;
+  MHIT_CUDA_TRY(launch_init_tg(c->U[k], c->V[k], c->W[k], static_cast<const double*>(dt.p), nx, ny, nz, c->st));
   MHIT_CUDA_TRY(cudaStreamSynchronize(c->st));
   return reset_history(c);
 }
@@ -1171,8 +1172,9 @@ int mhit_init_velocity_modes(mhit_ctx* c, int kmax, const double* modes, double 
   const int npart = modes_partials(nx, ny);
   MHIT_CUDA_TRY(cudaMalloc(&dpart.p, (size_t)npart * sizeof(double)));
   std::vector<double> part(npart);
-  double* dst[3] = {c->U[0], c->V[0], c->W[0]};
-  c->cur = 0;
+  // into the current ping-pong slot: phi (when present) stays where it is; on an error return
+  // the velocity is undefined
+  double* dst[3] = {c->U[c->cur], c->V[c->cur], c->W[c->cur]};
   for (int comp = 0; comp < 3; ++comp) {
     // index phases theta = (i + shift) 2 pi/n per axis (x: shift 0, y and z: yz_shift), the
     // component's own axis half a cell back (its face position, multi/main.f90:331); for a box of

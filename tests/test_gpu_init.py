@@ -135,3 +135,24 @@ def test_device_tracers_step_like_uploaded_ones(gpu):
             s.step(4)
             res.append(s.download_particles())
     assert np.array_equal(res[0], res[1])
+
+
+def test_velocity_inits_keep_phi_after_odd_steps(gpu):
+    """The velocity generators write the current ping-pong slot: phi survives, whatever the
+    parity of the step count."""
+    n = 32
+    prm = Params(nx=n, phiflag=1, radius=0.5, sigma=0.2, mu=0.01, dt=2e-4)
+    with Solver(prm) as s:
+        s.init_solenoidal(seed=1)
+        s.init_drops([[1.0, 2.0, 3.0]], 0.5)
+        s.step(3)
+        before = s.download(("phi",))["phi"]
+        s.init_solenoidal(seed=2)
+        assert np.array_equal(s.download(("phi",))["phi"], before)
+        s.step(1)
+        before = s.download(("phi",))["phi"]
+        s.init_taylor_green()
+        assert np.array_equal(s.download(("phi",))["phi"], before)
+        tg = s.download(("u",))["u"]
+    u, _, _ = orc.taylor_green(orc.Params(nx=n))
+    assert np.max(np.abs(tg - u)) <= 4e-16

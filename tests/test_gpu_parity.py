@@ -63,7 +63,7 @@ def test_ns_fp64_one_step(gpu, n):
 
 
 def test_ns_fp64_100_steps_64(gpu):
-    """64^3 NS, FP64 Poisson, 100 steps, <= 1e-12 relative."""
+    """The 64^3 NS case (FP64 Poisson, seeded solenoidal start, 100 steps): <= 1e-12 relative."""
     prm, u, v, w, phi, part = make_case(64)
     st, out, dg, _ = run_both(prm, u, v, w, phi, part, 100)
     errs = {f: relerr(out[f], getattr(st, f)) for f in ("u", "v", "w")}
