@@ -145,3 +145,21 @@ def test_init_without_gpu_fails_cleanly():
         pytest.skip("a GPU is present")
     with pytest.raises(api.MhitError):
         api.Solver(api.Params(nx=32))
+
+
+def test_entry_points_reject_a_null_context():
+    """Every context entry point validates its handle before touching the device."""
+    lib = _lib.load()
+    buf = (ctypes.c_double * 64)()
+    calls = {
+        "mhit_step": (None, 1),
+        "mhit_init_taylor_green": (None,),
+        "mhit_init_velocity_modes": (None, 1, buf, 1.0),
+        "mhit_init_drops": (None, 1, buf, 0.5),
+        "mhit_init_particles": (None, 10, 1),
+        "mhit_energy_spectrum": (None, buf, 8),
+        "mhit_diagnostics": (None, None),
+        "mhit_label_drops": (None, 0.5, 6, None, 0, None, None),
+    }
+    for name, args in calls.items():
+        assert getattr(lib, name)(*args) == _lib.MHIT_ERR_ARG, name
