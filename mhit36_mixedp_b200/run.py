@@ -81,9 +81,10 @@ def main(argv=None):
         else:  # centred drop, multi/main.f90:370-382
             dx = 8.0 * math.atan(1.0) / n
             x = np.arange(n) * dx
-            y = (np.arange(n) + prm.yz_shift) * dx
+            y = (np.arange(prm.ny) + prm.yz_shift) * dx
+            z = (np.arange(prm.nz) + prm.yz_shift) * dx
             lx = 8.0 * math.atan(1.0)
-            pos = ((x - lx / 2) ** 2)[None, None, :] + ((y - lx / 2) ** 2)[None, :, None] + ((y - lx / 2) ** 2)[:, None, None]
+            pos = ((x - lx / 2) ** 2)[None, None, :] + ((y - lx / 2) ** 2)[None, :, None] + ((z - lx / 2) ** 2)[:, None, None]
             phi = 0.5 * (1.0 - np.tanh((np.sqrt(pos) - prm.radius) / 2 / (prm.epsr * dx)))
     steps = args.steps if args.steps is not None else run["tfin"] - run["tstart"]
     with api.Solver(prm) as s:
