@@ -23,17 +23,21 @@ import numpy as np
 from . import api, synth
 
 
-def taylor_green(n, yz_shift=1):
-    """multi/main.f90:324-337 with the accumulated grid x(i) = x(i-1) + dx."""
+def taylor_green(n, yz_shift=1, ny=None, nz=None):
+    """multi/main.f90:324-337 with the accumulated grid x(i) = x(i-1) + dx (one spacing 2 pi/n
+    on every axis, y and z read yz_shift entries on)."""
+    ny = ny or n
+    nz = nz or n
     dx = 8.0 * math.atan(1.0) / n
-    xs = np.zeros(n + 1)
+    m = max(n, ny, nz)
+    xs = np.zeros(m + 1)
     acc = 0.0
-    for i in range(1, n + 1):
+    for i in range(1, m + 1):
         acc = acc + dx
         xs[i] = acc
-    X, Y = xs[:n], xs[yz_shift:yz_shift + n]
-    u = np.sin(X - dx / 2)[None, None, :] * np.cos(Y)[None, :, None] * np.cos(Y)[:, None, None]
-    v = -np.cos(X)[None, None, :] * np.sin(Y - dx / 2)[None, :, None] * np.cos(Y)[:, None, None]
+    X, Y, Z = xs[:n], xs[yz_shift:yz_shift + ny], xs[yz_shift:yz_shift + nz]
+    u = np.sin(X - dx / 2)[None, None, :] * np.cos(Y)[None, :, None] * np.cos(Z)[:, None, None]
+    v = -np.cos(X)[None, None, :] * np.sin(Y - dx / 2)[None, :, None] * np.cos(Z)[:, None, None]
     return u, v, np.zeros_like(u)
 
 
@@ -74,7 +78,7 @@ def main(argv=None):
         u, v, w = (np.fromfile(os.path.join(args.indir, f"{c}.dat"), dtype=np.float64).reshape(prm.shape)
                    for c in "uvw")
     else:
-        u, v, w = taylor_green(n, prm.yz_shift)
+        u, v, w = taylor_green(n, prm.yz_shift, prm.ny, prm.nz)
     if prm.phiflag and phi is None:
         if run.get("inphi", 0) == 1:
             phi = np.fromfile(os.path.join(args.indir, "phi.dat"), dtype=np.float64).reshape(prm.shape)
