@@ -49,3 +49,23 @@ def test_seeded_particles_follow_splitmix64():
     assert np.array_equal(part[:, 0], np.arange(1, 51)) and not part[:, 4:].any()
     for a in range(3):
         assert (part[:, 1 + a] >= 0).all() and (part[:, 1 + a] < lengths[a]).all()
+
+
+def test_solenoidal_modes_are_divergence_free_in_the_box_metric():
+    """k . c = 0 with the physical wavenumbers of a box nx dx by ny dx by nz dx, and the
+    non-cubic field holds only index wavenumbers |m| <= kmax along each axis (periodic)."""
+    kmax = 3
+    scale = (1.0, 2.0, 0.5)  # nx/ny, nx/nz for nx = 32, ny = 16, nz = 64
+    c = synth.solenoidal_modes(9, kmax, scale)
+    ks = np.arange(-kmax, kmax + 1)
+    KZ, KY, KX = np.meshgrid(ks, ks, ks, indexing="ij")
+    kdotc = KX * scale[0] * c[0] + KY * scale[1] * c[1] + KZ * scale[2] * c[2]
+    assert np.max(np.abs(kdotc)) < 1e-12 * np.max(np.abs(c))
+    u, v, w = synth.solenoidal_velocity(32, 9, kmax=kmax, ny=16, nz=64)
+    for f in (u, v, w):
+        F = np.abs(np.fft.fftn(f))
+        mz = np.abs(np.fft.fftfreq(64, 1 / 64))[:, None, None]
+        my = np.abs(np.fft.fftfreq(16, 1 / 16))[None, :, None]
+        mx = np.abs(np.fft.fftfreq(32, 1 / 32))[None, None, :]
+        outside = (mx > kmax) | (my > kmax) | (mz > kmax)
+        assert F[np.broadcast_to(outside, F.shape)].max() < 1e-9 * F.max()
