@@ -12,10 +12,16 @@ Fields are 1.07 GB each, larger than L2, so no flush is needed between steps.
 Timing: W warm-up steps, then K steps between two CUDA events on the library's stream
 (mhit_time_steps), max over ranks.  ``e2e`` repeats the mixed run through the public API with
 pinned host buffers: upload u,v,w,phi -> K x mhit_step(1) (each reads back the step
-scalars) -> download u,v,w,p,phi, all inside the timed region.
+scalars) -> download u,v,w,p,phi, all inside the timed region.  ``gpu_launches`` is K times the
+kernel nodes of the library's captured step graph.  ``configs`` carries the other scope-table
+configurations at N = 1: 1024^3 NS (FP32 and FP64 Poisson), 512^3 NS+ACDI with 1e6 tracers, and
+the 32-box ensemble (fields built on the device from the same seeds).
 
---impl reference times the CPU restatement of the reference loop (oracle/, the reference
-itself is Fortran/OpenACC with no compiler on this image) on a bounded sample.
+--impl reference times the reference loop on the host cores.  The reference is Fortran + OpenACC +
+cuDecomp and no Fortran compiler exists on this image, so its CPU implementation is the C/OpenMP
+restatement in oracle/ (kind "port"), run on the bench workload itself at the same size and
+Poisson precision; the line reports the warm-up and timed steps it actually ran.  ``cpu_baseline``
+in the GPU arm's line is a bounded sample of the same run (one Euler step, then a few AB2 steps).
 With torchrun (N > 1) every rank advances its own box (replicas; the step does not shard).
 """
 from __future__ import annotations
@@ -45,12 +51,13 @@ BYTES_PER_POINT = {
              "k_fft_cols_yinv": 16, "k_fftx_inv": 16, "k_correct+k_finalize": 56},
 }
 # DRAM bytes per grid point and launch measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum
-# of one launch / cells): k_phase, k_mom from profiles/k_phase_k_mom_ns_acdi_256.md (256^3); the
-# Poisson and projection kernels from profiles/poisson_projection_fp32_512x512x256.md.  Traffic
-# scales with the cell count for these streaming kernels, so a launch at 512^3 moves 8x the bytes.
+# of one launch / cells): k_phase and k_mom from a 256^3 capture, the Poisson and projection kernels
+# from a 512x512x256 capture.  Traffic scales with the cell count for these streaming kernels, so
+# the line reports these per-cell figures times the bench's cell count and says so.
 TRAFFIC_PER_POINT = {"k_phase": 55.1, "k_mom": 104.4, "k_div_fftx": 28.4, "k_fft_cols_yfwd": 7.5,
                      "k_fft_cols_zsolve": 7.5, "k_fft_cols_yinv": 7.5, "k_fftx_inv": 7.5,
                      "k_correct+k_finalize": 51.2}
+TRAFFIC_SOURCE = {"k_phase": "256^3", "k_mom": "256^3"}
 # the step-level model: NS+ACDI 256 B/pt (FP32 Poisson), 280 B/pt (FP64)
 STEP_BYTES = {"fp32": 256, "fp64": 280}
 
@@ -144,10 +151,10 @@ def max_over_ranks(values, dist, device):
     return [float(x) for x in t]
 
 
-def run_ours(args, rank, world, dev):
+def run_ours(args, rank, world, dev, fields):
     from mhit36_mixedp_b200 import Params, Solver
     n = args.n
-    prm, u, v, w, phi = workload(n)
+    prm, u, v, w, phi = fields
     res = {}
     for mode in ("fp32", "fp64"):
         with Solver(Params(device=dev, poisson=mode, **prm)) as s:
@@ -157,6 +164,7 @@ def run_ours(args, rank, world, dev):
                 ms = s.time_steps(args.steps)
             clocks = clk.summary()
             s.step(0)  # flag check of the timed steps
+            kernels = s.kernels_per_step()
             prof = [s.profile_step() for _ in range(3)]
             dg = s.diagnostics()
             if mode == "fp32":
@@ -179,11 +187,12 @@ def run_ours(args, rank, world, dev):
                 except Exception as ex:  # pragma: no cover - reported, not hidden
                     res["spectrum"] = {"error": str(ex)}
         stages = {k: statistics.mean(p[k] for p in prof) for k in prof[0]}
-        res[mode] = {"ms": ms / args.steps, "stages": stages, "diag": dg, "clocks": clocks}
+        res[mode] = {"ms": ms / args.steps, "stages": stages, "diag": dg, "clocks": clocks,
+                     "kernels_per_step": kernels}
     # the discrete-Laplacian solve, where divergence after projection is round-off: FP64, plain
     # FP32 and FP32 + one FP64 residual sweep, on the same inputs
     modified = {}
-    for mode in ("fp64", "fp32", "fp32_refined"):
+    for mode in MODIFIED_MODES:
         with Solver(Params(device=dev, poisson=mode, laplacian="modified", **prm)) as s:
             s.upload(u, v, w, phi)
             s.step(max(args.warmup, 3))
@@ -191,7 +200,7 @@ def run_ours(args, rank, world, dev):
             s.step(0)
             dg = s.diagnostics()
         modified[mode] = {"ms_per_step": ms / max(args.steps // 2, 3), "maxdiv": dg["maxdiv"],
-                          "dissipation": dg["dissipation"]}
+                          "dissipation": dg["dissipation"], "ke": dg["ke"]}
     res["modified"] = modified
     # e2e through the public API with pinned host buffers (mixed mode)
     e2e = None
@@ -226,47 +235,68 @@ def run_ours(args, rank, world, dev):
     return res, e2e
 
 
-def cpu_sample(n_sample=256, steps=3, n_target=512):
-    """C/OpenMP restatement of the reference loop (oracle/mhit_oracle.c) on a bounded sample:
-    NS+ACDI with FP32 Poisson at n_sample^3, all host threads, best AB2 step scaled by the
-    point count to n_target^3 (every pass of the loop is linear in the points up to the
-    log factor of the FFT)."""
+MODIFIED_MODES = ("fp64", "fp32", "fp32_refined")
+
+
+def headline_config(n, world):
+    return {"workload": f"NS+ACDI {n}^3, 64 drops R=0.3 eps=dx, We=1, nu=0.003, dt=2e-4, "
+                        f"seeds drops=1 vel=2; value: FP32 Poisson (mixed)",
+            "parallelism": "replicas" if world > 1 else "single", "l2": "inputs larger than L2"}
+
+
+def cpu_reference(fields, warmup, steps, budget_s):
+    """The C/OpenMP restatement of the reference loop (oracle/mhit_oracle.c, multi/main.f90:456-1007
+    pass by pass) on the bench workload itself (same size, same inputs, FP32 Poisson), on all host
+    threads: `warmup` untimed steps (the first is the Euler step), then up to `steps` timed steps,
+    fewer when the first step's time says the run would not end within `budget_s` seconds.
+    Returns (ms per timed step, warm-up steps run, timed steps run, threads)."""
     from oracle.coracle import COracle, threads
-    prm, u, v, w, phi = workload(n_sample)
+    prm, u, v, w, phi = fields
     c = COracle(poisson="fp32", **prm)
-    c.set_fields(u, v, w, phi)
-    times = []
-    for _ in range(steps):
+    try:
+        c.set_fields(u, v, w, phi)
         t0 = time.perf_counter()
         c.step(1)
-        times.append(time.perf_counter() - t0)
-    c.close()
-    per_step_s = min(times[1:] or times)
-    scale = (n_target / n_sample) ** 3
-    return {"value": per_step_s * 1e3 * scale, "unit": "ms/timestep", "cores": threads(), "kind": "port",
-            "sample": f"C/OpenMP restatement of multi/main.f90:456-1007, NS+ACDI FP32 Poisson at {n_sample}^3, "
-                      f"{steps} steps, best AB2 step x (512/{n_sample})^3 = {scale:g}"}
+        t_step = time.perf_counter() - t0
+        nwarm = max(1, min(int(warmup), int(0.25 * budget_s / max(t_step, 1e-9))))
+        for _ in range(nwarm - 1):
+            c.step(1)
+        ntimed = max(1, min(int(steps), int((budget_s - nwarm * t_step) / max(t_step, 1e-9))))
+        t0 = time.perf_counter()
+        c.step(ntimed)
+        ms = (time.perf_counter() - t0) * 1e3 / ntimed
+    finally:
+        c.close()
+    return ms, nwarm, ntimed, threads()
+
+
+def cpu_baseline_line(fields, warmup, steps, budget_s):
+    ms, nwarm, ntimed, cores = cpu_reference(fields, warmup, steps, budget_s)
+    n = fields[0]["nx"]
+    return {"value": ms, "unit": "ms/timestep", "cores": cores, "kind": "port",
+            "sample": f"C/OpenMP restatement of multi/main.f90:456-1007 on the bench workload itself "
+                      f"({n}^3 NS+ACDI, FP32 Poisson): {nwarm} untimed step(s) including the Euler step, "
+                      f"then {ntimed} timed AB2 step(s), mean"}
 
 
 def ensemble_workload(indices=None):
     """32 NS+ACDI boxes: 16 x 64^3, 10 x 128^3, 6 x 192^3; per-box seeds 100+b; nu ~ U[0.002,0.01],
-    We ~ U[0.5,5], 32-256 drops of radius 0.3 (eps = dx), FP32 Poisson, dt = 2e-4.  With indices,
-    only those boxes' fields are built (the parameters of every box come from one seeded stream)."""
+    We ~ U[0.5,5], 32-256 drops of radius 0.3 (eps = dx), FP32 Poisson, dt = 2e-4.  Returns the
+    parameters of every box (from one seeded stream) and, per box, the seed and drop centres the
+    fields are built from on the device (seeded solenoidal velocity of unit rms, drops at seeded
+    uniform centres); with indices, only those boxes."""
     from mhit36_mixedp_b200 import Params, synth
     rng = np.random.default_rng(99)
-    sizes = ENSEMBLE_SIZES
     boxes = []
-    for b, n in enumerate(sizes):
+    for b, n in enumerate(ENSEMBLE_SIZES):
         nu = float(rng.uniform(0.002, 0.01))
         we = float(rng.uniform(0.5, 5.0))
         ndrops = int(rng.integers(32, 257))
         if indices is not None and b not in indices:
             continue
-        u, v, w = synth.solenoidal_velocity(n, 100 + b)
-        phi = synth.drops_phi(n, synth.drop_centres(ndrops, 100 + b), 0.3, 2 * math.pi / n)
         prm = Params(nx=n, dt=2e-4, mu=nu, rho=1.0, radius=0.3, sigma=synth.sigma_from_weber(1.0, 1.0, 0.3, we),
                      phiflag=1, poisson="fp32", acdi_clamp=1)
-        boxes.append((prm, u, v, w, phi))
+        boxes.append((prm, 100 + b, synth.drop_centres(ndrops, 100 + b)))
     return boxes
 
 
@@ -286,11 +316,29 @@ def partition_boxes(sizes, nranks):
     return [sorted(p) for p in parts]
 
 
+def ensemble_measure(indices, device, steps, warmup):
+    """Advance the given boxes of the 32-box ensemble as one ensemble on `device` and time `steps`
+    graph-launched ensemble steps.  Returns (ms per step, tuning, clocks)."""
+    from mhit36_mixedp_b200 import Ensemble
+    boxes = ensemble_workload(set(indices))
+    for b in boxes:
+        b[0].device = device
+    with Ensemble([b[0] for b in boxes]) as ens:
+        tuning = ens.autotune(trials=2)
+        for box, (prm, seed, centres) in zip(ens.boxes, boxes):
+            box.init_solenoidal(seed=seed, kmax=4)
+            box.init_drops(centres, prm.radius)
+        ens.step(max(warmup, 3))
+        with Clocks(device) as clk:
+            ms = ens.time_steps(steps)
+        ens.step(0)
+    return ms / steps, tuning, clk.summary()
+
+
 def run_ensemble(args):
     """The 32-box ensemble; under torchrun the boxes are shared out over the ranks (strong
     scaling: the same 32 boxes whatever N), each rank steps its share as one ensemble, and the
     step time is the max over ranks."""
-    from mhit36_mixedp_b200 import Ensemble
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -304,32 +352,19 @@ def run_ensemble(args):
         dist = tdist
     mine = partition_boxes(ENSEMBLE_SIZES, world)[rank]
     ms, tuning, clocks = 0.0, None, None
-    if mine:
-        boxes = ensemble_workload(set(mine))
-        for b in boxes:
-            b[0].device = local
-        with Ensemble([b[0] for b in boxes]) as ens:
-            tuning = ens.autotune(trials=2)
-            for box, (prm, u, v, w, phi) in zip(ens.boxes, boxes):
-                box.upload(u, v, w, phi)
-            ens.step(max(args.warmup, 3))
-            if dist:
-                dist.barrier()
-            with Clocks(local) as clk:
-                ms = ens.time_steps(args.steps)
-            ens.step(0)
-            clocks = clk.summary()
-    elif dist:
+    if dist:
         dist.barrier()
+    if mine:
+        ms, tuning, clocks = ensemble_measure(mine, local, args.steps, args.warmup)
     if dist:
         ms = max_over_ranks([ms], dist, f"cuda:{local}")[0]
         dist.barrier()
     if rank == 0:
         npts = sum(n ** 3 for n in ENSEMBLE_SIZES)
         peak, kind = peaks()
-        frac = STEP_BYTES["fp32"] * npts / (ms / args.steps * 1e-3) / 1e9 / peak / world
+        frac = STEP_BYTES["fp32"] * npts / (ms * 1e-3) / 1e9 / peak / world
         line = {"metric": "ms per ensemble step, 32 NS+ACDI boxes (16x64^3, 10x128^3, 6x192^3), FP32 Poisson",
-                "value": ms / args.steps, "unit": "ms/timestep", "n_gpus": world, "steps": args.steps,
+                "value": ms, "unit": "ms/timestep", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "higher_is_better": False, "scaling": "strong", "data": "synthetic",
                 "dtype": "f64+f32",
                 "config": {"workload": "ensemble", "boxes": len(ENSEMBLE_SIZES), "points": npts,
@@ -341,64 +376,123 @@ def run_ensemble(args):
     return 0
 
 
-def run_large_ns(args):
-    """1024^3 NS (no phase field), FP32 against FP64 Poisson, nu = 8e-4: the seeded random
-    solenoidal velocity (seed 4, 0 < |k| <= 4, unit rms) synthesised on the device (its host
-    version would need tens of GB of host memory at this size), ABC forcing on."""
+def large_ns_measure(n, device, steps, warmup):
+    """n^3 NS (no phase field), FP32 and FP64 Poisson, nu = 8e-4: the seeded random solenoidal
+    velocity (seed 4, 0 < |k| <= 4, unit rms) synthesised on the device (its host version would
+    need tens of GB of host memory at 1024^3), ABC forcing on."""
     from mhit36_mixedp_b200 import Params, Solver
-    n = 1024 if args.n == 512 else args.n
     prm = dict(nx=n, dt=2e-4, mu=8e-4, rho=1.0, f1=1.0, f2=1.0, f3=1.0, k0=2.0)
     res = {}
+    peak, _ = peaks()
+    ns_bytes = {"fp32": 192, "fp64": 216}  # NS step model: 192 / 216 B per point
     for mode in ("fp32", "fp64"):
-        with Solver(Params(poisson=mode, **prm)) as s:
+        with Solver(Params(device=device, poisson=mode, **prm)) as s:
             s.init_solenoidal(seed=4, kmax=4)
-            s.step(max(args.warmup, 3))
-            with Clocks(0) as clk:
-                ms = s.time_steps(args.steps)
+            s.step(max(warmup, 3))
+            with Clocks(device) as clk:
+                ms = s.time_steps(steps)
             s.step(0)
             prof = s.profile_step()
             dg = s.diagnostics()
-        res[mode] = {"ms_per_step": ms / args.steps, "stages_ms": prof, "maxdiv": dg["maxdiv"], "ke": dg["ke"],
+        res[mode] = {"ms_per_step": ms / steps, "stages_ms": prof, "maxdiv": dg["maxdiv"], "ke": dg["ke"],
+                     "step_roofline_frac": ns_bytes[mode] * n ** 3 / (ms / steps * 1e-3) / 1e9 / peak,
                      "clocks": clk.summary()}
-    peak, kind = peaks()
-    npts = n ** 3
-    ns_bytes = {"fp32": 192, "fp64": 216}  # NS step model: 192 / 216 B per point
-    for mode in res:
-        res[mode]["step_roofline_frac"] = ns_bytes[mode] * npts / (res[mode]["ms_per_step"] * 1e-3) / 1e9 / peak
+    return res
+
+
+def run_large_ns(args):
+    n = 1024 if args.n == 512 else args.n
+    res = large_ns_measure(n, 0, args.steps, args.warmup)
     line = {"metric": f"ms/timestep {n}^3 NS, 1 B200, FP32 vs FP64 Poisson", "value": res["fp32"]["ms_per_step"],
             "unit": "ms/timestep", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
             "data": "synthetic (seeded solenoidal modes 0<|k|<=4, seed 4, built on the device)", "dtype": "f64+f32",
             "config": {"workload": f"NS {n}^3, nu=8e-4, dt=2e-4", "l2": "inputs larger than L2"},
-            "fp64_ms_per_step": res["fp64"]["ms_per_step"], "detail": res, "peak_kind": kind}
+            "fp64_ms_per_step": res["fp64"]["ms_per_step"], "detail": res, "peak_kind": peaks()[1]}
     print(json.dumps(line), flush=True)
     return 0
 
 
-def run_tracers(args):
-    """512^3 NS+ACDI with 1e6 tracers, FP64 Poisson, both interpolation modes."""
+def tracers_measure(fields, device, steps, warmup, npart=1_000_000):
+    """512^3 NS+ACDI with 1e6 uniform tracers (seed 3): FP64 Poisson with both interpolation modes
+    and FP32 Poisson with trilinear interpolation."""
     from mhit36_mixedp_b200 import Params, Solver, synth
-    n = args.n
-    prm, u, v, w, phi = workload(n)
-    npart = 1_000_000
+    prm, u, v, w, phi = fields
     part = synth.uniform_particles(npart, 3)
     prm = dict(prm, partflag=1, npart=npart)
     res = {}
-    for interp in ("linear1d", "trilinear"):
-        with Solver(Params(poisson="fp64", interp=interp, **prm)) as s:
+    for poisson, interp in (("fp64", "linear1d"), ("fp64", "trilinear"), ("fp32", "trilinear")):
+        with Solver(Params(device=device, poisson=poisson, interp=interp, **prm)) as s:
             s.upload(u, v, w, phi)
             s.upload_particles(part)
-            s.step(max(args.warmup, 3))
-            ms = s.time_steps(args.steps)
+            s.step(max(warmup, 3))
+            with Clocks(device) as clk:
+                ms = s.time_steps(steps)
             s.step(0)
             prof = [s.profile_step() for _ in range(3)]
-        tr = statistics.mean(p["k_tracer"] for p in prof if "k_tracer" in p) if "k_tracer" in prof[0] else None
-        res[interp] = {"ms_per_step": ms / args.steps, "tracer_stage_ms": tr}
-    line = {"metric": f"ms/timestep {n}^3 NS+ACDI + 1e6 tracers, 1 B200, FP64 Poisson",
-            "value": res["linear1d"]["ms_per_step"], "unit": "ms/timestep", "n_gpus": 1, "steps": args.steps,
+        tr = statistics.mean(p["k_tracer"] for p in prof)
+        res[f"{poisson}_{interp}"] = {"ms_per_step": ms / steps, "tracer_stage_ms": tr, "clocks": clk.summary()}
+    return res
+
+
+def run_tracers(args):
+    fields = workload(args.n)
+    res = tracers_measure(fields, 0, args.steps, args.warmup)
+    line = {"metric": f"ms/timestep {args.n}^3 NS+ACDI + 1e6 tracers, 1 B200",
+            "value": res["fp64_linear1d"]["ms_per_step"], "unit": "ms/timestep", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "higher_is_better": False, "data": "synthetic", "dtype": "f64",
-            "config": {"workload": f"NS+ACDI {n}^3 + 1e6 uniform tracers (seed 3)"}, "detail": res}
+            "config": {"workload": f"NS+ACDI {args.n}^3 + 1e6 uniform tracers (seed 3)"}, "detail": res}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def run_reference(args):
+    """--impl reference: the reference's loop on the host cores.  The reference itself is Fortran
+    + OpenACC + cuDecomp with no Fortran compiler on this image, so its CPU implementation is the C
+    restatement (kind "port") on the bench workload at the same size and Poisson precision as the
+    GPU arm's value, timed on all host threads.  Under torchrun only rank 0 runs."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    fields = workload(args.n)
+    ms, nwarm, ntimed, cores = cpu_reference(fields, args.warmup, args.steps, REFERENCE_BUDGET_S)
+    cb = {"value": ms, "unit": "ms/timestep", "cores": cores, "kind": "port",
+          "sample": f"the whole bench workload ({args.n}^3 NS+ACDI, FP32 Poisson), {nwarm} untimed step(s) "
+                    f"including the Euler step, {ntimed} timed AB2 step(s), mean; C/OpenMP restatement of "
+                    f"multi/main.f90:456-1007"}
+    line = {"impl": "reference", "metric": METRIC, "value": ms, "unit": "ms/timestep", "n_gpus": args.gpus,
+            "steps": ntimed, "warmup": nwarm, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic", "config": headline_config(args.n, world),
+            "requested": {"steps": args.steps, "warmup": args.warmup}, "cpu_baseline": cb,
+            "e2e": {"value": ms, "unit": "ms/timestep", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# wall-clock budget of the reference arm's steps (about a minute on a 16-core host at 512^3)
+REFERENCE_BUDGET_S = 120.0
+# the GPU arm's CPU-baseline sample: one Euler + a few AB2 steps of the same workload
+CPU_SAMPLE_BUDGET_S = 15.0
+
+
+def measure_configs(args, dev, fields):
+    """The other scope-table configurations, compact: 1024^3 NS (FP32 / FP64 Poisson), 512^3
+    NS+ACDI + 1e6 tracers, the 32-box ensemble.  A failure is reported in its entry."""
+    out = {}
+    jobs = (("ns_1024", large_ns_measure, (1024, dev, min(args.steps, 5), 3)),
+            ("tracers_1e6", tracers_measure, (fields, dev, min(args.steps, 10), 3)),
+            ("ensemble_32", ensemble_measure, (range(len(ENSEMBLE_SIZES)), dev, args.steps, args.warmup)))
+    for name, fn, fargs in jobs:
+        try:
+            out[name] = fn(*fargs)
+        except Exception as ex:  # pragma: no cover - reported, not hidden
+            out[name] = {"error": str(ex)}
+    e = out["ensemble_32"]
+    if isinstance(e, tuple):
+        ms, tuning, clocks = e
+        npts = sum(m ** 3 for m in ENSEMBLE_SIZES)
+        out["ensemble_32"] = {"ms_per_step": ms, "tuning": tuning, "clocks": clocks,
+                              "step_roofline_frac": STEP_BYTES["fp32"] * npts / (ms * 1e-3) / 1e9 / peaks()[0]}
+    return out
 
 
 def main():
@@ -409,6 +503,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--n", type=int, default=512)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="only the headline configuration")
     ap.add_argument("--ensemble", action="store_true", help="time the 32-box ensemble instead")
     ap.add_argument("--workload", choices=["acdi", "ns-large", "tracers"], default="acdi",
                     help="acdi: the headline NS+ACDI step; ns-large: 1024^3 NS; tracers: + 1e6 tracers")
@@ -419,31 +514,11 @@ def main():
         return run_large_ns(args)
     if args.workload == "tracers":
         return run_tracers(args)
+    if args.impl == "reference":
+        return run_reference(args)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-
-    if args.impl == "reference":
-        if rank != 0:
-            return 0
-        times = []
-        for _ in range(args.warmup):
-            pass
-        cb = None
-        for _ in range(max(1, min(args.steps, 2))):
-            cb = cpu_sample()
-            times.append(cb["value"])
-        val = min(times)
-        cb["value"] = val
-        line = {"impl": "reference", "metric": METRIC, "value": val, "unit": "ms/timestep", "n_gpus": args.gpus,
-                "steps": args.steps, "warmup": args.warmup, "ms_per_step": val, "higher_is_better": False,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic",
-                "config": {"workload": "NS+ACDI 512^3, 64 drops, FP32 Poisson", "sample": cb["sample"]},
-                "cpu_baseline": cb, "e2e": {"value": val, "unit": "ms/timestep", "h2d_bytes_per_step": 0,
-                                             "d2h_bytes_per_step": 0}}
-        print(json.dumps(line), flush=True)
-        return 0
-
     dist = None
     if world > 1:
         import datetime
@@ -453,13 +528,15 @@ def main():
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
         dist = tdist
     dev = local
+    fields = workload(args.n)
     if dist:
         dist.barrier()
-    res, e2e = run_ours(args, rank, world, dev)
+    res, e2e = run_ours(args, rank, world, dev, fields)
     ms32, ms64 = res["fp32"]["ms"], res["fp64"]["ms"]
     if dist:
         ms32, ms64 = max_over_ranks([ms32, ms64], dist, f"cuda:{local}")
         dist.barrier()
+    extras = measure_configs(args, dev, fields) if world == 1 and not args.no_extras else None
     if rank == 0:
         n = args.n
         npts = n ** 3
@@ -473,30 +550,30 @@ def main():
             traffic = TRAFFIC_PER_POINT[dom] * npts
         roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                "traffic_how": f"ncu DRAM bytes per cell of a {TRAFFIC_SOURCE.get(dom, '512x512x256')} capture of "
+                               f"{dom} x the {n}^3 cells (scaled, not measured in this run)",
                 "algorithmic_bytes_per_launch": dom_bytes, "launch_ms": st[dom]}
         step_roof = {m: STEP_BYTES[m] * npts / (res[m]["ms"] * 1e-3) / 1e9 / peak for m in ("fp32", "fp64")}
         cb = None
-        if not args.no_cpu_baseline:
+        if not args.no_cpu_baseline and world == 1:
             try:
-                cb = cpu_sample()
+                cb = cpu_baseline_line(fields, 1, 3, CPU_SAMPLE_BUDGET_S)
             except Exception as ex:
                 cb = {"value": None, "error": str(ex)}
-        clocks = res["fp32"]["clocks"]
         line = {
             "metric": METRIC, "value": ms32, "unit": "ms/timestep", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms32, "higher_is_better": False, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic",
-            "config": {"workload": f"NS+ACDI {n}^3, 64 drops R=0.3 eps=dx, We=1, nu=0.003, dt=2e-4, "
-                                   f"seeds drops=1 vel=2; value: FP32 Poisson (mixed)",
-                       "parallelism": "replicas" if world > 1 else "single", "l2": "inputs larger than L2"},
+            "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic", "config": headline_config(n, world),
             "fp64_ms_per_step": ms64, "mixed_speedup_vs_fp64": ms64 / ms32,
             "maxdiv": {"fp32": res["fp32"]["diag"]["maxdiv"], "fp64": res["fp64"]["diag"]["maxdiv"]},
             "dissipation": {"fp32": res["fp32"]["diag"]["dissipation"], "fp64": res["fp64"]["diag"]["dissipation"]},
             "step_roofline_frac": step_roof, "stages_ms": {m: res[m]["stages"] for m in ("fp32", "fp64")},
             "roofline": roof, "cpu_baseline": cb, "e2e": e2e,
-            "gpu_launches": 9 * args.steps, "clocks": clocks,
+            "gpu_launches": res["fp32"]["kernels_per_step"] * args.steps,
+            "kernels_per_step": {m: res[m]["kernels_per_step"] for m in ("fp32", "fp64")},
+            "clocks": res["fp32"]["clocks"], "clocks_fp64": res["fp64"]["clocks"],
             "modified_laplacian": res["modified"], "drop_labelling": res.get("drops"),
-            "energy_spectrum": res.get("spectrum"),
+            "energy_spectrum": res.get("spectrum"), "configs": extras,
         }
         print(json.dumps(line), flush=True)
     if dist:

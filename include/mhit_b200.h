@@ -217,6 +217,9 @@ int mhit_label_drops(mhit_ctx* ctx, double thresh, int connectivity, mhit_drop* 
  * NULL) receives static strings; *nstages is in/out (capacity / count). */
 int mhit_time_steps(mhit_ctx* ctx, int nsteps, double* ms);
 int mhit_profile_step(mhit_ctx* ctx, double* ms, const char** names, int* nstages);
+/* Number of kernels one step after the first launches: the kernel nodes of the captured step
+ * graph (captured here if no step has needed it yet). */
+int mhit_kernels_per_step(mhit_ctx* ctx, int* n);
 
 /* Ensemble of independent boxes of uneven sizes (the reference runs one box per job; this is
  * the batched mode of its timestep loop).  Every box is a full context -- upload, download,
@@ -274,19 +277,27 @@ int mhit_ensemble_tuning(mhit_ensemble* e, int* nlanes, int* zchunk_phase, int* 
  * already holds, or a run with the GPU's memory nearly fully committed, where an extra cudaMalloc
  * can fail and a cudaFree synchronises the device.  Computes, from caller-owned device arrays
  * u, v, w (x-fastest nx*ny*nz float64), stats[0] = max|div u|, stats[1] = KE = 0.5 <u.u>,
- * stats[2] = 2 nu <S_ij S_ij> -- the same quantities as mhit_diagnostics -- into the caller's
- * device array stats[3], on `stream` (a cudaStream_t, NULL for the default stream).
+ * stats[2] = 2 nu <S_ij S_ij> -- the formulas of mhit_diagnostics, applied to the arrays as
+ * passed (no mean is removed; mhit_diagnostics first subtracts its context's lazily removed
+ * mean, so the two agree on downloaded or zero-mean fields) -- into the caller's device array
+ * stats[3], on `stream` (a cudaStream_t, NULL for the default stream).  A NaN in u, v or w
+ * gives NaN in stats[0] and stats[1].
  * It calls no cudaMalloc/cudaFree: its only scratch is a file-scope device array with one slot
  * per z plane, so nz may not exceed MHIT_STATS_NOALLOC_MAX_PLANES (MHIT_ERR_ARG otherwise).
- * The first call on a device looks up that array's device address (cudaGetSymbolAddress, no
- * allocation); make that first call before any stream capture.  All calls share the array:
- * calls whose kernels overlap on the GPU race and must be serialised by the caller. */
+ * The first call on a device (and the first after the device's CUDA context changed, e.g. after
+ * cudaDeviceReset) looks up that array's device address (cudaGetSymbolAddress, no allocation);
+ * make that first call before any stream capture.  All calls share the array: calls whose
+ * kernels overlap on the GPU race and must be serialised by the caller. */
 #define MHIT_STATS_NOALLOC_MAX_PLANES 1024
 int mhit_field_stats_noalloc(int nx, int ny, int nz, double nu, const double* u, const double* v, const double* w,
                              double* stats, void* stream);
 
 int mhit_debug_run_stage(mhit_ctx* ctx, int stage);
 int mhit_debug_commit_step(mhit_ctx* ctx);
+/* Iteration bound of mhit_label_drops' union-find loops (0, the default: the cell count, which
+ * no parent chain or link retry sequence can exceed).  A small bound makes a legitimate chain
+ * run out, so a test can drive the bounded-loop error path (MHIT_ERR_STATE) without a fault. */
+int mhit_debug_set_label_bound(mhit_ctx* ctx, long long bound);
 long long mhit_debug_buffer_len(mhit_ctx* ctx, int which);
 int mhit_debug_get_buffer(mhit_ctx* ctx, int which, double* out);
 

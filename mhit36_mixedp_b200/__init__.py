@@ -1,8 +1,9 @@
 """B200-native (sm_100a) MHIT36 timestep hot path behind a C ABI.
 
 ``libmhit_b200.so`` (built from ``csrc/`` by ``build.py``) holds the CUDA kernels and the C ABI
-declared in ``include/mhit_b200.h``; ``api`` is the Python host side over it, ``fieldio`` the
-reference's field-file and input formats, ``synth`` the seeded synthetic initial conditions.
+declared in ``include/mhit_b200.h``; ``api`` is the Python host side over it (including the
+reference's field-file and ``input.inp`` formats, read and written by the library), ``run`` the
+time loop of ``program main``, ``synth`` the seeded synthetic initial conditions.
 """
 from .api import (Ensemble, FIELD_P, FIELD_PHI, FIELD_U, FIELD_V, FIELD_W, MhitArgError, MhitCFLError,
                   MhitCudaError, MhitError, MhitIOError, MhitNaNError, MhitStateError, Params,

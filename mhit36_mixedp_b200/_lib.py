@@ -18,6 +18,7 @@ MHIT_ERR_NAN = -3
 MHIT_ERR_CFL = -4
 MHIT_ERR_IO = -5
 MHIT_ERR_STATE = -6
+MHIT_STATS_NOALLOC_MAX_PLANES = 1024  # include/mhit_b200.h
 
 POISSON = {"fp64": 0, "fp32": 1, "fp32_refined": 2}
 LAPLACIAN = {"exact": 0, "modified": 1}
@@ -84,6 +85,7 @@ SIGNATURES = {
                                     _c.c_void_p]),
     "mhit_time_steps": (_c.c_int, [_c.c_void_p, _c.c_int, _dp]),
     "mhit_profile_step": (_c.c_int, [_c.c_void_p, _dp, _P(_c.c_char_p), _P(_c.c_int)]),
+    "mhit_kernels_per_step": (_c.c_int, [_c.c_void_p, _P(_c.c_int)]),
     "mhit_ensemble_create": (_c.c_int, [_P(MhitParams), _c.c_int, _P(_c.c_void_p)]),
     "mhit_ensemble_destroy": (None, [_c.c_void_p]),
     "mhit_ensemble_box": (_c.c_int, [_c.c_void_p, _c.c_int, _P(_c.c_void_p)]),
@@ -95,6 +97,7 @@ SIGNATURES = {
                                             _c.c_void_p, _c.c_void_p, _c.c_void_p]),
     "mhit_debug_run_stage": (_c.c_int, [_c.c_void_p, _c.c_int]),
     "mhit_debug_commit_step": (_c.c_int, [_c.c_void_p]),
+    "mhit_debug_set_label_bound": (_c.c_int, [_c.c_void_p, _c.c_longlong]),
     "mhit_debug_buffer_len": (_c.c_longlong, [_c.c_void_p, _c.c_int]),
     "mhit_debug_get_buffer": (_c.c_int, [_c.c_void_p, _c.c_int, _dp]),
 }

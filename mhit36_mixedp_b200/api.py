@@ -326,6 +326,12 @@ class Solver:
         _check(self._lib.mhit_time_steps(self._ctx, int(nsteps), ctypes.byref(ms)))
         return ms.value
 
+    def kernels_per_step(self) -> int:
+        """Kernels one step after the first launches (nodes of the captured step graph)."""
+        n = ctypes.c_int()
+        _check(self._lib.mhit_kernels_per_step(self._ctx, ctypes.byref(n)))
+        return n.value
+
     # -------------------------------------------------------------- test hooks
     def run_stage(self, stage: str):
         """Run one stage of the step being built (see mhit_debug_run_stage)."""

@@ -47,6 +47,10 @@ struct Geo {
   double f1, f2, f3;
 };
 
+// max that propagates NaN (fmax returns the other operand): a NaN anywhere in a reduced field
+// shows up in the reduced maximum
+__device__ __forceinline__ double nanmax(double a, double b) { return (a != a) ? a : ((b != b) ? b : fmax(a, b)); }
+
 __device__ __forceinline__ int wrapp(int i, int n) { return (i + 1 == n) ? 0 : i + 1; }
 __device__ __forceinline__ int wrapm(int i, int n) { return (i == 0) ? n - 1 : i - 1; }
 __device__ __forceinline__ size_t lin(int i, int j, int k, int nx, int ny) {

@@ -213,7 +213,8 @@ cudaError_t launch_correct(const CorrectArgs& a, cudaStream_t st) {
 
 // ------------------------------------------------------------------ diagnostics
 // max |div u| (the operator of :841-843 without rho/dt), kinetic energy, and the dissipation
-// 2 nu <S_ij S_ij> with central differences (post/compute_diss/main.f90:72-117).
+// 2 nu <S_ij S_ij> with central differences (post/compute_diss/main.f90:72-117).  The maximum
+// propagates NaN, so a NaN velocity gives a NaN max|div| as well as a NaN KE.
 __global__ void __launch_bounds__(CNT) k_diag(DiagArgs a) {
   const Geo& g = a.g;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
@@ -235,7 +236,7 @@ __global__ void __launch_bounds__(CNT) k_diag(DiagArgs a) {
     const double u0 = F(U, mu_, i, j, k), v0 = F(V, mv_, i, j, k), w0 = F(W, mw_, i, j, k);
     const double div = (F(U, mu_, ip, j, k) - u0) * dxi + (F(V, mv_, i, jp, k) - v0) * dxi +
                        (F(W, mw_, i, j, kp) - w0) * dxi;
-    mdiv = fmax(mdiv, fabs(div));
+    mdiv = nanmax(mdiv, fabs(div));
     ke += u0 * u0 + v0 * v0 + w0 * w0;
     const double dudx = (F(U, mu_, ip, j, k) - F(U, mu_, im, j, k)) * h;
     const double dudy = (F(U, mu_, i, jp, k) - F(U, mu_, i, jm, k)) * h;
@@ -258,7 +259,7 @@ __global__ void __launch_bounds__(CNT) k_diag(DiagArgs a) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
       const double y = __shfl_down_sync(0xffffffffu, x, o);
-      x = q == 0 ? fmax(x, y) : x + y;
+      x = q == 0 ? nanmax(x, y) : x + y;
     }
     if ((threadIdx.x & 31) == 0) red[q][threadIdx.x >> 5] = x;
   }
@@ -266,7 +267,7 @@ __global__ void __launch_bounds__(CNT) k_diag(DiagArgs a) {
   if (threadIdx.x < 3) {
     const int q = threadIdx.x;
     double x = red[q][0];
-    for (int wv = 1; wv < CNT / 32; ++wv) x = q == 0 ? fmax(x, red[q][wv]) : x + red[q][wv];
+    for (int wv = 1; wv < CNT / 32; ++wv) x = q == 0 ? nanmax(x, red[q][wv]) : x + red[q][wv];
     a.partials[(size_t)blockIdx.x * 4 + q] = x;
   }
 }
@@ -276,7 +277,7 @@ __global__ void __launch_bounds__(1024) k_diag_finalize(const double* __restrict
   __shared__ double red[3][32];
   double vals[3] = {0.0, 0.0, 0.0};
   for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
-    vals[0] = fmax(vals[0], partials[(size_t)b * 4 + 0]);
+    vals[0] = nanmax(vals[0], partials[(size_t)b * 4 + 0]);
     vals[1] += partials[(size_t)b * 4 + 1];
     vals[2] += partials[(size_t)b * 4 + 2];
   }
@@ -286,7 +287,7 @@ __global__ void __launch_bounds__(1024) k_diag_finalize(const double* __restrict
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
       const double y = __shfl_down_sync(0xffffffffu, x, o);
-      x = q == 0 ? fmax(x, y) : x + y;
+      x = q == 0 ? nanmax(x, y) : x + y;
     }
     if ((threadIdx.x & 31) == 0) red[q][threadIdx.x >> 5] = x;
   }
@@ -296,7 +297,7 @@ __global__ void __launch_bounds__(1024) k_diag_finalize(const double* __restrict
     double r[3];
     for (int q = 0; q < 3; ++q) {
       double x = red[q][0];
-      for (int wv = 1; wv < nw; ++wv) x = q == 0 ? fmax(x, red[q][wv]) : x + red[q][wv];
+      for (int wv = 1; wv < nw; ++wv) x = q == 0 ? nanmax(x, red[q][wv]) : x + red[q][wv];
       r[q] = x;
     }
     const double n = (double)g.nx * g.ny * g.nz;

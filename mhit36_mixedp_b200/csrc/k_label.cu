@@ -63,7 +63,7 @@ __global__ void k_lab_init(const double* __restrict__ phi, double thresh, int* _
     lab[c] = phi[c] >= thresh ? c : -1;  // post/unionfind_periodic/main.f90:141
 }
 
-__global__ void k_lab_merge(int* lab, int nx, int ny, int nz, int nfwd, int* err) {
+__global__ void k_lab_merge(int* lab, int nx, int ny, int nz, int nfwd, long long bound, int* err) {
   const int n = nx * ny * nz;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
     if (lab[c] < 0) continue;
@@ -74,14 +74,14 @@ __global__ void k_lab_merge(int* lab, int nx, int ny, int nz, int nfwd, int* err
       jj = jj < 0 ? jj + ny : (jj >= ny ? jj - ny : jj);
       kk = kk >= nz ? kk - nz : kk;
       const int d = (kk * ny + jj) * nx + ii;
-      if (d != c && lab[d] >= 0) unite(lab, c, d, n, err);
+      if (d != c && lab[d] >= 0) unite(lab, c, d, bound, err);
     }
   }
 }
 
-__global__ void k_lab_flatten(int* lab, int n, int* err) {
+__global__ void k_lab_flatten(int* lab, int n, long long bound, int* err) {
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
-    if (lab[c] >= 0) lab[c] = find_root(lab, c, n, err);
+    if (lab[c] >= 0) lab[c] = find_root(lab, c, bound, err);
 }
 
 // roots per chunk of LCHUNK consecutive cells (one block per chunk)
@@ -206,8 +206,11 @@ cudaError_t launch_label_components(const LabelArgs& a, cudaStream_t st) {
   const int n = a.nx * a.ny * a.nz;
   const int grid = 148 * 8;
   k_lab_init<<<grid, 256, 0, st>>>(a.phi, a.thresh, a.lab, n);
-  k_lab_merge<<<grid, 256, 0, st>>>(a.lab, a.nx, a.ny, a.nz, a.connectivity == 26 ? 13 : 3, a.err);
-  k_lab_flatten<<<grid, 256, 0, st>>>(a.lab, n, a.err);
+  // the loops' bound: the cell count (no chain or retry sequence is longer), or a smaller test
+  // bound that makes a legitimate chain run out and exercises the error path
+  const long long bound = a.bound > 0 ? a.bound : n;
+  k_lab_merge<<<grid, 256, 0, st>>>(a.lab, a.nx, a.ny, a.nz, a.connectivity == 26 ? 13 : 3, bound, a.err);
+  k_lab_flatten<<<grid, 256, 0, st>>>(a.lab, n, bound, a.err);
   k_lab_count<<<label_chunks(n), LTHREADS, 0, st>>>(a.lab, n, a.counts);
   return cudaGetLastError();
 }

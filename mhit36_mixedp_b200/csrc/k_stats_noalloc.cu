@@ -10,11 +10,18 @@
 // and the only scratch is the file-scope array below, one partial-result slot per z plane.
 //
 // The array lives in every GPU that loads the library until the process exits (32 KB).  Its
-// host-side symbol is not a device address: the address is looked up once per device with
-// cudaGetSymbolAddress, by the first call made on that device.  All calls share the array:
-// two calls whose kernels overlap on the GPU (different streams, or different host threads on
-// the same device) race on it and must be serialised by the caller.  Each call writes the slots
-// of planes 0..nz-1 before it reads them, so nothing has to start at zero.
+// host-side symbol is not a device address: the address is looked up with cudaGetSymbolAddress
+// by the first call made on a device, and again whenever the CUDA context current on that
+// device has changed since (after a cudaDeviceReset the old address belongs to a destroyed
+// context).  All calls share the array: two calls whose kernels overlap on the GPU (different
+// streams, or different host threads on the same device) race on it and must be serialised by
+// the caller.  Each call writes the slots of planes 0..nz-1 before it reads them, so nothing has
+// to start at zero.
+//
+// The kinetic energy is that of the arrays as passed: no mean is removed (mhit_diagnostics
+// subtracts its context's lazily removed mean first; on fields downloaded from a context, or
+// with zero mean, the two agree).  A NaN anywhere in u, v or w makes stats[0] (and stats[1])
+// NaN: the maxima propagate NaN instead of dropping it.
 #include <cmath>
 #include <cstdio>
 #include <mutex>
@@ -50,7 +57,7 @@ __global__ void __launch_bounds__(STATS_NT) k_stats_planes(int nx, int ny, int n
 #define F(A, ii, jj, kk) __ldg(A + lin(ii, jj, kk, nx, ny))
     const double u0 = F(U, i, j, k), v0 = F(V, i, j, k), w0 = F(W, i, j, k);
     const double div = (F(U, ip, j, k) - u0) * dxi + (F(V, i, jp, k) - v0) * dxi + (F(W, i, j, kp) - w0) * dxi;
-    mdiv = fmax(mdiv, fabs(div));
+    mdiv = nanmax(mdiv, fabs(div));
     ke += u0 * u0 + v0 * v0 + w0 * w0;
     const double dudx = (F(U, ip, j, k) - F(U, im, j, k)) * h;
     const double dudy = (F(U, i, jp, k) - F(U, i, jm, k)) * h;
@@ -73,7 +80,7 @@ __global__ void __launch_bounds__(STATS_NT) k_stats_planes(int nx, int ny, int n
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
       const double y = __shfl_down_sync(0xffffffffu, x, o);
-      x = q == 0 ? fmax(x, y) : x + y;
+      x = q == 0 ? nanmax(x, y) : x + y;
     }
     if ((threadIdx.x & 31) == 0) red[q][threadIdx.x >> 5] = x;
   }
@@ -81,7 +88,7 @@ __global__ void __launch_bounds__(STATS_NT) k_stats_planes(int nx, int ny, int n
   if (threadIdx.x < 3) {
     const int q = threadIdx.x;
     double x = red[q][0];
-    for (int wv = 1; wv < STATS_NT / 32; ++wv) x = q == 0 ? fmax(x, red[q][wv]) : x + red[q][wv];
+    for (int wv = 1; wv < STATS_NT / 32; ++wv) x = q == 0 ? nanmax(x, red[q][wv]) : x + red[q][wv];
     slots[(size_t)k * STATS_SLOT + q] = x;
   }
 }
@@ -92,7 +99,7 @@ __global__ void __launch_bounds__(1024) k_stats_reduce(const double* __restrict_
   __shared__ double red[3][32];
   double vals[3] = {0.0, 0.0, 0.0};
   for (int k = threadIdx.x; k < nz; k += blockDim.x) {
-    vals[0] = fmax(vals[0], slots[(size_t)k * STATS_SLOT + 0]);
+    vals[0] = nanmax(vals[0], slots[(size_t)k * STATS_SLOT + 0]);
     vals[1] += slots[(size_t)k * STATS_SLOT + 1];
     vals[2] += slots[(size_t)k * STATS_SLOT + 2];
   }
@@ -102,7 +109,7 @@ __global__ void __launch_bounds__(1024) k_stats_reduce(const double* __restrict_
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
       const double y = __shfl_down_sync(0xffffffffu, x, o);
-      x = q == 0 ? fmax(x, y) : x + y;
+      x = q == 0 ? nanmax(x, y) : x + y;
     }
     if ((threadIdx.x & 31) == 0) red[q][threadIdx.x >> 5] = x;
   }
@@ -112,7 +119,7 @@ __global__ void __launch_bounds__(1024) k_stats_reduce(const double* __restrict_
     double r[3];
     for (int q = 0; q < 3; ++q) {
       double x = red[q][0];
-      for (int wv = 1; wv < nw; ++wv) x = q == 0 ? fmax(x, red[q][wv]) : x + red[q][wv];
+      for (int wv = 1; wv < nw; ++wv) x = q == 0 ? nanmax(x, red[q][wv]) : x + red[q][wv];
       r[q] = x;
     }
     const double n = (double)nx * ny * nz;
@@ -123,19 +130,50 @@ __global__ void __launch_bounds__(1024) k_stats_reduce(const double* __restrict_
 }
 
 std::mutex g_scratch_mutex;
-void* g_scratch_addr[64] = {};
+struct ScratchSlot {
+  void* ctx = nullptr;   // CUDA context the address belongs to
+  void* addr = nullptr;  // device address of g_stats_scratch in that context
+};
+ScratchSlot g_scratch[64];
 
-// Device address of g_stats_scratch on the current device, looked up on first use.
+// The driver's cuCtxGetCurrent, reached through the runtime (the library links only cudart).
+using CtxGetCurrentFn = int (*)(void**);
+CtxGetCurrentFn ctx_get_current() {
+  static CtxGetCurrentFn fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<CtxGetCurrentFn>(p);
+  }
+  return fn;
+}
+
+void* current_context() {
+  void* ctx = nullptr;
+  CtxGetCurrentFn fn = ctx_get_current();
+  if (fn && fn(&ctx) != 0) ctx = nullptr;
+  return ctx;
+}
+
+// Device address of g_stats_scratch on the current device, looked up on the first call and
+// again whenever the current context differs from the one the cached address belongs to.
 int scratch_address(int dev, void** out) {
   if (dev < 0 || dev >= 64) return set_error(MHIT_ERR_ARG, "device ordinal out of range");
   std::lock_guard<std::mutex> lock(g_scratch_mutex);
-  if (!g_scratch_addr[dev]) {
+  ScratchSlot& slot = g_scratch[dev];
+  void* ctx = current_context();
+  if (!slot.addr || !ctx || ctx != slot.ctx) {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_stats_scratch);
     if (e != cudaSuccess) return set_cuda_error(e, "cudaGetSymbolAddress(g_stats_scratch)", __FILE__, __LINE__);
-    g_scratch_addr[dev] = p;
+    slot.addr = p;
+    slot.ctx = current_context();  // the lookup made the device's primary context current if none was
   }
-  *out = g_scratch_addr[dev];
+  *out = slot.addr;
   return MHIT_OK;
 }
 

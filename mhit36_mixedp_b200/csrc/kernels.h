@@ -123,6 +123,7 @@ struct LabelArgs {
   double* acc;                  // [ndrops][9]
   unsigned long long* cells;    // [ndrops]
   int* out;                     // label field (0 background, 1.. drop) or nullptr
+  long long bound = 0;          // iteration bound of the union-find loops (0: the cell count)
 };
 int label_chunks(int n);
 cudaError_t launch_label_components(const LabelArgs& a, cudaStream_t st);  // init, merge, flatten, count

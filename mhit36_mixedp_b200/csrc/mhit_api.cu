@@ -88,6 +88,8 @@ struct mhit_ctx {
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
   cudaEvent_t ev[2 * ST_COUNT] = {};
   int zchunk_phase = 0, zchunk_mom = 0;  // z planes per block of k_phase / k_mom (0: default)
+  long long label_bound = 0;              // test hook: union-find loop bound (0: the cell count)
+  int graph_kernels = 0;                  // kernel nodes in a captured step graph
 };
 
 // ------------------------------------------------------------------ helpers
@@ -318,6 +320,22 @@ static int build_graphs(mhit_ctx* c) {
     cudaError_t e = cudaStreamEndCapture(c->st, &graph);
     if (rc) return rc;
     if (e != cudaSuccess) return set_cuda_error(e, "cudaStreamEndCapture", __FILE__, __LINE__);
+    // count the kernels one replayed step launches (reported by mhit_kernels_per_step)
+    size_t nn = 0;
+    e = cudaGraphGetNodes(graph, nullptr, &nn);
+    std::vector<cudaGraphNode_t> nodes(nn);
+    if (e == cudaSuccess && nn) e = cudaGraphGetNodes(graph, nodes.data(), &nn);
+    int nk = 0;
+    for (size_t q = 0; e == cudaSuccess && q < nn; ++q) {
+      cudaGraphNodeType t;
+      e = cudaGraphNodeGetType(nodes[q], &t);
+      if (e == cudaSuccess && t == cudaGraphNodeTypeKernel) ++nk;
+    }
+    if (e != cudaSuccess) {
+      cudaGraphDestroy(graph);
+      return set_cuda_error(e, "cudaGraphGetNodes", __FILE__, __LINE__);
+    }
+    c->graph_kernels = nk;
     e = cudaGraphInstantiate(&c->gexec[par], graph, 0);
     cudaGraphDestroy(graph);
     if (e != cudaSuccess) return set_cuda_error(e, "cudaGraphInstantiate", __FILE__, __LINE__);
@@ -728,6 +746,15 @@ int mhit_time_steps(mhit_ctx* c, int nsteps, double* ms) {
   return MHIT_OK;
 }
 
+int mhit_kernels_per_step(mhit_ctx* c, int* n) {
+  int rc;
+  if ((rc = check_ctx(c))) return rc;
+  if (!n) return set_error(MHIT_ERR_ARG, "null argument");
+  if (!c->graph_built && (rc = build_graphs(c))) return rc;
+  *n = c->graph_kernels;
+  return MHIT_OK;
+}
+
 int mhit_profile_step(mhit_ctx* c, double* ms, const char** names, int* nstages) {
   int rc;
   if ((rc = check_ctx(c))) return rc;
@@ -965,6 +992,23 @@ int mhit_read_checkpoint(mhit_ctx* c, const char* path) {
       h.partflag != c->prm.partflag || h.poisson != c->prm.poisson || h.pbytes != (int32_t)tsize(c) ||
       h.np < 0 || h.nstep < 0)
     return set_error(MHIT_ERR_ARG, "checkpoint was written by a context of another size or mode");
+  // the whole file must be there before any device state changes: a truncated checkpoint
+  // leaves the context as it was
+  {
+    size_t want = sizeof(CkptHeader) + sizeof(DevScalars);
+    for (const CkptArray& a : ckpt_arrays(c)) want += a.bytes;
+    if (c->prm.partflag) want += (size_t)h.np * 12 * sizeof(double);
+    const long here = ftell(fc.f);
+    if (here < 0 || fseek(fc.f, 0, SEEK_END) != 0) return set_error(MHIT_ERR_IO, std::string("cannot seek in ") + path);
+    const long size = ftell(fc.f);
+    if (size < 0 || fseek(fc.f, here, SEEK_SET) != 0)
+      return set_error(MHIT_ERR_IO, std::string("cannot seek in ") + path);
+    if ((size_t)size != want) {
+      char b[160];
+      snprintf(b, sizeof(b), "checkpoint holds %ld bytes, its header needs %zu: ", size, want);
+      return set_error(MHIT_ERR_IO, std::string(b) + path);
+    }
+  }
   DevScalars s;
   if (fread(&s, sizeof(s), 1, fc.f) != 1) return set_error(MHIT_ERR_IO, std::string("short read from ") + path);
   MHIT_CUDA_TRY(cudaStreamSynchronize(c->st));
@@ -1067,6 +1111,7 @@ int mhit_label_drops(mhit_ctx* c, double thresh, int connectivity, mhit_drop* dr
   a.acc = nullptr;
   a.cells = nullptr;
   a.out = nullptr;
+  a.bound = c->label_bound;
   MHIT_CUDA_TRY(launch_label_components(a, c->st));
   std::vector<int> cnt(nch + 1);
   MHIT_CUDA_TRY(cudaMemcpyAsync(cnt.data(), counts, sizeof(int) * (nch + 1), cudaMemcpyDeviceToHost, c->st));
@@ -1321,6 +1366,13 @@ int mhit_debug_run_stage(mhit_ctx* c, int stage) {
   const bool first = c->nstep == 0;
   if ((rc = enqueue_stage(c, stage, first ? 1.0 : 1.5, first ? 0.0 : 0.5, c->cur))) return rc;
   MHIT_CUDA_TRY(cudaStreamSynchronize(c->st));
+  return MHIT_OK;
+}
+
+int mhit_debug_set_label_bound(mhit_ctx* c, long long bound) {
+  if (!c) return set_error(MHIT_ERR_ARG, "null context");
+  if (bound < 0) return set_error(MHIT_ERR_ARG, "bound must be >= 0");
+  c->label_bound = bound;
   return MHIT_OK;
 }
 

@@ -11,7 +11,7 @@
    NS FP32 Poisson; 10 steps each) so the GPU path and the oracle can both be checked
    against stored numbers.
 
-Usage: python tests/golden/make_golden.py [/path/to/reference]
+Usage: python tests/golden/make_golden.py /path/to/reference
 """
 import json
 import os
@@ -80,7 +80,9 @@ def oracle_fixtures():
 
 
 if __name__ == "__main__":
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <path to the reference checkout>")
+    ref = sys.argv[1]
     tg_curve(ref, 128)
     tg_curve(ref, 512)
     oracle_fixtures()

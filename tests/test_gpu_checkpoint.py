@@ -98,3 +98,18 @@ def test_checkpoint_rejects_other_sizes_and_files(gpu, tmp_path):
     with Solver(prm) as s:
         with pytest.raises(MhitIOError):
             s.read_checkpoint(str(short))
+    # a checkpoint cut off in its last array is rejected before any device state changes
+    cut = tmp_path / "cut.ckp"
+    cut.write_bytes(open(ck, "rb").read()[:-8])
+    prm_, u_, v_, w_, phi_ = case()[:5]
+    with Solver(prm) as s:
+        s.upload(u_, v_, w_, phi_)
+        s.step(2)
+        before = s.download()
+        nstep = s.diagnostics()["nstep"]
+        with pytest.raises(MhitIOError, match="needs"):
+            s.read_checkpoint(str(cut))
+        after = s.download()
+        assert s.diagnostics()["nstep"] == nstep
+        for k in before:
+            np.testing.assert_array_equal(after[k], before[k])

@@ -1,5 +1,8 @@
-"""Parity at the metric's size (512^3 NS+ACDI) through size-independent properties: the oracle
-cannot step 512^3 in seconds, so these check what holds at any size.
+"""Parity at the metric's size (512^3 NS+ACDI) through size-independent properties.
+
+The bench workload itself is compared step for step with the C oracle in
+tests/test_gpu_oracle_configs.py; these tests check, on a different input (an ABC velocity with
+six drops), the identities that hold at any size and that the oracle comparison does not show.
 
 * FP64 Poisson with the discrete Laplacian leaves a divergence at round-off
   (max |div| <= 1e-11 u_max n/2pi), the property that makes it the reference for matched
