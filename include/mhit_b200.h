@@ -43,6 +43,11 @@ extern "C" {
 #define MHIT_POISSON_FP32 1    /* this branch: rhs cast to FP32, FP32 transforms, FP32 pressure */
 #define MHIT_POISSON_FP32_REFINED 2 /* FP32 solve + one FP64 residual sweep (needs MHIT_LAP_MODIFIED):
                                        r = rhs - L_h p32 in FP64, L_h d = r in FP32, p = p32 + d */
+#define MHIT_POISSON_FP32_INCREMENTAL 3 /* one FP32 solve for the increment over the previous
+                                       step's pressure q (needs MHIT_LAP_MODIFIED): r = rhs - L_h q
+                                       in FP64, L_h d = r in FP32, p = q + d in FP64 for the
+                                       projection, q <- fl32(p) for the next step; q = 0 after an
+                                       upload or an initial-condition call */
 
 /* Laplacian symbol of the spectral divide */
 #define MHIT_LAP_EXACT 0       /* exact integer k^2, as multi/main.f90:889 */

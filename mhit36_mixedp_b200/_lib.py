@@ -20,7 +20,7 @@ MHIT_ERR_IO = -5
 MHIT_ERR_STATE = -6
 MHIT_STATS_NOALLOC_MAX_PLANES = 1024  # include/mhit_b200.h
 
-POISSON = {"fp64": 0, "fp32": 1, "fp32_refined": 2}
+POISSON = {"fp64": 0, "fp32": 1, "fp32_refined": 2, "fp32_incremental": 3}
 LAPLACIAN = {"exact": 0, "modified": 1}
 INTERP = {"linear1d": 0, "trilinear": 1}
 

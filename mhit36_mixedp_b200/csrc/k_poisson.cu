@@ -36,8 +36,10 @@ template <> __device__ __forceinline__ void store2<float>(float* p, float a, flo
 template <typename T, int M> __host__ __device__ constexpr int xpass_threads() { return fft_threads<M, Tile<T>::B>(); }
 
 // ------------------------------------------------------------------ forward x + divergence
-// SRC 0: the divergence of u*; SRC 1: the real FP32 field `rr` (the residual of the refinement
-// sweep); SRC 2: the real FP64 field `u` (the energy spectrum of a velocity component).
+// SRC 0: the divergence of u*; SRC 2: the real FP64 field `u` (the energy spectrum of a
+// velocity component); SRC 3: the FP64 residual rho/dt div(u*) - L_h q of the FP32 pressure q in
+// `rr` (L_h the 7-point Laplacian, the operator whose symbol the modified divide uses), rounded
+// to FP32 -- the right-hand side of the refinement sweep and of the incremental solve.
 template <typename T, int M, int SRC>
 __global__ void __launch_bounds__(xpass_threads<T, M>())
 k_div_fftx(const double* __restrict__ u, const double* __restrict__ v, const double* __restrict__ w,
@@ -59,11 +61,7 @@ k_div_fftx(const double* __restrict__ u, const double* __restrict__ v, const dou
     const int b = e / M, n = e - b * M;
     const int line = min(line0 + b, nlines - 1);  // a tail tile repeats the last line
     Cx<T> z;
-    if constexpr (SRC == 1) {
-      const float2 r2 = __ldg(reinterpret_cast<const float2*>(rr + (size_t)line * nx + 2 * n));
-      z.x = (T)r2.x;
-      z.y = (T)r2.y;
-    } else if constexpr (SRC == 2) {
+    if constexpr (SRC == 2) {
       const double2 r2 = __ldg(reinterpret_cast<const double2*>(u + (size_t)line * nx + 2 * n));
       z.x = (T)r2.x;
       z.y = (T)r2.y;
@@ -87,6 +85,27 @@ k_div_fftx(const double* __restrict__ u, const double* __restrict__ v, const dou
       double r1 = cdiv * (un - uu.y);
       r1 = r1 + cdiv * (vp.y - vv.y);
       r1 = r1 + cdiv * (wp.y - ww.y);
+      if constexpr (SRC == 3) {
+        // L_h q at cells i and i+1, summed per axis as (q+ - 2 q + q-) ddxi
+        const int jm = wrapm(j, ny), km = wrapm(k, nz);
+        const double ddxi = g.ddxi;
+        const float2 qc = __ldg(reinterpret_cast<const float2*>(rr + row + i));
+        const float qxm = __ldg(rr + row + (i == 0 ? nx - 1 : i - 1));
+        const float qxp = __ldg(rr + row + (i + 2 == nx ? 0 : i + 2));
+        const float2 qyp = __ldg(reinterpret_cast<const float2*>(rr + rowy + i));
+        const float2 qym = __ldg(reinterpret_cast<const float2*>(rr + ((size_t)k * ny + jm) * nx + i));
+        const float2 qzp = __ldg(reinterpret_cast<const float2*>(rr + rowz + i));
+        const float2 qzm = __ldg(reinterpret_cast<const float2*>(rr + ((size_t)km * ny + j) * nx + i));
+        const double q0 = (double)qc.x, q1 = (double)qc.y;
+        const double l0 = ((double)qc.y - 2.0 * q0 + (double)qxm) * ddxi +
+                          ((double)qyp.x - 2.0 * q0 + (double)qym.x) * ddxi +
+                          ((double)qzp.x - 2.0 * q0 + (double)qzm.x) * ddxi;
+        const double l1 = ((double)qxp - 2.0 * q1 + (double)qc.x) * ddxi +
+                          ((double)qyp.y - 2.0 * q1 + (double)qym.y) * ddxi +
+                          ((double)qzp.y - 2.0 * q1 + (double)qzm.y) * ddxi;
+        r0 = r0 - l0;
+        r1 = r1 - l1;
+      }
       z.x = (T)r0;
       z.y = (T)r1;
     }
@@ -136,9 +155,13 @@ k_div_fftx(const double* __restrict__ u, const double* __restrict__ v, const dou
 }
 
 // ------------------------------------------------------------------ inverse x -> pressure
-template <typename T, int M>
+// INC (incremental FP32 solve): the transform is the correction delta; with q the FP32 predictor
+// in `pred`, s = q + delta in FP64 is split into hi = fl32(s), written over q (the next step's
+// predictor), and lo = fl32(s - hi), written to p, so that hi + lo carries s to the projection.
+template <typename T, int M, bool INC>
 __global__ void __launch_bounds__(xpass_threads<T, M>())
-k_fftx_inv(const Cx<T>* __restrict__ spec, T* __restrict__ p, const Cx<T>* __restrict__ twx, Geo g) {
+k_fftx_inv(const Cx<T>* __restrict__ spec, T* __restrict__ p, const Cx<T>* __restrict__ twx, Geo g,
+           float* __restrict__ pred) {
   constexpr int B = Tile<T>::B;
   constexpr int NT = xpass_threads<T, M>();
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -185,7 +208,16 @@ k_fftx_inv(const Cx<T>* __restrict__ spec, T* __restrict__ p, const Cx<T>* __res
     const int line = line0 + b;
     if (line < nlines) {
       const Cx<T> z = s[sw<B>(n, b)];
-      store2<T>(p + (size_t)line * nx + 2 * n, z.x, z.y);
+      if constexpr (INC) {
+        float2* q = reinterpret_cast<float2*>(pred + (size_t)line * nx + 2 * n);
+        const float2 q2 = *q;
+        const double s0 = (double)q2.x + (double)z.x, s1 = (double)q2.y + (double)z.y;
+        const float h0 = (float)s0, h1 = (float)s1;
+        *q = make_float2(h0, h1);
+        store2<T>(p + (size_t)line * nx + 2 * n, (T)(s0 - (double)h0), (T)(s1 - (double)h1));
+      } else {
+        store2<T>(p + (size_t)line * nx + 2 * n, z.x, z.y);
+      }
     }
   }
 }
@@ -352,11 +384,11 @@ template <typename T, int M>
 static cudaError_t launch_xfwd_m(const PoissonArgs& a, cudaStream_t st) {
   constexpr int B = Tile<T>::B;
   const size_t smem = (size_t)(M + 1) * B * sizeof(Cx<T>);
-  auto kern = a.rreal ? k_div_fftx<T, M, 1> : (a.real64 ? k_div_fftx<T, M, 2> : k_div_fftx<T, M, 0>);
+  auto kern = a.presid ? k_div_fftx<T, M, 3> : (a.real64 ? k_div_fftx<T, M, 2> : k_div_fftx<T, M, 0>);
   cudaError_t e = prep_smem(kern, smem);
   if (e != cudaSuccess) return e;
   const int nlines = a.g.ny * a.g.nz;
-  kern<<<(nlines + B - 1) / B, xpass_threads<T, M>(), smem, st>>>(a.u, a.v, a.w, a.rreal, (Cx<T>*)a.spec,
+  kern<<<(nlines + B - 1) / B, xpass_threads<T, M>(), smem, st>>>(a.u, a.v, a.w, a.presid, (Cx<T>*)a.spec,
                                                                   (const Cx<T>*)a.twx, a.g, a.cdiv);
   return cudaGetLastError();
 }
@@ -365,11 +397,12 @@ template <typename T, int M>
 static cudaError_t launch_xinv_m(const PoissonArgs& a, cudaStream_t st) {
   constexpr int B = Tile<T>::B;
   const size_t smem = (size_t)(M + 1) * B * sizeof(Cx<T>);
-  auto kern = k_fftx_inv<T, M>;
+  auto kern = a.pinc ? k_fftx_inv<T, M, true> : k_fftx_inv<T, M, false>;
   cudaError_t e = prep_smem(kern, smem);
   if (e != cudaSuccess) return e;
   const int nlines = a.g.ny * a.g.nz;
-  kern<<<(nlines + B - 1) / B, xpass_threads<T, M>(), smem, st>>>((const Cx<T>*)a.spec, (T*)a.p, (const Cx<T>*)a.twx, a.g);
+  kern<<<(nlines + B - 1) / B, xpass_threads<T, M>(), smem, st>>>((const Cx<T>*)a.spec, (T*)a.p, (const Cx<T>*)a.twx,
+                                                                  a.g, a.pinc);
   return cudaGetLastError();
 }
 

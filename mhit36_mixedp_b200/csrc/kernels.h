@@ -21,20 +21,15 @@ struct PoissonArgs {
   const double *k2x, *k2y, *k2z;
   double cdiv;  // rho*dxi/dt
   double ntot;  // nx*ny*nz
-  const float* rreal = nullptr;  // non-null: x-forward transforms this FP32 field (refinement)
+  // non-null: x-forward transforms the FP64 residual rho/dt div(u*) - L_h presid of this FP32
+  // pressure (refinement sweep, incremental solve)
+  const float* presid = nullptr;
+  // non-null: x-inverse adds its transform to this FP32 predictor in FP64 and splits the sum
+  // into hi (written here) and lo (written to p) (incremental solve)
+  float* pinc = nullptr;
   bool real64 = false;           // x-forward transforms the FP64 field u (energy spectrum)
 };
 
-// FP64 residual of the FP32 solve: r = rho/dt div(u*) - L_h p (7-point Laplacian), stored as
-// FP32 for the second solve
-struct ResidArgs {
-  Geo g;
-  const double *u, *v, *w;  // u*
-  const float* p;           // p32 of the first solve
-  float* r;                 // out
-  double cdiv;
-};
-cudaError_t launch_residual(const ResidArgs& a, cudaStream_t st);
 cudaError_t launch_combine(const float* p32, const float* d32, double* p64, size_t n, cudaStream_t st);
 cudaError_t poisson_stage(const PoissonArgs& a, int stage, cudaStream_t st);
 bool poisson_size_supported(int n, bool is_x);

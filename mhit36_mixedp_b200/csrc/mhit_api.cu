@@ -49,7 +49,7 @@ enum {
 };
 static const char* kStageNames[ST_COUNT] = {"k_tracer", "k_phase", "k_mom", "k_div_fftx", "k_fft_cols_yfwd",
                                             "k_fft_cols_zsolve", "k_fft_cols_yinv", "k_fftx_inv",
-                                            "refine(k_residual+5 passes)", "k_correct+k_finalize"};
+                                            "refine(5 passes)", "k_correct+k_finalize"};
 
 struct mhit_ctx {
   mhit_params prm;
@@ -61,7 +61,7 @@ struct mhit_ctx {
   double *RU = nullptr, *RV = nullptr, *RW = nullptr;
   double *PHI[2] = {}, *RPHI = nullptr;
   void* P = nullptr;
-  float* P2 = nullptr;    // refinement: residual, then the pressure correction (FP32)
+  float* P2 = nullptr;    // refinement: the pressure correction; incremental: the lo part (FP32)
   double* P64 = nullptr;  // refinement: corrected pressure (FP64)
   double* Pw = nullptr;   // FP32 modes: the pressure widened to FP64 for a download (lazy)
   void* lab_small = nullptr;  // droplet labelling scratch (trig tables, chunk counts), grown lazily
@@ -94,6 +94,10 @@ struct mhit_ctx {
 
 // ------------------------------------------------------------------ helpers
 static size_t tsize(const mhit_ctx* c) { return c->prm.poisson == MHIT_POISSON_FP64 ? 8 : 4; }
+// the modes whose pressure is the FP64 sum of two FP32 arrays (P and P2)
+static bool two_part_pressure(const mhit_ctx* c) {
+  return c->prm.poisson == MHIT_POISSON_FP32_REFINED || c->prm.poisson == MHIT_POISSON_FP32_INCREMENTAL;
+}
 
 static int check_ctx(mhit_ctx* c) {
   if (!c) return set_error(MHIT_ERR_ARG, "null context");
@@ -132,12 +136,16 @@ static int upload_vec(void** dst, const std::vector<T>& v) {
   return MHIT_OK;
 }
 
-static int reset_history(mhit_ctx* c) {
+static int reset_history(mhit_ctx* c, bool keep_pressure = false) {
   const size_t bytes = c->n * sizeof(double);
   MHIT_CUDA_TRY(cudaMemsetAsync(c->RU, 0, bytes, c->st));
   MHIT_CUDA_TRY(cudaMemsetAsync(c->RV, 0, bytes, c->st));
   MHIT_CUDA_TRY(cudaMemsetAsync(c->RW, 0, bytes, c->st));
   if (c->RPHI) MHIT_CUDA_TRY(cudaMemsetAsync(c->RPHI, 0, bytes, c->st));
+  if (c->prm.poisson == MHIT_POISSON_FP32_INCREMENTAL && !keep_pressure) {  // the predictor restarts at 0
+    MHIT_CUDA_TRY(cudaMemsetAsync(c->P, 0, c->n * sizeof(float), c->st));
+    MHIT_CUDA_TRY(cudaMemsetAsync(c->P2, 0, c->n * sizeof(float), c->st));
+  }
   DevScalars s;
   memset(&s, 0, sizeof(s));
   s.gumax = 1.0;  // multi/main.f90:442
@@ -262,22 +270,21 @@ static int enqueue_stage(mhit_ctx* c, int stage, double alpha, double beta, int 
       a.k2z = c->k2z;
       a.cdiv = p.rho * c->g.dxi / p.dt;  // (rho*dxi/dt), multi/main.f90:841
       a.ntot = (double)c->g.nx * (double)c->g.ny * (double)c->g.nz;
+      if (p.poisson == MHIT_POISSON_FP32_INCREMENTAL) {
+        // the residual of the predictor P in the x pass; P <- hi, P2 <- lo in the x-inverse
+        if (stage == ST_XFWD) a.presid = static_cast<const float*>(c->P);
+        if (stage == ST_XINV) {
+          a.pinc = static_cast<float*>(c->P);
+          a.p = c->P2;
+        }
+      }
       if (stage != ST_REFINE) {
         MHIT_CUDA_TRY(poisson_stage(a, stage - ST_XFWD, c->st));
         return MHIT_OK;
       }
-      // one FP64 residual sweep: r -> P2, L_h delta = r in FP32 (delta -> P2); the projection
-      // reads p = P + P2
-      ResidArgs r;
-      r.g = c->g;
-      r.u = c->U[nxt];
-      r.v = c->V[nxt];
-      r.w = c->W[nxt];
-      r.p = static_cast<const float*>(c->P);
-      r.r = c->P2;
-      r.cdiv = a.cdiv;
-      MHIT_CUDA_TRY(launch_residual(r, c->st));
-      a.rreal = c->P2;
+      // one FP64 residual sweep: the x pass forms r = rhs - L_h P in FP64, L_h delta = r in FP32
+      // (delta -> P2); the projection reads p = P + P2
+      a.presid = static_cast<const float*>(c->P);
       a.p = c->P2;
       for (int s = 0; s < PSTAGE_COUNT; ++s) MHIT_CUDA_TRY(poisson_stage(a, s, c->st));
       return MHIT_OK;
@@ -290,7 +297,7 @@ static int enqueue_stage(mhit_ctx* c, int stage, double alpha, double beta, int 
       a.w = c->W[nxt];
       a.p = c->P;
       a.fp32 = p.poisson != MHIT_POISSON_FP64;
-      a.pd = p.poisson == MHIT_POISSON_FP32_REFINED ? c->P2 : nullptr;
+      a.pd = two_part_pressure(c) ? c->P2 : nullptr;
       a.partials = c->partials;
       a.nblocks = c->nblk;
       a.sc = c->sc;
@@ -553,8 +560,9 @@ static int init_impl(const mhit_params* p, mhit_ctx* c) {
   if (p->phiflag) MHIT_CUDA_TRY(cudaMalloc(&c->RPHI, fb));
   const size_t ts = tsize(c);
   MHIT_CUDA_TRY(cudaMalloc(&c->P, n * ts));
-  if (p->poisson == MHIT_POISSON_FP32_REFINED) {
+  if (two_part_pressure(c)) {
     MHIT_CUDA_TRY(cudaMalloc(&c->P2, n * sizeof(float)));
+    MHIT_CUDA_TRY(cudaMemset(c->P2, 0, n * sizeof(float)));
     MHIT_CUDA_TRY(cudaMalloc(&c->P64, n * sizeof(double)));
     MHIT_CUDA_TRY(cudaMemset(c->P64, 0, n * sizeof(double)));
   }
@@ -571,12 +579,17 @@ static int init_impl(const mhit_params* p, mhit_ctx* c) {
     if ((rc = upload_vec(&c->twy, twiddles<double>(g.ny)))) return rc;
     if ((rc = upload_vec(&c->twz, twiddles<double>(g.nz)))) return rc;
   }
-  // k^2 per axis (multi/main.f90:234-240, 889), or the modified wavenumber
+  // k^2 per axis (multi/main.f90:234-240, 889), or the modified wavenumber.  The cells are cubes
+  // of side dx = lx/nx, so an axis of nn cells is nn dx long: its wavenumber of index kk is
+  // kk nx/nn (in units of 2 pi/lx = 1) and its modified symbol (2 - 2 cos(kk 2 pi/nn))/dx^2.  On
+  // the reference's cubic box these are the integer kk and (2 - 2 cos(kk dx))/dx^2.
   auto k2tab = [&](int nn, int len) {
     std::vector<double> t(len);
+    const double h = lx / nn, scale = (double)p->nx / (double)nn;
     for (int i = 0; i < len; ++i) {
       const double kk = (i < nn / 2) ? (double)i : (double)(i - nn);
-      t[i] = p->laplacian == MHIT_LAP_MODIFIED ? (2.0 - 2.0 * cos(kk * g.dx)) * g.ddxi : kk * kk;
+      const double kp = kk * scale;
+      t[i] = p->laplacian == MHIT_LAP_MODIFIED ? (2.0 - 2.0 * cos(kk * h)) * g.ddxi : kp * kp;
     }
     return t;
   };
@@ -620,11 +633,13 @@ int mhit_init(const mhit_params* p, mhit_ctx** out) {
   }
   if (p->nx != 2 * (p->nx / 2) || !(p->dt > 0) || !(p->rho > 0) || !(p->epsr > 0))
     return set_error(MHIT_ERR_ARG, "dt, rho and epsr must be positive");
-  if (p->poisson != MHIT_POISSON_FP64 && p->poisson != MHIT_POISSON_FP32 && p->poisson != MHIT_POISSON_FP32_REFINED)
-    return set_error(MHIT_ERR_ARG, "poisson must be MHIT_POISSON_FP64, _FP32 or _FP32_REFINED");
-  if (p->poisson == MHIT_POISSON_FP32_REFINED && p->laplacian != MHIT_LAP_MODIFIED)
-    return set_error(MHIT_ERR_ARG, "MHIT_POISSON_FP32_REFINED needs laplacian = MHIT_LAP_MODIFIED (its residual is the "
-                                   "7-point operator)");
+  if (p->poisson != MHIT_POISSON_FP64 && p->poisson != MHIT_POISSON_FP32 && p->poisson != MHIT_POISSON_FP32_REFINED &&
+      p->poisson != MHIT_POISSON_FP32_INCREMENTAL)
+    return set_error(MHIT_ERR_ARG, "poisson must be MHIT_POISSON_FP64, _FP32, _FP32_REFINED or _FP32_INCREMENTAL");
+  if ((p->poisson == MHIT_POISSON_FP32_REFINED || p->poisson == MHIT_POISSON_FP32_INCREMENTAL) &&
+      p->laplacian != MHIT_LAP_MODIFIED)
+    return set_error(MHIT_ERR_ARG, "MHIT_POISSON_FP32_REFINED and _FP32_INCREMENTAL need laplacian = MHIT_LAP_MODIFIED "
+                                   "(their residual is the 7-point operator)");
   if (p->laplacian != MHIT_LAP_EXACT && p->laplacian != MHIT_LAP_MODIFIED)
     return set_error(MHIT_ERR_ARG, "laplacian must be MHIT_LAP_EXACT or MHIT_LAP_MODIFIED");
   if (p->interp != MHIT_INTERP_LINEAR1D && p->interp != MHIT_INTERP_TRILINEAR)
@@ -802,7 +817,7 @@ int mhit_download_fields(mhit_ctx* c, double* u, double* v, double* w, double* p
   if (phi) MHIT_CUDA_TRY(cudaMemcpyAsync(phi, c->PHI[c->cur], fb, cudaMemcpyDeviceToHost, c->st));
   if (p) {
     const double* src = static_cast<const double*>(c->P);
-    if (c->P64) {  // refinement: materialise p = P + P2 in FP64
+    if (c->P64) {  // refinement / incremental: materialise p = P + P2 in FP64
       MHIT_CUDA_TRY(launch_combine(static_cast<const float*>(c->P), c->P2, c->P64, c->n, c->st));
       src = c->P64;
     } else if (tsize(c) == 4) {
@@ -891,9 +906,15 @@ int mhit_read_field(mhit_ctx* c, const char* path, int fieldn) {
     MHIT_CUDA_TRY(cudaMemcpyAsync(c->PHI[c->cur], buf.data(), fb, cudaMemcpyHostToDevice, c->st));
   } else {
     if (tsize(c) == 4) {
-      std::vector<float> pf(c->n);
-      for (size_t i = 0; i < c->n; ++i) pf[i] = (float)buf[i];
+      // FP32 pressure; in the two-part modes also the remainder, so P + P2 is the file's value
+      // to FP64 precision (the incremental solve's predictor for the next step)
+      std::vector<float> pf(c->n), lo(c->P2 ? c->n : 0);
+      for (size_t i = 0; i < c->n; ++i) {
+        pf[i] = (float)buf[i];
+        if (c->P2) lo[i] = (float)(buf[i] - (double)pf[i]);
+      }
       MHIT_CUDA_TRY(cudaMemcpyAsync(c->P, pf.data(), c->n * 4, cudaMemcpyHostToDevice, c->st));
+      if (c->P2) MHIT_CUDA_TRY(cudaMemcpyAsync(c->P2, lo.data(), c->n * 4, cudaMemcpyHostToDevice, c->st));
       MHIT_CUDA_TRY(cudaStreamSynchronize(c->st));
     } else {
       MHIT_CUDA_TRY(cudaMemcpyAsync(c->P, buf.data(), fb, cudaMemcpyHostToDevice, c->st));
@@ -901,8 +922,9 @@ int mhit_read_field(mhit_ctx* c, const char* path, int fieldn) {
   }
   MHIT_CUDA_TRY(cudaStreamSynchronize(c->st));
   // a field read happens at setup: the next step is an Euler step with empty history
-  // (multi/main.f90:440-441; rhs_o is not part of the files)
-  return reset_history(c);
+  // (multi/main.f90:440-441; rhs_o is not part of the files); a pressure read is kept as the
+  // incremental solve's predictor
+  return reset_history(c, fieldn == 4);
 }
 
 // ------------------------------------------------------------------ checkpoint
@@ -930,7 +952,7 @@ std::vector<CkptArray> ckpt_arrays(mhit_ctx* c) {
     a.push_back({c->RPHI, fb});
   }
   a.push_back({c->P, c->n * tsize(c)});
-  if (c->P2) a.push_back({c->P2, c->n * sizeof(float)});  // refinement: the correction
+  if (c->P2) a.push_back({c->P2, c->n * sizeof(float)});  // refinement / incremental: the second part
   return a;
 }
 

@@ -13,7 +13,8 @@ module mhit_gpu
 
   integer(c_int), parameter :: MHIT_OK = 0, MHIT_ERR_ARG = -1, MHIT_ERR_CUDA = -2, MHIT_ERR_NAN = -3
   integer(c_int), parameter :: MHIT_ERR_CFL = -4, MHIT_ERR_IO = -5, MHIT_ERR_STATE = -6
-  integer(c_int), parameter :: MHIT_POISSON_FP64 = 0, MHIT_POISSON_FP32 = 1, MHIT_POISSON_FP32_REFINED = 2
+  integer(c_int), parameter :: MHIT_POISSON_FP64 = 0, MHIT_POISSON_FP32 = 1, MHIT_POISSON_FP32_REFINED = 2, &
+                                MHIT_POISSON_FP32_INCREMENTAL = 3
   integer(c_int), parameter :: MHIT_LAP_EXACT = 0, MHIT_LAP_MODIFIED = 1
   integer(c_int), parameter :: MHIT_INTERP_LINEAR1D = 0, MHIT_INTERP_TRILINEAR = 1
 

@@ -38,7 +38,7 @@ struct Options {
 void usage() {
   std::printf(
       "usage: mhit_main [--input input.inp] [--n N] [--ny N] [--nz N] [--steps S] [--phiflag 0|1]\n"
-      "                 [--poisson fp64|fp32|fp32_refined] [--laplacian exact|modified] [--dt DT]\n"
+      "                 [--poisson fp64|fp32|fp32_refined|fp32_incremental] [--laplacian exact|modified] [--dt DT]\n"
       "                 [--indir DIR] [--outdir DIR] [--device D] [--quiet] [--dry-run]\n"
       "Runs tfin - tstart steps of the MHIT36 loop (multi/main.f90) on one GPU; --dry-run prints the\n"
       "parameters read from input.inp and exits without touching the GPU.\n");
@@ -82,6 +82,7 @@ bool parse(int argc, char** argv, Options& o) {
       if (v == "fp64") o.poisson = MHIT_POISSON_FP64;
       else if (v == "fp32") o.poisson = MHIT_POISSON_FP32;
       else if (v == "fp32_refined") o.poisson = MHIT_POISSON_FP32_REFINED;
+      else if (v == "fp32_incremental") o.poisson = MHIT_POISSON_FP32_INCREMENTAL;
       else return false;
     } else if (a == "--laplacian") {
       const std::string v = val("--laplacian");

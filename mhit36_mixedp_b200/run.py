@@ -49,7 +49,7 @@ def main(argv=None):
     ap.add_argument("--nz", type=int, help="grid points in z (default n)")
     ap.add_argument("--steps", type=int, help="steps to run (default tfin - tstart)")
     ap.add_argument("--phiflag", type=int, default=0)
-    ap.add_argument("--poisson", default="fp64", choices=["fp64", "fp32", "fp32_refined"])
+    ap.add_argument("--poisson", default="fp64", choices=["fp64", "fp32", "fp32_refined", "fp32_incremental"])
     ap.add_argument("--laplacian", default="exact", choices=["exact", "modified"])
     ap.add_argument("--synthetic", action="store_true", help="seeded solenoidal velocity (+ 64 drops)")
     ap.add_argument("--indir", default="input", help="directory of u.dat, v.dat, w.dat, phi.dat")

@@ -57,6 +57,7 @@ class Params:
     phiflag: int = 0
     partflag: int = 0
     poisson: str = "fp64"          # "fp64" | "fp32" (multi/main.f90:844,853-912) | "fp32_refined"
+    #                                | "fp32_incremental"
     laplacian: str = "exact"       # "exact" k^2 (multi/main.f90:889) | "modified" (2-2cos)/dx^2
     yz_shift: int = 1              # 1: reference labelling of y/z planes, 0: grid aligned
     interp: str = "linear1d"       # "linear1d" (multi/particles.f90:114-117) | "trilinear"
@@ -172,6 +173,7 @@ class State:
     phi: np.ndarray | None = None
     rhsphi_o: np.ndarray | None = None
     part: np.ndarray | None = None   # (np, 12) table, multi/particles.f90:15-22 (0-based cols)
+    p32: np.ndarray | None = None    # fp32_incremental: the FP32 pressure predictor (0 at start)
     alpha: float = 1.0               # Euler on the first step, multi/main.f90:440-441
     beta: float = 0.0
     gumax: float = 1.0               # multi/main.f90:442
@@ -186,6 +188,8 @@ def new_state(p: Params, u, v, w, phi=None, part=None) -> State:
         st.rhsphi_o = z()
     if p.partflag:
         st.part = part.copy()
+    if p.poisson == "fp32_incremental":
+        st.p32 = np.zeros(u.shape, dtype=np.float32)
     return st
 
 
@@ -394,17 +398,22 @@ def poisson_rhs(p: Params, u, v, w):
 
 
 def k2_table(p: Params):
-    """k^2 on the half spectrum (nz, ny, nx//2+1) in FP64, multi/main.f90:884-890."""
+    """k^2 on the half spectrum (nz, ny, nx//2+1) in FP64, multi/main.f90:884-890.
+
+    The cells are cubes of side dx = lx/nx, so an axis of n cells is n dx long: its wavenumber of
+    index k is k nx/n (2 pi/lx = 1) and its modified symbol (2 - 2 cos(2 pi k/n))/dx^2.  On the
+    reference's cubic box these reduce to the integer k and (2 - 2 cos(k dx))/dx^2."""
     kx = wavenumbers(p.nx)[: p.nx // 2 + 1].copy()
     kx[p.nx // 2] = -(p.nx // 2)   # kx(nx/2+1) = (nx/2 - nx)
     ky = wavenumbers(p.ny)
     kz = wavenumbers(p.nz)
     if p.laplacian == "modified":
-        # (2 - 2 cos(k dx)) / dx^2 per axis: the symbol of the 7-point staggered Laplacian
-        mx = (2.0 - 2.0 * np.cos(kx * p.dx)) * p.ddxi
-        my = (2.0 - 2.0 * np.cos(ky * p.dx)) * p.ddxi
-        mz = (2.0 - 2.0 * np.cos(kz * p.dx)) * p.ddxi
+        # (2 - 2 cos(k h)) / dx^2 per axis, h = lx/n: the symbol of the 7-point staggered Laplacian
+        mx = (2.0 - 2.0 * np.cos(kx * (p.lx / p.nx))) * p.ddxi
+        my = (2.0 - 2.0 * np.cos(ky * (p.lx / p.ny))) * p.ddxi
+        mz = (2.0 - 2.0 * np.cos(kz * (p.lx / p.nz))) * p.ddxi
         return mx[None, None, :] + my[None, :, None] + mz[:, None, None]
+    kx, ky, kz = kx * (p.nx / p.nx), ky * (p.nx / p.ny), kz * (p.nx / p.nz)
     return kx[None, None, :] ** 2 + ky[None, :, None] ** 2 + kz[:, None, None] ** 2
 
 
@@ -424,21 +433,47 @@ def poisson_solve(p: Params, rhsp):
             pr = np.fft.irfftn(hat, s=rhsp.shape, axes=(0, 1, 2), norm="forward")
             return pr
         if p.poisson in ("fp32", "fp32_refined"):
-            def solve32(rhs):
-                hat = fft3_r2c_f32(rhs.astype(np.float32))
-                hat = (-(hat.astype(np.complex128)) / k2 / float(n)).astype(np.complex64)
-                hat[0, 0, 0] = 0.0
-                return fft3_c2r_f32(hat, rhsp.shape)
-            p32 = solve32(rhsp)
+            p32 = solve32(p, rhsp)
             if p.poisson == "fp32":
                 return p32
             # one FP64 residual sweep: r = rhs - L_h p32 in FP64, L_h delta = r in FP32
             q = p32.astype(np.float64)
-            lap = ((xp(q) - 2.0 * q + xm(q)) * p.ddxi + (yp(q) - 2.0 * q + ym(q)) * p.ddxi
-                   + (zp(q) - 2.0 * q + zm(q)) * p.ddxi)
-            delta = solve32(rhsp - lap)
+            delta = solve32(p, rhsp - laplacian7(p, q))
             return q + delta.astype(np.float64)
     raise ValueError(p.poisson)
+
+
+def solve32(p: Params, rhs):
+    """The FP32 branch's solve (multi/main.f90:844-912): rhs rounded to FP32, FP32 transforms,
+    the divide in FP64 rounded back (complex(4)/real(8) promotes, :890), FP32 pressure."""
+    n = p.nx * p.ny * p.nz
+    with np.errstate(divide="ignore", invalid="ignore"):
+        hat = fft3_r2c_f32(rhs.astype(np.float32))
+        hat = (-(hat.astype(np.complex128)) / k2_table(p) / float(n)).astype(np.complex64)
+    hat[0, 0, 0] = 0.0
+    return fft3_c2r_f32(hat, rhs.shape)
+
+
+def laplacian7(p: Params, q):
+    """The 7-point Laplacian L_h q (the operator whose symbol the modified divide uses), summed
+    per axis as (q+ - 2 q + q-) ddxi."""
+    return ((xp(q) - 2.0 * q + xm(q)) * p.ddxi + (yp(q) - 2.0 * q + ym(q)) * p.ddxi
+            + (zp(q) - 2.0 * q + zm(q)) * p.ddxi)
+
+
+def poisson_solve_incremental(p: Params, rhsp, pred32):
+    """One FP32 solve for the increment over the previous step's pressure (needs the modified
+    Laplacian).  r = rhs - L_h q in FP64 with q the FP32 predictor, L_h delta = r in FP32, and
+    s = q + delta in FP64, kept as hi = fl32(s) and lo = fl32(s - hi).  Returns (hi + lo in FP64,
+    the pressure the projection uses; hi, the next step's predictor)."""
+    if p.laplacian != "modified":
+        raise ValueError("fp32_incremental needs the modified Laplacian")
+    q = pred32.astype(np.float64)
+    delta = solve32(p, rhsp - laplacian7(p, q))
+    s = q + delta.astype(np.float64)
+    hi = s.astype(np.float32)
+    lo = (s - hi.astype(np.float64)).astype(np.float32)
+    return hi.astype(np.float64) + lo.astype(np.float64), hi
 
 
 def fft3_r2c_f32(a32):
@@ -487,7 +522,10 @@ def step(p: Params, st: State, tables=None):
         phase_step(p, st)
     momentum_step(p, st, tables)
     rhsp = poisson_rhs(p, st.u, st.v, st.w)
-    pr = poisson_solve(p, rhsp)
+    if p.poisson == "fp32_incremental":
+        pr, st.p32 = poisson_solve_incremental(p, rhsp, st.p32)
+    else:
+        pr = poisson_solve(p, rhsp)
     means = correct(p, st, pr)
     st.nstep += 1
     return means

@@ -8,6 +8,7 @@ import os
 import numpy as np
 import pytest
 
+from mhit36_mixedp_b200 import synth
 from oracle import mhit_oracle as orc
 from tests.golden.make_golden import CASES, NSTEPS, case_inputs
 
@@ -152,3 +153,49 @@ def test_mean_removed_and_gumax_signed():
     orc.step(op, st)
     assert abs(st.u.mean()) < 1e-15 and abs(st.v.mean()) < 1e-15
     assert st.gumax == max(st.u.max(), st.v.max(), st.w.max())
+
+
+def test_oracle_incremental_fp32_solve():
+    """The oracle's incremental FP32 solve (one FP32 solve per step for the increment over the
+    previous pressure, the residual in FP64) stays within FP32 round-off of its FP64 step and,
+    from the third step on, leaves a divergence far below the plain FP32 solve's."""
+    n = 32
+    u, v, w = synth.solenoidal_velocity(n, 0)
+    phi = synth.drops_phi(n, synth.drop_centres(8, 1), 0.3, 2 * np.pi / n)
+    runs = {}
+    for mode in ("fp64", "fp32", "fp32_incremental"):
+        op = orc.Params(nx=n, dt=5e-4, mu=0.006, radius=0.3, sigma=0.5, phiflag=1, poisson=mode,
+                        laplacian="modified")
+        st = orc.new_state(op, u, v, w, phi=phi)
+        divs = []
+        for _ in range(6):
+            orc.step(op, st)
+            divs.append(float(np.abs(orc.divergence(op, st.u, st.v, st.w)).max()))
+        runs[mode] = (st, divs)
+    ref = runs["fp64"][0]
+    st, divs = runs["fp32_incremental"]
+    for f in ("u", "v", "w", "phi"):
+        a, b = getattr(st, f), getattr(ref, f)
+        assert np.abs(a - b).max() / np.abs(b).max() < 1e-8, f
+    assert max(divs[3:]) < 1e-2 * min(runs["fp32"][1][3:]), (divs, runs["fp32"][1])
+    assert st.p32.dtype == np.float32 and np.abs(st.p32 - st.p).max() <= 1e-6 * np.abs(st.p).max()
+
+
+@pytest.mark.parametrize("laplacian", ["exact", "modified"])
+def test_oracle_k2_table_non_cubic(laplacian):
+    """On a box of nx x ny x nz cubic cells the wavenumbers are physical (index x nx/n per axis):
+    only the zero mode has k^2 = 0, and with the modified Laplacian one FP64 step leaves the
+    discrete divergence at round-off."""
+    nx, ny, nz = 32, 16, 64
+    op = orc.Params(nx=nx, ny=ny, nz=nz, dt=5e-4, mu=0.006, laplacian=laplacian)
+    k2 = orc.k2_table(op)
+    assert k2.shape == (nz, ny, nx // 2 + 1)
+    assert k2[0, 0, 0] == 0.0 and np.count_nonzero(k2 == 0.0) == 1
+    if laplacian == "exact":
+        assert k2[0, 1, 0] == (nx / ny) ** 2 and k2[1, 0, 0] == (nx / nz) ** 2
+    u, v, w = synth.solenoidal_velocity(nx, 3, ny=ny, nz=nz)
+    st = orc.new_state(op, u, v, w)
+    orc.step(op, st)
+    div = np.abs(orc.divergence(op, st.u, st.v, st.w)).max()
+    if laplacian == "modified":
+        assert div < 1e-11 * np.abs(st.u).max() * nx / (2 * np.pi), div
