@@ -106,7 +106,6 @@ __global__ void __launch_bounds__(MNT, 3) k_mom(MomArgs a) {
   auto issue_phi = [&](int m) { copy_phi(m, (size_t)pmod_int(m, nz) * plane); };
 
   const double eps = g.eps, epsi = g.epsi, ddxi = g.ddxi, dxi = g.dxi;
-  const double s6 = 6.0 * g.sigma;
   // chemical potential (multi/main.f90:735) of plane m over the CPX x CPY region
   auto chempot_plane = [&](int m) {
     if constexpr (PHI) {
@@ -148,9 +147,12 @@ __global__ void __launch_bounds__(MNT, 3) k_mom(MomArgs a) {
   const double* t = a.tabs;
   const double sxi = own ? __ldg(t + i) : 0.0, cxi = own ? __ldg(t + nx + i) : 0.0;
   const double syj = own ? __ldg(t + 2 * nx + j) : 0.0, cyj = own ? __ldg(t + 2 * nx + ny + j) : 0.0;
-  const double mu = g.mu, rhoi = g.rhoi, dt = g.dt, al = a.alpha, be = a.beta;
-  // (h*0.25)*dxi == h*(0.25*dxi) exactly: scaling by 0.25 does not round
-  const double q4 = 0.25 * dxi;
+  // constant factors of the right-hand side, applied once per sum of terms (the reference's
+  // expression up to rounding: a few ulp of the terms, far inside the 1e-12 parity bound)
+  const double c_adv = -0.25 * dxi;                    // -(h11 + h12 + h13) / 4 dxi
+  const double c_vis = g.mu * ddxi * g.rhoi;           // mu lap(u) / rho
+  const double c_st = 6.0 * g.sigma * 0.25 * dxi * g.rhoi;  // face average of the force / rho
+  const double dta = g.dt * a.alpha, dtb = g.dt * a.beta;
   const int uq = (ty + 1) * UPX + (tx + 2);   // own cell in the u/v/w plane
   const int pq = (ty + 2) * PPX + (tx + 2);   // own cell in the phi plane
   const int cq = (ty + 1) * CPX + (tx + 1);   // own cell in the chempot plane
@@ -191,52 +193,52 @@ __global__ void __launch_bounds__(MNT, 3) k_mom(MomArgs a) {
       const double wzp = S.w[sp][uq] - mw_, wzm = S.w[sm][uq] - mw_;
       const double v_imjp = V0[uq + UPX - 1] - mv_, w_imkp = S.w[sp][uq - 1] - mw_, u_ipjm = U0[uq - UPX + 1] - mu_;
       const double w_jmkp = S.w[sp][uq - UPX] - mw_, u_ipkm = S.u[sm][uq + 1] - mu_, v_jpkm = S.v[sm][uq + UPX] - mv_;
-      // multi/main.f90:672-694
-      double h11 = (uxp + u0) * (uxp + u0) - (u0 + uxm) * (u0 + uxm);
-      double h12 = (uyp + u0) * (vyp + v_imjp) - (u0 + uym) * (v0 + vxm);
-      double h13 = (uzp + u0) * (wzp + w_imkp) - (u0 + uzm) * (w0 + wxm);
-      double ru = -(h11 * q4 + h12 * q4 + h13 * q4);
-      double h21 = (uxp + u_ipjm) * (vxp + v0) - (u0 + uym) * (v0 + vxm);
-      double h22 = (vyp + v0) * (vyp + v0) - (v0 + vym) * (v0 + vym);
-      double h23 = (wzp + w_jmkp) * (vzp + v0) - (w0 + wym) * (v0 + vzm);
-      double rv = -(h21 * q4 + h22 * q4 + h23 * q4);
-      double h31 = (wxp + w0) * (uxp + u_ipkm) - (w0 + wxm) * (u0 + uzm);
-      double h32 = (vyp + v_jpkm) * (wyp + w0) - (v0 + vzm) * (w0 + wym);
-      double h33 = (wzp + w0) * (wzp + w0) - (w0 + wzm) * (w0 + wzm);
-      double rw = -(h31 * q4 + h32 * q4 + h33 * q4);
-      // :696-707
-      ru = ru + (mu * (uxp - 2.0 * u0 + uxm) * ddxi + mu * (uyp - 2.0 * u0 + uym) * ddxi +
-                 mu * (uzp - 2.0 * u0 + uzm) * ddxi) * rhoi;
-      rv = rv + (mu * (vxp - 2.0 * v0 + vxm) * ddxi + mu * (vyp - 2.0 * v0 + vym) * ddxi +
-                 mu * (vzp - 2.0 * v0 + vzm) * ddxi) * rhoi;
-      rw = rw + (mu * (wxp - 2.0 * w0 + wxm) * ddxi + mu * (wyp - 2.0 * w0 + wym) * ddxi +
-                 mu * (wzp - 2.0 * w0 + wzm) * ddxi) * rhoi;
+      // multi/main.f90:672-694: the fluxes h = a^2 - b^2 and h = a c - b d as one product and
+      // one fused multiply-add each
+      auto dsq = [](double a1, double b1) { return __fma_rn(a1, a1, -(b1 * b1)); };
+      auto dpr = [](double a1, double c1, double b1, double d1) { return __fma_rn(a1, c1, -(b1 * d1)); };
+      const double h11 = dsq(uxp + u0, u0 + uxm);
+      const double h12 = dpr(uyp + u0, vyp + v_imjp, u0 + uym, v0 + vxm);
+      const double h13 = dpr(uzp + u0, wzp + w_imkp, u0 + uzm, w0 + wxm);
+      const double h21 = dpr(uxp + u_ipjm, vxp + v0, u0 + uym, v0 + vxm);
+      const double h22 = dsq(vyp + v0, v0 + vym);
+      const double h23 = dpr(wzp + w_jmkp, vzp + v0, w0 + wym, v0 + vzm);
+      const double h31 = dpr(wxp + w0, uxp + u_ipkm, w0 + wxm, u0 + uzm);
+      const double h32 = dpr(vyp + v_jpkm, wyp + w0, v0 + vzm, w0 + wym);
+      const double h33 = dsq(wzp + w0, w0 + wzm);
+      // :696-707: mu (sum of the six neighbours - 6 u) ddxi / rho
+      const double lu = ((uxp + uxm) + (uyp + uym)) + __fma_rn(-6.0, u0, uzp + uzm);
+      const double lv = ((vxp + vxm) + (vyp + vym)) + __fma_rn(-6.0, v0, vzp + vzm);
+      const double lw = ((wxp + wxm) + (wyp + wym)) + __fma_rn(-6.0, w0, wzp + wzm);
+      double ru = __fma_rn(c_adv, (h11 + h12) + h13, c_vis * lu);
+      double rv = __fma_rn(c_adv, (h21 + h22) + h23, c_vis * lv);
+      double rw = __fma_rn(c_adv, (h31 + h32) + h33, c_vis * lw);
       // :712-714
       const double szk = __ldg(t + 2 * nx + 2 * ny + k), czk = __ldg(t + 2 * nx + 2 * ny + nz + k);
-      ru = ru + g.f3 * szk + g.f2 * cyj;
-      rv = rv + g.f1 * sxi + g.f3 * czk;
-      rw = rw + g.f2 * syj + g.f1 * cxi;
+      ru = __fma_rn(g.f3, szk, __fma_rn(g.f2, cyj, ru));
+      rv = __fma_rn(g.f1, sxi, __fma_rn(g.f3, czk, rv));
+      rw = __fma_rn(g.f2, syj, __fma_rn(g.f1, cxi, rw));
       if constexpr (PHI) {
-        // :737-739 at the cell and at its -x/-y/-z neighbours, :768-770 face average
+        // :737-739 at the cell and at its -x/-y/-z neighbours, :768-770 face average:
+        // 6 sigma mu_c grad(phi) / rho averaged to the face, the central differences taken as
+        // (phi+ - phi-) dxi / 2
         auto& SP = reinterpret_cast<MomSmem<true>&>(S);
         const int pmm = (k - k0 + 14) & 7, pm = (k - k0 + 15) & 7, p0 = (k - k0 + 16) & 7, pp = (k - k0 + 17) & 7;
         const int c0s = (k - k0 + 16) & 3, cms = (k - k0 + 15) & 3;
         const double* P0 = SP.phi[p0];
         const double pc = P0[pq];
         const double c0 = SP.cp[c0s][cq];
-        const double fx0 = s6 * c0 * 0.5 * (P0[pq + 1] - P0[pq - 1]) * dxi;
-        const double fy0 = s6 * c0 * 0.5 * (P0[pq + PPX] - P0[pq - PPX]) * dxi;
-        const double fz0 = s6 * c0 * 0.5 * (SP.phi[pp][pq] - SP.phi[pm][pq]) * dxi;
-        const double fxm = s6 * SP.cp[c0s][cq - 1] * 0.5 * (pc - P0[pq - 2]) * dxi;
-        const double fym = s6 * SP.cp[c0s][cq - CPX] * 0.5 * (pc - P0[pq - 2 * PPX]) * dxi;
-        const double fzm = s6 * SP.cp[cms][cq] * 0.5 * (pc - SP.phi[pmm][pq]) * dxi;
-        ru = ru + 0.5 * (fxm + fx0) * rhoi;
-        rv = rv + 0.5 * (fym + fy0) * rhoi;
-        rw = rw + 0.5 * (fzm + fz0) * rhoi;
+        const double fx = __fma_rn(c0, P0[pq + 1] - P0[pq - 1], SP.cp[c0s][cq - 1] * (pc - P0[pq - 2]));
+        const double fy = __fma_rn(c0, P0[pq + PPX] - P0[pq - PPX], SP.cp[c0s][cq - CPX] * (pc - P0[pq - 2 * PPX]));
+        const double fz = __fma_rn(c0, SP.phi[pp][pq] - SP.phi[pm][pq], SP.cp[cms][cq] * (pc - SP.phi[pmm][pq]));
+        ru = __fma_rn(c_st, fx, ru);
+        rv = __fma_rn(c_st, fy, rv);
+        rw = __fma_rn(c_st, fz, rw);
       }
-      a.un[c] = u0 + dt * (al * ru - be * ruo);
-      a.vn[c] = v0 + dt * (al * rv - be * rvo);
-      a.wn[c] = w0 + dt * (al * rw - be * rwo);
+      // :771-776 / :787-792
+      a.un[c] = __fma_rn(dta, ru, __fma_rn(-dtb, ruo, u0));
+      a.vn[c] = __fma_rn(dta, rv, __fma_rn(-dtb, rvo, v0));
+      a.wn[c] = __fma_rn(dta, rw, __fma_rn(-dtb, rwo, w0));
       a.ru[c] = ru;
       a.rv[c] = rv;
       a.rw[c] = rw;

@@ -126,9 +126,10 @@ __global__ void __launch_bounds__(PNT, 1) k_phase(PhaseArgs a) {
 
   const double gamma = 1.0 * a.sc->gumax;
   const double mu_ = a.sc->mean[0], mv_ = a.sc->mean[1], mw_ = a.sc->mean[2];
-  const double dxi = g.dxi, ddxi = g.ddxi, dt = g.dt;
+  const double dxi = g.dxi, ddxi = g.ddxi;
   const double hdxi = 0.5 * dxi;  // (x*0.5)*dxi == x*(0.5*dxi) exactly
-  const double alpha = a.alpha, beta = a.beta;
+  // the right-hand side's constant factors, applied once per sum of terms (see the output block)
+  const double c_lap = gamma * (eps * ddxi), c_shp = gamma * -hdxi;
   int c = k0 * plane + col;  // own cell (output role)
   const int dux = (i + 1 == nx) ? 1 - nx : 1;
   const int dvy = (j + 1 == ny) ? (1 - ny) * nx : nx;
@@ -181,18 +182,21 @@ __global__ void __launch_bounds__(PNT, 1) k_phase(PhaseArgs a) {
       const double p0 = f_0;
       const double pxp = P0[1], pxm = P0[-1], pyp = P0[PHX], pym = P0[-PHX];
       const double pzp = f_p1, pzm = f_m1;
-      // multi/main.f90:551-557
-      double rhs = -((u_x * 0.5 * (pxp + p0) - u_0 * 0.5 * (p0 + pxm)) * dxi) -
-                   (v_y * 0.5 * (pyp + p0) - v_0 * 0.5 * (p0 + pym)) * dxi -
-                   (w_z * 0.5 * (pzp + p0) - w_0 * 0.5 * (p0 + pzm)) * dxi +
-                   gamma * (eps * (pxp - 2.0 * p0 + pxm) * ddxi + eps * (pyp - 2.0 * p0 + pym) * ddxi +
-                            eps * (pzp - 2.0 * p0 + pzm) * ddxi);
-      // :609-614
+      // multi/main.f90:551-557 and :609-614, with each group's constant factor taken out of its
+      // sum (the same expression up to rounding: a few ulp of the terms, far inside the 1e-12
+      // parity bound):
+      //   rhs = -dxi/2 sum_d (u_d+ (phi+ + phi) - u_d (phi + phi-))                 advection
+      //         + gamma eps ddxi (sum of the six neighbours - 6 phi)                diffusion
+      //         - gamma dxi/2 sum_d (F_d+ - F_d-)                                   sharpening
       const double* Fx = sfx + slot(k);
       const double* Fy = sfy + slot(k);
-      rhs = rhs - gamma * ((Fx[1] - Fx[-1]) * hdxi + (Fy[PHX] - Fy[-PHX]) * hdxi + (z_p1 - z_m1) * hdxi);
+      const double adv = (__fma_rn(u_x, pxp + p0, -u_0 * (p0 + pxm)) + __fma_rn(v_y, pyp + p0, -v_0 * (p0 + pym))) +
+                         __fma_rn(w_z, pzp + p0, -w_0 * (p0 + pzm));
+      const double lap = ((pxp + pxm) + (pyp + pym)) + __fma_rn(-6.0, p0, pzp + pzm);
+      const double shp = ((Fx[1] - Fx[-1]) + (Fy[PHX] - Fy[-PHX])) + (z_p1 - z_m1);
+      const double rhs = __fma_rn(-hdxi, adv, __fma_rn(c_lap, lap, c_shp * shp));
       // :625-626
-      a.phin[c] = p0 + dt * (alpha * rhs - beta * ro);
+      a.phin[c] = __fma_rn(a.dta, rhs, __fma_rn(-a.dtb, ro, p0));
       a.rphio[c] = rhs;
       w0 = wzp;
       c += plane;
@@ -224,6 +228,8 @@ cudaError_t launch_phase(const PhaseArgs& a, cudaStream_t st) {
   // 148 SMs (the four planes of warm-up below a chunk cost 3% instead of 6%: 2.667 against
   // 2.723 ms at 512^3), otherwise PZC.  Results do not depend on the chunk.
   PhaseArgs b = a;
+  b.dta = a.g.dt * a.alpha;
+  b.dtb = a.g.dt * a.beta;
   if (b.zchunk <= 0) {
     const long long cols = (long long)((a.g.nx + PTX - 1) / PTX) * ((a.g.ny + PTY - 1) / PTY);
     b.zchunk = cols * ((a.g.nz + 127) / 128) >= 8 * 148 ? 128 : PZC;

@@ -45,6 +45,7 @@ struct PhaseArgs {
   double alpha, beta;
   int clamp;            // 1: phi clamped to [0,1] before the log
   int zchunk;           // z planes per block (0: default)
+  double dta = 0, dtb = 0;  // dt alpha, dt beta (set by launch_phase)
 };
 cudaError_t launch_phase(const PhaseArgs& a, cudaStream_t st);
 

@@ -922,9 +922,9 @@ int mhit_read_field(mhit_ctx* c, const char* path, int fieldn) {
   }
   MHIT_CUDA_TRY(cudaStreamSynchronize(c->st));
   // a field read happens at setup: the next step is an Euler step with empty history
-  // (multi/main.f90:440-441; rhs_o is not part of the files); a pressure read is kept as the
-  // incremental solve's predictor
-  return reset_history(c, fieldn == 4);
+  // (multi/main.f90:440-441; rhs_o is not part of the files); the pressure stays (a pressure
+  // read is the incremental solve's predictor, whichever field is read after it)
+  return reset_history(c, true);
 }
 
 // ------------------------------------------------------------------ checkpoint

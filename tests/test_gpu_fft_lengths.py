@@ -12,7 +12,9 @@ applies the same transform of ``multi/main.f90:853-912`` to the GPU's own input 
 stage.  Tolerances are relative to the largest magnitude of the stage's output:
 * FP64: 1e-12;
 * FP32 storage: 4e-6 -- a few FP32 rounding steps per butterfly stage (eps32 = 6e-8), far below
-  any indexing or twiddle error, which shows up at O(1).
+  any indexing or twiddle error, which shows up at O(1) -- except the z solve, 3e-5: its divide
+  by k^2 amplifies the forward transform's FP32 rounding at the smallest |k|, and on these thin
+  boxes (1024 cells of dx along x, 16 along y and z) k^2 spans five decades.
 The whole FP64 solve is also compared with the oracle's ``poisson_solve``.
 """
 import numpy as np
@@ -81,7 +83,7 @@ def test_poisson_stages_at_length(gpu, shape, poisson):
             hz = round32(hz)
         want = np.fft.ifft(hz, axis=0, norm="forward")
         e = rel(got, want)
-        assert e < tol, ("zsolve", e)
+        assert e < (3e-5 if f32 else tol), ("zsolve", e)
         # y inverse (:906)
         prev = got
         s.run_stage("yinv")
