@@ -37,6 +37,7 @@ extern "C" {
 #define MHIT_ERR_CFL (-4)      /* CFL > 7 after a step: the reference stops (multi/main.f90:1006) */
 #define MHIT_ERR_IO (-5)       /* file missing, short read or write */
 #define MHIT_ERR_STATE (-6)    /* call out of order (e.g. particles on a context without them) */
+#define MHIT_ERR_TIMEOUT (-7)  /* a bounded wait inside a kernel ran out (tensor-core z solve) */
 
 /* Poisson precision (multi/main.f90:844,853-912) */
 #define MHIT_POISSON_FP64 0    /* the intended FP64 solve of the main branch */
@@ -76,6 +77,8 @@ typedef struct mhit_params {
   int device;                /* CUDA device ordinal */
   int acdi_clamp;            /* 0: reference psi (phi < -1e-16 gives NaN, multi/main.f90:527-528);
                                 1: phi also clamped below at 0 before the log (opt-in deviation) */
+  int zsolve_tc;             /* 1: the 512-point z solve of the FP32 modes as BF16x3 split DFT-matrix
+                                GEMMs on the tensor cores (needs nz = 512 and a FP32 Poisson mode) */
 } mhit_params;
 
 /* Run control lines of input.inp (multi/readinput.f90:14-19, 34-35). */

@@ -18,6 +18,7 @@ MHIT_ERR_NAN = -3
 MHIT_ERR_CFL = -4
 MHIT_ERR_IO = -5
 MHIT_ERR_STATE = -6
+MHIT_ERR_TIMEOUT = -7
 MHIT_STATS_NOALLOC_MAX_PLANES = 1024  # include/mhit_b200.h
 
 POISSON = {"fp64": 0, "fp32": 1, "fp32_refined": 2, "fp32_incremental": 3}
@@ -38,6 +39,7 @@ class MhitParams(_c.Structure):
         ("phiflag", _c.c_int), ("partflag", _c.c_int), ("npart", _c.c_int),
         ("poisson", _c.c_int), ("laplacian", _c.c_int), ("interp", _c.c_int),
         ("yz_shift", _c.c_int), ("use_graph", _c.c_int), ("device", _c.c_int), ("acdi_clamp", _c.c_int),
+        ("zsolve_tc", _c.c_int),
     ]
 
 

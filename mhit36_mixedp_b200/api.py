@@ -53,6 +53,10 @@ class MhitStateError(MhitError):
     pass
 
 
+class MhitTimeoutError(MhitError):
+    pass
+
+
 _ERRS = {
     _lib.MHIT_ERR_ARG: MhitArgError,
     _lib.MHIT_ERR_CUDA: MhitCudaError,
@@ -60,6 +64,7 @@ _ERRS = {
     _lib.MHIT_ERR_CFL: MhitCFLError,
     _lib.MHIT_ERR_IO: MhitIOError,
     _lib.MHIT_ERR_STATE: MhitStateError,
+    _lib.MHIT_ERR_TIMEOUT: MhitTimeoutError,
 }
 
 
@@ -102,6 +107,7 @@ class Params:
     use_graph: bool = True
     acdi_clamp: int = 0
     device: int = 0
+    zsolve_tc: int = 0
 
     def __post_init__(self):
         self.ny = self.ny or self.nx
@@ -110,7 +116,7 @@ class Params:
     def to_c(self) -> MhitParams:
         c = MhitParams()
         _check(_lib.load().mhit_params_default(ctypes.byref(c)))
-        for f in ("nx", "ny", "nz", "phiflag", "partflag", "npart", "yz_shift", "device", "acdi_clamp"):
+        for f in ("nx", "ny", "nz", "phiflag", "partflag", "npart", "yz_shift", "device", "acdi_clamp", "zsolve_tc"):
             setattr(c, f, int(getattr(self, f)))
         for f in ("dt", "mu", "rho", "f1", "f2", "f3", "k0", "radius", "sigma", "epsr"):
             setattr(c, f, float(getattr(self, f)))

@@ -484,7 +484,9 @@ static cudaError_t poisson_stage_t(const PoissonArgs& a, int stage, cudaStream_t
   switch (stage) {
     case PSTAGE_XFWD: return launch_xfwd<T>(a, st);
     case PSTAGE_YFWD: return launch_cols<T, 0>(a, 1, st);
-    case PSTAGE_ZSOLVE: return launch_cols<T, 2>(a, 2, st);
+    case PSTAGE_ZSOLVE:
+      if (sizeof(T) == 4 && a.tcz) return launch_zsolve_tc(a.tcz, a, a.sc, st);
+      return launch_cols<T, 2>(a, 2, st);
     case PSTAGE_YINV: return launch_cols<T, 1>(a, 1, st);
     case PSTAGE_XINV: return launch_xinv<T>(a, st);
     case PSTAGE_ZFWD: return launch_cols<T, 0>(a, 2, st);

@@ -1,11 +1,18 @@
 // Host-side launchers of the timestep kernels (internal to libmhit_b200.so).
 #pragma once
 #include <cuda_runtime.h>
+
+#include <string>
+
+#include "../../include/mhit_b200.h"
 #include "common.cuh"
 
 namespace mhit {
 
+int set_error(int code, const std::string& msg);
 int set_cuda_error(cudaError_t e, const char* expr, const char* file, int line);
+
+struct ZsolveTc;  // tensor-core 512-point z solve: tensor map of the spectrum, DFT-matrix image, twiddles
 
 // ---------------------------------------------------------------- Poisson
 enum { PSTAGE_XFWD = 0, PSTAGE_YFWD, PSTAGE_ZSOLVE, PSTAGE_YINV, PSTAGE_XINV, PSTAGE_COUNT };
@@ -28,7 +35,13 @@ struct PoissonArgs {
   // into hi (written here) and lo (written to p) (incremental solve)
   float* pinc = nullptr;
   bool real64 = false;           // x-forward transforms the FP64 field u (energy spectrum)
+  const ZsolveTc* tcz = nullptr;  // non-null (FP32, nz = 512): the z solve runs on the tensor cores
+  DevScalars* sc = nullptr;       // flag word for the tensor-core z solve's bounded waits
 };
+bool zsolve_tc_supported(const Geo& g);
+int zsolve_tc_create(const Geo& g, void* spec, ZsolveTc** out);
+void zsolve_tc_destroy(ZsolveTc* z);
+cudaError_t launch_zsolve_tc(const ZsolveTc* z, const PoissonArgs& a, DevScalars* sc, cudaStream_t st);
 
 cudaError_t launch_combine(const float* p32, const float* d32, double* p64, size_t n, cudaStream_t st);
 cudaError_t poisson_stage(const PoissonArgs& a, int stage, cudaStream_t st);

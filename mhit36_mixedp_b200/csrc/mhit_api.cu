@@ -89,6 +89,7 @@ struct mhit_ctx {
   cudaEvent_t ev[2 * ST_COUNT] = {};
   int zchunk_phase = 0, zchunk_mom = 0;  // z planes per block of k_phase / k_mom (0: default)
   long long label_bound = 0;              // test hook: union-find loop bound (0: the cell count)
+  ZsolveTc* tcz = nullptr;                // tensor-core z solve (zsolve_tc = 1)
   int graph_kernels = 0;                  // kernel nodes in a captured step graph
 };
 
@@ -270,6 +271,8 @@ static int enqueue_stage(mhit_ctx* c, int stage, double alpha, double beta, int 
       a.k2z = c->k2z;
       a.cdiv = p.rho * c->g.dxi / p.dt;  // (rho*dxi/dt), multi/main.f90:841
       a.ntot = (double)c->g.nx * (double)c->g.ny * (double)c->g.nz;
+      a.tcz = c->tcz;
+      a.sc = c->sc;
       if (p.poisson == MHIT_POISSON_FP32_INCREMENTAL) {
         // the residual of the predictor P in the x pass; P <- hi, P2 <- lo in the x-inverse
         if (stage == ST_XFWD) a.presid = static_cast<const float*>(c->P);
@@ -502,6 +505,7 @@ void mhit_destroy(mhit_ctx* c) {
   cudaFree(c->k2z);
   cudaFree(c->tabs);
   cudaFree(c->partials);
+  zsolve_tc_destroy(c->tcz);
   cudaFree(c->sc);
   cudaFree(c->part);
   if (c->sc_host) cudaFreeHost(c->sc_host);
@@ -570,6 +574,7 @@ static int init_impl(const mhit_params* p, mhit_ctx* c) {
   MHIT_CUDA_TRY(cudaMalloc(&c->spec, (size_t)g.pitch * g.ny * g.nz * 2 * ts));
   MHIT_CUDA_TRY(cudaMemset(c->spec, 0, (size_t)g.pitch * g.ny * g.nz * 2 * ts));
   int rc;
+  if (p->zsolve_tc && (rc = zsolve_tc_create(g, c->spec, &c->tcz))) return rc;
   if (ts == 4) {
     if ((rc = upload_vec(&c->twx, twiddles<float>(g.nx)))) return rc;
     if ((rc = upload_vec(&c->twy, twiddles<float>(g.ny)))) return rc;
@@ -646,6 +651,9 @@ int mhit_init(const mhit_params* p, mhit_ctx** out) {
     return set_error(MHIT_ERR_ARG, "interp must be MHIT_INTERP_LINEAR1D or MHIT_INTERP_TRILINEAR");
   if (p->yz_shift != 0 && p->yz_shift != 1) return set_error(MHIT_ERR_ARG, "yz_shift must be 0 or 1");
   if (p->acdi_clamp != 0 && p->acdi_clamp != 1) return set_error(MHIT_ERR_ARG, "acdi_clamp must be 0 or 1");
+  if (p->zsolve_tc != 0 && p->zsolve_tc != 1) return set_error(MHIT_ERR_ARG, "zsolve_tc must be 0 or 1");
+  if (p->zsolve_tc && (p->poisson == MHIT_POISSON_FP64 || p->nz != 512))
+    return set_error(MHIT_ERR_ARG, "zsolve_tc needs nz = 512 and a FP32 Poisson mode");
   int ndev = 0;
   cudaError_t e = cudaGetDeviceCount(&ndev);
   if (e != cudaSuccess) return set_cuda_error(e, "cudaGetDeviceCount", __FILE__, __LINE__);
@@ -738,6 +746,8 @@ int mhit_step(mhit_ctx* c, int nsteps) {
   if (nsteps < 0) return set_error(MHIT_ERR_ARG, "nsteps < 0");
   if ((rc = enqueue_steps(c, nsteps))) return rc;
   if ((rc = fetch_scalars(c))) return rc;
+  if (c->sc_host->flag & 4)
+    return set_error(MHIT_ERR_TIMEOUT, "the tensor-core z solve gave up on a bounded wait (results invalid)");
   if (c->sc_host->flag & 1) return set_error(MHIT_ERR_NAN, "NaN in the velocity field");
   if (c->sc_host->flag & 2) {
     char b[128];

@@ -12,7 +12,7 @@ module mhit_gpu
   implicit none
 
   integer(c_int), parameter :: MHIT_OK = 0, MHIT_ERR_ARG = -1, MHIT_ERR_CUDA = -2, MHIT_ERR_NAN = -3
-  integer(c_int), parameter :: MHIT_ERR_CFL = -4, MHIT_ERR_IO = -5, MHIT_ERR_STATE = -6
+  integer(c_int), parameter :: MHIT_ERR_CFL = -4, MHIT_ERR_IO = -5, MHIT_ERR_STATE = -6, MHIT_ERR_TIMEOUT = -7
   integer(c_int), parameter :: MHIT_POISSON_FP64 = 0, MHIT_POISSON_FP32 = 1, MHIT_POISSON_FP32_REFINED = 2, &
                                 MHIT_POISSON_FP32_INCREMENTAL = 3
   integer(c_int), parameter :: MHIT_LAP_EXACT = 0, MHIT_LAP_MODIFIED = 1
@@ -26,6 +26,7 @@ module mhit_gpu
     integer(c_int) :: phiflag, partflag, npart
     integer(c_int) :: poisson, laplacian, interp, yz_shift, use_graph, device
     integer(c_int) :: acdi_clamp
+    integer(c_int) :: zsolve_tc
   end type mhit_params
 
   type, bind(C) :: mhit_run

@@ -126,7 +126,9 @@ def test_read_input_errors(tmp_path):
         api.read_input(str(p))
 
 
-@pytest.mark.parametrize("bad", [dict(nx=100), dict(nx=2048), dict(dt=-1.0), dict(poisson="fp16")])
+@pytest.mark.parametrize("bad", [dict(nx=100), dict(nx=2048), dict(dt=-1.0), dict(poisson="fp16"),
+                                 dict(poisson="fp32_incremental"), dict(zsolve_tc=1, poisson="fp32"),
+                                 dict(zsolve_tc=1, nz=512, poisson="fp64"), dict(zsolve_tc=2, nz=512, poisson="fp32")])
 def test_init_rejects_bad_params(bad):
     kw = dict(nx=32)
     kw.update(bad)
