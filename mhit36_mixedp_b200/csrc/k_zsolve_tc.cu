@@ -18,7 +18,7 @@
 // A CTA owns a tile of 8 kx columns at one y: 512 x 8 complex FP32 values, brought into shared
 // memory by two TMA boxes and written back the same way.  Its 128 threads (TMEM lanes 0-127)
 // own one GEMM row each: stage 1 and 4 rows (c, n2) (256 rows, two M = 128 MMAs), stage 2 and 3
-// rows (c, k1) (128 rows).  Between the GEMMs each thread reads its row of the accumulator
+// rows (c, k1) (128 rows); two CTAs share an SM.  Between the GEMMs each thread reads its row of the accumulator
 // (tcgen05.ld), applies the twiddles, the divide or the conjugations, splits the values into
 // BF16 terms and writes the next GEMM's A operand (canonical K-major layout, no swizzle).  The
 // DFT matrices (B operands) are staged once per CTA.  One elected thread issues the MMAs and
@@ -44,25 +44,26 @@ constexpr int TC_N = 512;           // transform length
 constexpr int TC_TMEM_COLS = 64;    // accumulator columns (power of two >= 32)
 
 // Canonical K-major layouts (no swizzle): a core matrix is 8 rows x 16 bytes; LBO is the byte
-// distance between core matrices along K, SBO along M/N.  The A operands use LBO = 144 (a
-// 16-byte pad per core matrix) so that the scattered 4-byte writes of a warp spread over all 32
-// banks; the B images use the dense LBO = 128.
-constexpr int A_LBO = 144;
-constexpr int A1_SBO = 592;                 // K = 32: 4 chunks of 144 bytes, padded to 592
-constexpr int A2_SBO = 1152;                // K = 64: 8 chunks of 144 bytes
-constexpr int A_TERM = 32 * A1_SBO;         // 18944 bytes: 256 rows of K = 32 (>= 16 groups x 1152)
+// distance between core matrices along K (dense: 128), SBO along M/N (all K chunks of a row
+// group).  Row orders are chosen so that every shared-memory access of a warp is free of bank
+// conflicts: stage 1 and 4 rows (c, n2) are m = 128 (n2 / 16) + 8 (n2 % 16) + c, stage 2 and 3 rows
+// (c, k1) are m = 8 k1 + c, i.e. the tile column c runs fastest in both.
+constexpr int A_LBO = 128;
+constexpr int A1_SBO = 4 * A_LBO;           // K = 32: 4 chunks
+constexpr int A2_SBO = 8 * A_LBO;           // K = 64: 8 chunks
+constexpr int A_TERM = 32 * A1_SBO;         // 16384 bytes: 256 rows of K = 32 = 128 rows of K = 64
 constexpr int B1_TERM = 4 * 512;            // N = 32, K = 32: 4 row groups x 4 chunks x 128 bytes
 constexpr int B2_TERM = 8 * 1024;           // N = 64, K = 64
 constexpr int B_IMAGE = 3 * (B1_TERM + B2_TERM);
 static_assert(16 * A2_SBO <= A_TERM, "A region holds every stage's operand");
 
-// shared memory plan (bytes from a 1024-aligned base)
+// shared memory plan (bytes from a 128-aligned base): 110 KB, two CTAs per SM
 constexpr int SM_TILE = 0;                            // 512 x 8 complex float = 32768
 constexpr int SM_A = SM_TILE + TC_N * TC_C * 8;       // 3 terms
 constexpr int SM_B = SM_A + 3 * A_TERM;               // B1 terms then B2 terms
 constexpr int SM_BAR = SM_B + B_IMAGE;                // two mbarriers + the TMEM address
 constexpr int SM_TOTAL = SM_BAR + 64;
-constexpr size_t SMEM_BYTES = SM_TOTAL + 1024;        // slack for the 1024-byte alignment
+constexpr size_t SMEM_BYTES = SM_TOTAL + 128;         // slack for the 128-byte alignment
 
 constexpr long long WAIT_LIMIT = 1ll << 26;  // polls of an mbarrier before giving up (seconds)
 
@@ -207,13 +208,13 @@ __device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 
-__global__ void __launch_bounds__(TC_NT, 1)
+__global__ void __launch_bounds__(TC_NT, 2)
 k_zsolve_tc(const __grid_constant__ CUtensorMap tmap, const uint4* __restrict__ bimg,
             const float2* __restrict__ w512, Geo g, const double* __restrict__ k2x,
             const double* __restrict__ k2y, const double* __restrict__ k2z, double ntot, int ntx,
             DevScalars* __restrict__ sc) {
   extern __shared__ unsigned char smraw[];
-  unsigned char* sm = reinterpret_cast<unsigned char*>(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
+  unsigned char* sm = reinterpret_cast<unsigned char*>(((uintptr_t)smraw + 127) & ~(uintptr_t)127);
   const int tid = threadIdx.x, warp = tid >> 5;
   float2* tile = reinterpret_cast<float2*>(sm + SM_TILE);
   unsigned char* A = sm + SM_A;
@@ -283,15 +284,16 @@ k_zsolve_tc(const __grid_constant__ CUtensorMap tmap, const uint4* __restrict__ 
       tma_phase ^= 1;
       if (!__syncthreads_and(done)) { ok = false; break; }
     }
-    // ---- stage 1 operand: rows (c, n2) = t and t + 128, K = (n1, re/im)
-    const int n2 = tid & 31;
+    // ---- stage 1 operand: rows (c, n2) = 128 h + tid with c = tid % 8, n2 = 16 h + tid / 8;
+    // K = (n1, re/im).  A warp reads 32 consecutive complex values of the tile per n1.
+    const int cc = tid & 7, nq = tid >> 3;
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
-      const int c = 4 * h + warp;
+      const int n2 = 16 * h + nq;
       float v[32];
 #pragma unroll
       for (int n1 = 0; n1 < 16; ++n1) {
-        const float2 z = tile[(32 * n1 + n2) * TC_C + c];
+        const float2 z = tile[(32 * n1 + n2) * TC_C + cc];
         v[2 * n1] = z.x;
         v[2 * n1 + 1] = z.y;
       }
@@ -308,16 +310,16 @@ k_zsolve_tc(const __grid_constant__ CUtensorMap tmap, const uint4* __restrict__ 
     }
     mma_pending = true;
     if (!wait_mma()) { ok = false; break; }
-    // ---- twiddle W512^(n2 k1), stage 2 operand: rows (c, k1), K = (n2, re/im)
+    // ---- twiddle W512^(n2 k1), stage 2 operand: rows (c, k1) = 8 k1 + c, K = (n2, re/im)
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       float r[32];
       tmem_ld32(lane_addr + 32 * h, r);
-      const int c = 4 * h + warp;
+      const int n2 = 16 * h + nq;
 #pragma unroll
       for (int k1 = 0; k1 < 16; ++k1) {
         const float2 z = cmulf(make_float2(r[2 * k1], r[2 * k1 + 1]), __ldg(&w512[(n2 * k1) & 511]));
-        put_pair(A, 16 * c + k1, n2, A2_SBO, z.x, z.y);
+        put_pair(A, 8 * k1 + cc, n2, A2_SBO, z.x, z.y);
       }
     }
     fence_before_sync();
@@ -334,7 +336,7 @@ k_zsolve_tc(const __grid_constant__ CUtensorMap tmap, const uint4* __restrict__ 
       float r[64];
       tmem_ld32(lane_addr, *reinterpret_cast<float(*)[32]>(r));
       tmem_ld32(lane_addr + 32, *reinterpret_cast<float(*)[32]>(r + 32));
-      const int c = tid >> 4, k1 = tid & 15, kx = kx0 + c;
+      const int c = cc, k1 = nq, kx = kx0 + c;  // row 8 k1 + c
       const bool col = kx < nkx;
       const double kxy = col ? k2x[kx] + k2y[y] : 0.0;
 #pragma unroll
@@ -361,16 +363,17 @@ k_zsolve_tc(const __grid_constant__ CUtensorMap tmap, const uint4* __restrict__ 
     }
     mma_pending = true;
     if (!wait_mma()) { ok = false; break; }
-    // ---- twiddle W512^(n2 k1) of conj(Z), stage 4 operand: rows (c, n2), K = (k1, re/im)
+    // ---- twiddle W512^(n2 k1) of conj(Z), stage 4 operand: rows (c, n2) as in stage 1,
+    // K = (k1, re/im)
     {
       float r[64];
       tmem_ld32(lane_addr, *reinterpret_cast<float(*)[32]>(r));
       tmem_ld32(lane_addr + 32, *reinterpret_cast<float(*)[32]>(r + 32));
-      const int c = tid >> 4, k1 = tid & 15;
+      const int k1 = nq;
 #pragma unroll
       for (int m2 = 0; m2 < 32; ++m2) {
         const float2 z = cmulf(make_float2(r[2 * m2], r[2 * m2 + 1]), __ldg(&w512[(m2 * k1) & 511]));
-        put_pair(A, 32 * c + m2, k1, A1_SBO, z.x, z.y);
+        put_pair(A, 128 * (m2 >> 4) + 8 * (m2 & 15) + cc, k1, A1_SBO, z.x, z.y);
       }
     }
     fence_before_sync();
@@ -390,9 +393,9 @@ k_zsolve_tc(const __grid_constant__ CUtensorMap tmap, const uint4* __restrict__ 
     for (int h = 0; h < 2; ++h) {
       float r[32];
       tmem_ld32(lane_addr + 32 * h, r);
-      const int c = 4 * h + warp;
+      const int n2 = 16 * h + nq;
 #pragma unroll
-      for (int n1 = 0; n1 < 16; ++n1) tile[(32 * n1 + n2) * TC_C + c] = make_float2(r[2 * n1], -r[2 * n1 + 1]);
+      for (int n1 = 0; n1 < 16; ++n1) tile[(32 * n1 + n2) * TC_C + cc] = make_float2(r[2 * n1], -r[2 * n1 + 1]);
     }
     fence_async_smem();
     fence_before_sync();
@@ -532,7 +535,7 @@ cudaError_t launch_zsolve_tc(const ZsolveTc* z, const PoissonArgs& a, DevScalars
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   const int ntiles = ntx * g.ny;
-  const int grid = ntiles < nsm ? ntiles : nsm;
+  const int grid = ntiles < 2 * nsm ? ntiles : 2 * nsm;  // two CTAs per SM
   k_zsolve_tc<<<grid, TC_NT, SMEM_BYTES, st>>>(z->tmap, static_cast<const uint4*>(z->bimg),
                                                static_cast<const float2*>(z->w512), g, a.k2x, a.k2y, a.k2z, a.ntot,
                                                ntx, sc);
