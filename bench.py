@@ -430,15 +430,20 @@ def run_large_ns(args):
 
 
 def tracers_measure(fields, device, steps, warmup, npart=1_000_000):
-    """512^3 NS+ACDI with 1e6 uniform tracers (seed 3): FP64 Poisson with both interpolation modes
-    and FP32 Poisson with trilinear interpolation."""
+    """512^3 NS+ACDI with 1e6 uniform tracers (seed 3): FP64 Poisson with both interpolation modes,
+    FP32 Poisson with trilinear interpolation, and the configuration's own Poisson: the
+    tensor-core DFT z solve (BF16x3 split, FP32 accumulation) inside the incremental FP32 solve,
+    whose right-hand side is the FP64 residual (discrete Laplacian)."""
     from mhit36_mixedp_b200 import Params, Solver, synth
     prm, u, v, w, phi = fields
     part = synth.uniform_particles(npart, 3)
     prm = dict(prm, partflag=1, npart=npart)
     res = {}
-    for poisson, interp in (("fp64", "linear1d"), ("fp64", "trilinear"), ("fp32", "trilinear")):
-        with Solver(Params(device=device, poisson=poisson, interp=interp, **prm)) as s:
+    for poisson, interp, lap, tc in (("fp64", "linear1d", "exact", 0), ("fp64", "trilinear", "exact", 0),
+                                     ("fp32", "trilinear", "exact", 0),
+                                     ("fp32_incremental", "trilinear", "modified", 0),
+                                     ("fp32_incremental", "trilinear", "modified", 1)):
+        with Solver(Params(device=device, poisson=poisson, interp=interp, laplacian=lap, zsolve_tc=tc, **prm)) as s:
             s.upload(u, v, w, phi)
             s.upload_particles(part)
             s.step(max(warmup, 3))
@@ -446,8 +451,12 @@ def tracers_measure(fields, device, steps, warmup, npart=1_000_000):
                 ms = s.time_steps(steps)
             s.step(0)
             prof = [s.profile_step() for _ in range(3)]
+            dg = s.diagnostics()
         tr = statistics.mean(p["k_tracer"] for p in prof)
-        res[f"{poisson}_{interp}"] = {"ms_per_step": ms / steps, "tracer_stage_ms": tr, "clocks": clk.summary()}
+        zs = statistics.mean(p["k_fft_cols_zsolve"] for p in prof)
+        key = f"{poisson}_{interp}" + ("_tensorcore_zsolve" if tc else "") + ("_modified" if lap == "modified" else "")
+        res[key] = {"ms_per_step": ms / steps, "tracer_stage_ms": tr, "zsolve_stage_ms": zs, "maxdiv": dg["maxdiv"],
+                    "clocks": clk.summary()}
     return res
 
 

@@ -72,8 +72,13 @@ k_div_fftx(const double* __restrict__ u, const double* __restrict__ v, const dou
       const size_t row = ((size_t)k * ny + j) * nx;
       const size_t rowy = ((size_t)k * ny + jp) * nx;
       const size_t rowz = ((size_t)kp * ny + j) * nx;
+      // with M a multiple of 32 a warp covers 32 consecutive pairs of one line (n % 32 == lane), so
+      // the x neighbours of a pair come from the adjacent lanes; only the warp's edge lanes load
+      constexpr bool SHFL = M % 32 == 0;
+      const int lane = threadIdx.x & 31;
       const double2 uu = __ldg(reinterpret_cast<const double2*>(u + row + i));
-      const double un = __ldg(u + row + (i + 2 == nx ? 0 : i + 2));
+      double un = SHFL ? __shfl_down_sync(0xffffffffu, uu.x, 1) : 0.0;
+      if (!SHFL || lane == 31) un = __ldg(u + row + (i + 2 == nx ? 0 : i + 2));
       const double2 vv = __ldg(reinterpret_cast<const double2*>(v + row + i));
       const double2 vp = __ldg(reinterpret_cast<const double2*>(v + rowy + i));
       const double2 ww = __ldg(reinterpret_cast<const double2*>(w + row + i));
@@ -90,8 +95,10 @@ k_div_fftx(const double* __restrict__ u, const double* __restrict__ v, const dou
         const int jm = wrapm(j, ny), km = wrapm(k, nz);
         const double ddxi = g.ddxi;
         const float2 qc = __ldg(reinterpret_cast<const float2*>(rr + row + i));
-        const float qxm = __ldg(rr + row + (i == 0 ? nx - 1 : i - 1));
-        const float qxp = __ldg(rr + row + (i + 2 == nx ? 0 : i + 2));
+        float qxm = SHFL ? __shfl_up_sync(0xffffffffu, qc.y, 1) : 0.f;
+        float qxp = SHFL ? __shfl_down_sync(0xffffffffu, qc.x, 1) : 0.f;
+        if (!SHFL || lane == 0) qxm = __ldg(rr + row + (i == 0 ? nx - 1 : i - 1));
+        if (!SHFL || lane == 31) qxp = __ldg(rr + row + (i + 2 == nx ? 0 : i + 2));
         const float2 qyp = __ldg(reinterpret_cast<const float2*>(rr + rowy + i));
         const float2 qym = __ldg(reinterpret_cast<const float2*>(rr + ((size_t)k * ny + jm) * nx + i));
         const float2 qzp = __ldg(reinterpret_cast<const float2*>(rr + rowz + i));

@@ -56,11 +56,12 @@ def main(argv=None):
     ap.add_argument("--outdir", default=None, help="write field files here every dump steps")
     ap.add_argument("--dt", type=float)
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--zsolve-tc", action="store_true", help="512-point z solve on the tensor cores (FP32 modes)")
     args = ap.parse_args(argv)
 
     run = {"restart": 0, "tstart": 0, "tfin": 10, "dump": 10 ** 9, "inflow": 0, "inphi": 0}
     kw = dict(nx=args.n, ny=args.ny or args.n, nz=args.nz or args.n, phiflag=args.phiflag, poisson=args.poisson,
-              laplacian=args.laplacian, device=args.device)
+              laplacian=args.laplacian, device=args.device, zsolve_tc=int(args.zsolve_tc))
     if args.input:
         prm, run = api.read_input(args.input, **kw)
     else:
