@@ -62,12 +62,12 @@ TRAFFIC_PER_POINT = {"k_phase": 55.1, "k_mom": 104.4, "k_div_fftx": 28.4, "k_fft
                      "k_fft_cols_zsolve": 7.5, "k_fft_cols_yinv": 7.5, "k_fftx_inv": 7.5,
                      "k_correct+k_finalize": 51.2}
 TRAFFIC_SOURCE = {"k_phase": "256^3", "k_mom": "256^3"}
-BYTES_PER_POINT["fp32_incremental"] = dict(BYTES_PER_POINT["fp32"], k_div_fftx=32, k_fftx_inv=16,
+BYTES_PER_POINT["fp32_incremental"] = dict(BYTES_PER_POINT["fp32"], k_div_fftx=32, k_fftx_inv=20,
                                            **{"k_correct+k_finalize": 56})
 # the step-level model: NS+ACDI 256 B/pt (FP32 Poisson), 280 B/pt (FP64); the incremental FP32
-# solve adds the predictor's read in the x pass (4), its read and the hi/lo split in the x-inverse
-# (8) and the second pressure array in the projection (4): 272 B/pt
-STEP_BYTES = {"fp32": 256, "fp64": 280, "fp32_incremental": 272}
+# solve adds the predictor's read in the x pass (4), the predictor's read and rewrite and the
+# FP64 pressure's write in the x-inverse (12) and the FP64 pressure in the projection (4): 276 B/pt
+STEP_BYTES = {"fp32": 256, "fp64": 280, "fp32_incremental": 276}
 
 
 def peaks():

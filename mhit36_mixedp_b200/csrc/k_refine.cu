@@ -7,9 +7,7 @@
 //   L_h delta = r                    (a second FP32 solve, same kernels)
 //   p = p32 + delta                  (in FP64 inside k_correct)
 // which brings the projected divergence back to FP64 round-off.
-// MHIT_POISSON_FP32_INCREMENTAL: one FP32 solve per step for the increment over the previous
-// step's pressure, p = q + delta with q the predictor, kept as hi + lo (k_fftx_inv's split).
-// k_combine materialises either pressure in FP64 for a download.
+// k_combine materialises that pressure in FP64 for a download.
 #include "common.cuh"
 #include "kernels.h"
 

@@ -31,9 +31,10 @@ struct PoissonArgs {
   // non-null: x-forward transforms the FP64 residual rho/dt div(u*) - L_h presid of this FP32
   // pressure (refinement sweep, incremental solve)
   const float* presid = nullptr;
-  // non-null: x-inverse adds its transform to this FP32 predictor in FP64 and splits the sum
-  // into hi (written here) and lo (written to p) (incremental solve)
+  // non-null: x-inverse adds its transform to this FP32 predictor in FP64, writes the sum to p64
+  // and its FP32 rounding back here (incremental solve)
   float* pinc = nullptr;
+  double* p64 = nullptr;
   bool real64 = false;           // x-forward transforms the FP64 field u (energy spectrum)
   const ZsolveTc* tcz = nullptr;  // non-null (FP32, nz = 512): the z solve runs on the tensor cores
   DevScalars* sc = nullptr;       // flag word for the tensor-core z solve's bounded waits

@@ -61,8 +61,8 @@ struct mhit_ctx {
   double *RU = nullptr, *RV = nullptr, *RW = nullptr;
   double *PHI[2] = {}, *RPHI = nullptr;
   void* P = nullptr;
-  float* P2 = nullptr;    // refinement: the pressure correction; incremental: the lo part (FP32)
-  double* P64 = nullptr;  // refinement: corrected pressure (FP64)
+  float* P2 = nullptr;    // refinement: the pressure correction (FP32)
+  double* P64 = nullptr;  // refinement: corrected pressure for a download; incremental: the pressure (FP64)
   double* Pw = nullptr;   // FP32 modes: the pressure widened to FP64 for a download (lazy)
   void* lab_small = nullptr;  // droplet labelling scratch (trig tables, chunk counts), grown lazily
   size_t lab_small_bytes = 0;
@@ -95,10 +95,8 @@ struct mhit_ctx {
 
 // ------------------------------------------------------------------ helpers
 static size_t tsize(const mhit_ctx* c) { return c->prm.poisson == MHIT_POISSON_FP64 ? 8 : 4; }
-// the modes whose pressure is the FP64 sum of two FP32 arrays (P and P2)
-static bool two_part_pressure(const mhit_ctx* c) {
-  return c->prm.poisson == MHIT_POISSON_FP32_REFINED || c->prm.poisson == MHIT_POISSON_FP32_INCREMENTAL;
-}
+static bool refined(const mhit_ctx* c) { return c->prm.poisson == MHIT_POISSON_FP32_REFINED; }
+static bool incremental(const mhit_ctx* c) { return c->prm.poisson == MHIT_POISSON_FP32_INCREMENTAL; }
 
 static int check_ctx(mhit_ctx* c) {
   if (!c) return set_error(MHIT_ERR_ARG, "null context");
@@ -143,9 +141,9 @@ static int reset_history(mhit_ctx* c, bool keep_pressure = false) {
   MHIT_CUDA_TRY(cudaMemsetAsync(c->RV, 0, bytes, c->st));
   MHIT_CUDA_TRY(cudaMemsetAsync(c->RW, 0, bytes, c->st));
   if (c->RPHI) MHIT_CUDA_TRY(cudaMemsetAsync(c->RPHI, 0, bytes, c->st));
-  if (c->prm.poisson == MHIT_POISSON_FP32_INCREMENTAL && !keep_pressure) {  // the predictor restarts at 0
+  if (incremental(c) && !keep_pressure) {  // the pressure restarts at 0
     MHIT_CUDA_TRY(cudaMemsetAsync(c->P, 0, c->n * sizeof(float), c->st));
-    MHIT_CUDA_TRY(cudaMemsetAsync(c->P2, 0, c->n * sizeof(float), c->st));
+    MHIT_CUDA_TRY(cudaMemsetAsync(c->P64, 0, c->n * sizeof(double), c->st));
   }
   DevScalars s;
   memset(&s, 0, sizeof(s));
@@ -273,12 +271,13 @@ static int enqueue_stage(mhit_ctx* c, int stage, double alpha, double beta, int 
       a.ntot = (double)c->g.nx * (double)c->g.ny * (double)c->g.nz;
       a.tcz = c->tcz;
       a.sc = c->sc;
-      if (p.poisson == MHIT_POISSON_FP32_INCREMENTAL) {
-        // the residual of the predictor P in the x pass; P <- hi, P2 <- lo in the x-inverse
+      if (incremental(c)) {
+        // the residual of the predictor P in the x pass; the x-inverse writes the pressure
+        // P + delta to P64 in FP64 and its FP32 rounding to P
         if (stage == ST_XFWD) a.presid = static_cast<const float*>(c->P);
         if (stage == ST_XINV) {
           a.pinc = static_cast<float*>(c->P);
-          a.p = c->P2;
+          a.p64 = c->P64;
         }
       }
       if (stage != ST_REFINE) {
@@ -298,9 +297,9 @@ static int enqueue_stage(mhit_ctx* c, int stage, double alpha, double beta, int 
       a.u = c->U[nxt];
       a.v = c->V[nxt];
       a.w = c->W[nxt];
-      a.p = c->P;
-      a.fp32 = p.poisson != MHIT_POISSON_FP64;
-      a.pd = two_part_pressure(c) ? c->P2 : nullptr;
+      a.p = incremental(c) ? static_cast<void*>(c->P64) : c->P;
+      a.fp32 = p.poisson != MHIT_POISSON_FP64 && !incremental(c);
+      a.pd = refined(c) ? c->P2 : nullptr;
       a.partials = c->partials;
       a.nblocks = c->nblk;
       a.sc = c->sc;
@@ -564,9 +563,11 @@ static int init_impl(const mhit_params* p, mhit_ctx* c) {
   if (p->phiflag) MHIT_CUDA_TRY(cudaMalloc(&c->RPHI, fb));
   const size_t ts = tsize(c);
   MHIT_CUDA_TRY(cudaMalloc(&c->P, n * ts));
-  if (two_part_pressure(c)) {
+  if (refined(c)) {
     MHIT_CUDA_TRY(cudaMalloc(&c->P2, n * sizeof(float)));
     MHIT_CUDA_TRY(cudaMemset(c->P2, 0, n * sizeof(float)));
+  }
+  if (refined(c) || incremental(c)) {
     MHIT_CUDA_TRY(cudaMalloc(&c->P64, n * sizeof(double)));
     MHIT_CUDA_TRY(cudaMemset(c->P64, 0, n * sizeof(double)));
   }
@@ -827,7 +828,9 @@ int mhit_download_fields(mhit_ctx* c, double* u, double* v, double* w, double* p
   if (phi) MHIT_CUDA_TRY(cudaMemcpyAsync(phi, c->PHI[c->cur], fb, cudaMemcpyDeviceToHost, c->st));
   if (p) {
     const double* src = static_cast<const double*>(c->P);
-    if (c->P64) {  // refinement / incremental: materialise p = P + P2 in FP64
+    if (incremental(c)) {  // the FP64 pressure of the last projection
+      src = c->P64;
+    } else if (c->P2) {  // refinement: materialise p = P + P2 in FP64
       MHIT_CUDA_TRY(launch_combine(static_cast<const float*>(c->P), c->P2, c->P64, c->n, c->st));
       src = c->P64;
     } else if (tsize(c) == 4) {
@@ -916,15 +919,12 @@ int mhit_read_field(mhit_ctx* c, const char* path, int fieldn) {
     MHIT_CUDA_TRY(cudaMemcpyAsync(c->PHI[c->cur], buf.data(), fb, cudaMemcpyHostToDevice, c->st));
   } else {
     if (tsize(c) == 4) {
-      // FP32 pressure; in the two-part modes also the remainder, so P + P2 is the file's value
-      // to FP64 precision (the incremental solve's predictor for the next step)
-      std::vector<float> pf(c->n), lo(c->P2 ? c->n : 0);
-      for (size_t i = 0; i < c->n; ++i) {
-        pf[i] = (float)buf[i];
-        if (c->P2) lo[i] = (float)(buf[i] - (double)pf[i]);
-      }
+      // FP32 pressure (the incremental solve's predictor for the next step); the incremental
+      // mode also keeps the file's FP64 values
+      std::vector<float> pf(c->n);
+      for (size_t i = 0; i < c->n; ++i) pf[i] = (float)buf[i];
       MHIT_CUDA_TRY(cudaMemcpyAsync(c->P, pf.data(), c->n * 4, cudaMemcpyHostToDevice, c->st));
-      if (c->P2) MHIT_CUDA_TRY(cudaMemcpyAsync(c->P2, lo.data(), c->n * 4, cudaMemcpyHostToDevice, c->st));
+      if (incremental(c)) MHIT_CUDA_TRY(cudaMemcpyAsync(c->P64, buf.data(), fb, cudaMemcpyHostToDevice, c->st));
       MHIT_CUDA_TRY(cudaStreamSynchronize(c->st));
     } else {
       MHIT_CUDA_TRY(cudaMemcpyAsync(c->P, buf.data(), fb, cudaMemcpyHostToDevice, c->st));
@@ -962,7 +962,8 @@ std::vector<CkptArray> ckpt_arrays(mhit_ctx* c) {
     a.push_back({c->RPHI, fb});
   }
   a.push_back({c->P, c->n * tsize(c)});
-  if (c->P2) a.push_back({c->P2, c->n * sizeof(float)});  // refinement / incremental: the second part
+  if (c->P2) a.push_back({c->P2, c->n * sizeof(float)});  // refinement: the correction
+  if (incremental(c)) a.push_back({c->P64, c->n * sizeof(double)});  // incremental: the FP64 pressure
   return a;
 }
 

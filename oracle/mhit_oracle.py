@@ -464,16 +464,14 @@ def laplacian7(p: Params, q):
 def poisson_solve_incremental(p: Params, rhsp, pred32):
     """One FP32 solve for the increment over the previous step's pressure (needs the modified
     Laplacian).  r = rhs - L_h q in FP64 with q the FP32 predictor, L_h delta = r in FP32, and
-    s = q + delta in FP64, kept as hi = fl32(s) and lo = fl32(s - hi).  Returns (hi + lo in FP64,
-    the pressure the projection uses; hi, the next step's predictor)."""
+    s = q + delta in FP64.  Returns (s, the pressure the projection uses; fl32(s), the next
+    step's predictor)."""
     if p.laplacian != "modified":
         raise ValueError("fp32_incremental needs the modified Laplacian")
     q = pred32.astype(np.float64)
     delta = solve32(p, rhsp - laplacian7(p, q))
     s = q + delta.astype(np.float64)
-    hi = s.astype(np.float32)
-    lo = (s - hi.astype(np.float64)).astype(np.float32)
-    return hi.astype(np.float64) + lo.astype(np.float64), hi
+    return s, s.astype(np.float32)
 
 
 def fft3_r2c_f32(a32):
