@@ -306,6 +306,10 @@ int mhit_debug_commit_step(mhit_ctx* ctx);
  * no parent chain or link retry sequence can exceed).  A small bound makes a legitimate chain
  * run out, so a test can drive the bounded-loop error path (MHIT_ERR_STATE) without a fault. */
 int mhit_debug_set_label_bound(mhit_ctx* ctx, long long bound);
+/* 1 (the default): the momentum kernel fills the plane rings of the tiles that need no periodic
+ * wrap with TMA boxes; 0: every tile copies 16-byte pairs per thread.  Both give the same bits
+ * (a test compares them). */
+int mhit_debug_set_mom_tma(mhit_ctx* ctx, int on);
 long long mhit_debug_buffer_len(mhit_ctx* ctx, int which);
 int mhit_debug_get_buffer(mhit_ctx* ctx, int which, double* out);
 

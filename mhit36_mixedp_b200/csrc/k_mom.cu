@@ -40,16 +40,50 @@ constexpr int CPX = MTX + 1, CPY = MTY + 1;   // chempot plane: x,y in [-1, T)
 constexpr int CPL = CPX * CPY;
 constexpr int UPAIRS = UPY * (UPX / 2), PPAIRS = PPY * (PPX / 2);  // 16-byte copies per plane
 static_assert(UPAIRS <= MNT && PPAIRS <= MNT, "one pair per thread and plane");
+// ring slots padded to whole 128-byte lines, the alignment a TMA box destination needs
+constexpr int UPS = (UPL * 8 + 127) / 128 * 16, PPS = (PPL * 8 + 127) / 128 * 16;  // doubles
+constexpr unsigned UBYTES = UPL * 8, PBYTES = PPL * 8;  // bytes of one box
 
 template <bool PHI> struct MomSmem;
 template <> struct MomSmem<false> {
-  double u[4][UPL], v[4][UPL], w[4][UPL];
+  double u[4][UPS], v[4][UPS], w[4][UPS];
+  unsigned long long bar[2];  // TMA completion, one per alternating group of boxes
 };
 template <> struct MomSmem<true> {
-  double u[4][UPL], v[4][UPL], w[4][UPL];
-  double phi[8][PPL];
+  double u[4][UPS], v[4][UPS], w[4][UPS];
+  double phi[8][PPS];
   double cp[4][CPL];
+  unsigned long long bar[2];
 };
+
+constexpr long long MOM_WAIT_LIMIT = 1ll << 26;  // polls of an mbarrier before giving up (seconds)
+
+__device__ __forceinline__ uint32_t sm_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void tma_box(const void* dst, const CUtensorMap* map, int x, int y, int z, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+      ::"r"(sm_addr(dst)), "l"(map), "r"(x), "r"(y), "r"(z), "r"(bar)
+      : "memory");
+}
+
+__device__ __forceinline__ void expect_tx(uint32_t bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t parity) {
+  for (long long it = 0; it < MOM_WAIT_LIMIT; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (it > 64) __nanosleep(32);
+  }
+  return false;
+}
 
 // 16-byte global -> shared copy through L2 only (cp.async.cg)
 __device__ __forceinline__ void cp16(void* dst, const void* src) {
@@ -63,8 +97,8 @@ __device__ __forceinline__ int pmod_int(int x, int n) {
 }
 
 template <bool PHI>
-__global__ void __launch_bounds__(MNT, 3) k_mom(MomArgs a) {
-  extern __shared__ __align__(16) unsigned char smraw[];
+__global__ void __launch_bounds__(MNT, 3) k_mom(const __grid_constant__ MomArgs a) {
+  extern __shared__ __align__(128) unsigned char smraw[];
   MomSmem<PHI>& S = *reinterpret_cast<MomSmem<PHI>*>(smraw);
   const Geo& g = a.g;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
@@ -105,6 +139,33 @@ __global__ void __launch_bounds__(MNT, 3) k_mom(MomArgs a) {
   };
   auto issue_phi = [&](int m) { copy_phi(m, (size_t)pmod_int(m, nz) * plane); };
 
+  // A block whose rings need no periodic wrap in x and y has every ring plane in one TMA box per
+  // field (x from i0-2, y from j0-1 for u, v, w and from j0-2 for phi; z wraps by the plane
+  // index): one thread issues the boxes of a plane group and an mbarrier tracks their bytes.
+  // The other blocks copy 16-byte pairs per thread (cp.async).  Groups alternate between the two
+  // barriers: group g (0: the loop's prologue, then one per iteration) completes phase g/2 of
+  // bar[g % 2].
+  const bool tma = a.tma && i0 >= 2 && i0 + MTX + 2 <= nx && j0 >= 2 && j0 + MTY + 1 <= ny;
+  const uint32_t bar0 = sm_addr(&S.bar[0]);
+  if (tma && tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar0) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar0 + 8) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (tma) __syncthreads();
+  auto tma_uvw = [&](int m, uint32_t bar) {
+    const int su = (m - k0 + 16) & 3, z = pmod_int(m, nz);
+    tma_box(&S.u[su][0], &a.tmu, i0 - 2, j0 - 1, z, bar);
+    tma_box(&S.v[su][0], &a.tmv, i0 - 2, j0 - 1, z, bar);
+    tma_box(&S.w[su][0], &a.tmw, i0 - 2, j0 - 1, z, bar);
+  };
+  auto tma_phi = [&](int m, uint32_t bar) {
+    if constexpr (PHI)
+      tma_box(&reinterpret_cast<MomSmem<true>&>(S).phi[(m - k0 + 16) & 7][0], &a.tmphi, i0 - 2, j0 - 2,
+              pmod_int(m, nz), bar);
+  };
+  bool waits_ok = true;
+
   const double eps = g.eps, epsi = g.epsi, ddxi = g.ddxi, dxi = g.dxi;
   // chemical potential (multi/main.f90:735) of plane m over the CPX x CPY region
   auto chempot_plane = [&](int m) {
@@ -129,17 +190,34 @@ __global__ void __launch_bounds__(MNT, 3) k_mom(MomArgs a) {
   // earlier.  With the phase field the loop starts at k0-2 (k0-2, k0-1 only fill the chemical
   // potential of k0-1 and k0), so every chemical potential comes from the loop body.
   const int ks = PHI ? k0 - 2 : k0;
-  if constexpr (PHI) {
-    issue_phi(k0 - 2);
-    issue_phi(k0 - 1);
-    issue_phi(k0);
-    issue_uvw(k0 - 1);
+  if (tma) {
+    if (tid == 0) {
+      if constexpr (PHI) {
+        expect_tx(bar0, 3 * UBYTES + 3 * PBYTES);
+        tma_phi(k0 - 2, bar0);
+        tma_phi(k0 - 1, bar0);
+        tma_phi(k0, bar0);
+        tma_uvw(k0 - 1, bar0);
+      } else {
+        expect_tx(bar0, 9 * UBYTES);
+        tma_uvw(k0 - 1, bar0);
+        tma_uvw(k0, bar0);
+        tma_uvw(k0 + 1, bar0);
+      }
+    }
   } else {
-    issue_uvw(k0 - 1);
-    issue_uvw(k0);
-    issue_uvw(k0 + 1);
+    if constexpr (PHI) {
+      issue_phi(k0 - 2);
+      issue_phi(k0 - 1);
+      issue_phi(k0);
+      issue_uvw(k0 - 1);
+    } else {
+      issue_uvw(k0 - 1);
+      issue_uvw(k0);
+      issue_uvw(k0 + 1);
+    }
+    __pipeline_commit();
   }
-  __pipeline_commit();
 
   const int tx = tid % MTX, ty = tid / MTX;
   const int i = i0 + tx, j = j0 + ty;
@@ -169,15 +247,29 @@ __global__ void __launch_bounds__(MNT, 3) k_mom(MomArgs a) {
       rvo = a.rv[c];
       rwo = a.rw[c];
     }
-    // this thread's copies landed; after the barrier everyone's have, and everyone is done
-    // with iteration k-1
-    __pipeline_wait_prior(0);
+    // the copies issued one iteration earlier have landed (this thread's, or the block's TMA
+    // group); after the barrier everyone's have, and everyone is done with iteration k-1
+    if (tma) {
+      const int gi = k - ks;
+      if (!bar_wait(bar0 + 8 * (gi & 1), (gi >> 1) & 1)) waits_ok = false;
+    } else {
+      __pipeline_wait_prior(0);
+    }
     __syncthreads();
     if (k + 1 < k1) {
-      issue_uvw(k + 2);
-      issue_phi(k + 3);
+      if (tma) {
+        if (tid == 0) {
+          const uint32_t b = bar0 + 8 * ((k - ks + 1) & 1);
+          expect_tx(b, PHI ? 3 * UBYTES + PBYTES : 3 * UBYTES);
+          tma_uvw(k + 2, b);
+          tma_phi(k + 3, b);
+        }
+      } else {
+        issue_uvw(k + 2);
+        issue_phi(k + 3);
+      }
     }
-    __pipeline_commit();
+    if (!tma) __pipeline_commit();
     if (k + 1 < k1) chempot_plane(k + 1);
     if (out) {
       const int sm = (k - k0 + 15) & 3, s0 = (k - k0 + 16) & 3, sp = (k - k0 + 17) & 3;
@@ -245,6 +337,9 @@ __global__ void __launch_bounds__(MNT, 3) k_mom(MomArgs a) {
     }
   }
   __pipeline_wait_prior(0);
+  // a TMA wait that ran out (the boxes never arrived) is reported through the flag word; the
+  // step then fails with MHIT_ERR_TIMEOUT
+  if (!waits_ok) atomicOr(&const_cast<DevScalars*>(a.sc)->flag, 4);
 }
 
 template <bool PHI>
@@ -273,6 +368,22 @@ static cudaError_t launch_mom_t(const MomArgs& a, cudaStream_t st) {
 
 cudaError_t launch_mom(const MomArgs& a, cudaStream_t st) {
   return a.phi ? launch_mom_t<true>(a, st) : launch_mom_t<false>(a, st);
+}
+
+int mom_field_map(CUtensorMap* map, const double* field, int nx, int ny, int nz, bool phi) {
+  EncodeTiledFn enc = tensor_map_encoder();
+  if (!enc) return set_error(MHIT_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+  // x-fastest float64 field; box UPX x UPY (PPX x PPY for phi) x 1 plane.  The row stride nx * 8
+  // bytes is a multiple of 16 (nx is even) and the box rows are 288 bytes.
+  const cuuint64_t dims[3] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz};
+  const cuuint64_t strides[2] = {(cuuint64_t)nx * 8, (cuuint64_t)nx * ny * 8};
+  const cuuint32_t box[3] = {(cuuint32_t)UPX, (cuuint32_t)(phi ? PPY : UPY), 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double*>(field), dims, strides, box, estr,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return set_error(MHIT_ERR_CUDA, "cuTensorMapEncodeTiled failed for a momentum ring map");
+  return MHIT_OK;
 }
 
 }  // namespace mhit

@@ -424,24 +424,6 @@ k_zsolve_tc(const __grid_constant__ CUtensorMap tmap, const uint4* __restrict__ 
 }
 
 // ------------------------------------------------------------------ host side
-using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
-                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
-                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-EncodeTiledFn encode_tiled() {
-  static EncodeTiledFn fn = nullptr;
-  static bool tried = false;
-  if (!tried) {
-    tried = true;
-    void* p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<EncodeTiledFn>(p);
-  }
-  return fn;
-}
-
 // B operand image of one DFT matrix of length L (L = 16: rows 2 k + ro, K = 2 n + ri), three
 // BF16 terms, canonical K-major layout with LBO = 128 and SBO = 128 * (2L / 8)
 void dft_image(int L, unsigned char* out) {
@@ -470,6 +452,20 @@ void dft_image(int L, unsigned char* out) {
 
 }  // namespace
 
+EncodeTiledFn tensor_map_encoder() {
+  static EncodeTiledFn fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
 struct ZsolveTc {
   CUtensorMap tmap;
   void* bimg = nullptr;
@@ -481,7 +477,7 @@ bool zsolve_tc_supported(const Geo& g) { return g.nz == TC_N; }
 int zsolve_tc_create(const Geo& g, void* spec, ZsolveTc** out) {
   *out = nullptr;
   if (!zsolve_tc_supported(g)) return set_error(MHIT_ERR_ARG, "the tensor-core z solve needs nz = 512");
-  EncodeTiledFn enc = encode_tiled();
+  EncodeTiledFn enc = tensor_map_encoder();
   if (!enc) return set_error(MHIT_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
   ZsolveTc* z = new ZsolveTc();
   // the FP32 spectrum as a 3-D float tensor: x = 2 pitch floats, y, z; box 16 floats (8 complex,

@@ -1,5 +1,6 @@
 // Host-side launchers of the timestep kernels (internal to libmhit_b200.so).
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <string>
@@ -13,6 +14,13 @@ int set_error(int code, const std::string& msg);
 int set_cuda_error(cudaError_t e, const char* expr, const char* file, int line);
 
 struct ZsolveTc;  // tensor-core 512-point z solve: tensor map of the spectrum, DFT-matrix image, twiddles
+
+// the driver's cuTensorMapEncodeTiled, reached through the runtime (the library links only cudart);
+// nullptr when the driver does not provide it
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn tensor_map_encoder();
 
 // ---------------------------------------------------------------- Poisson
 enum { PSTAGE_XFWD = 0, PSTAGE_YFWD, PSTAGE_ZSOLVE, PSTAGE_YINV, PSTAGE_XINV, PSTAGE_COUNT };
@@ -74,8 +82,15 @@ struct MomArgs {
   const DevScalars* sc;
   double alpha, beta;
   int zchunk;                // z planes per block (0: default)
+  // TMA tensor maps of u, v, w and phi^{n+1} (mom_field_maps); when `tma` is set the blocks whose
+  // rings need no periodic wrap in x and y fill them with TMA boxes instead of per-thread copies
+  int tma = 0;
+  CUtensorMap tmu, tmv, tmw, tmphi;
 };
 cudaError_t launch_mom(const MomArgs& a, cudaStream_t st);
+// tensor map of an x-fastest nx*ny*nz float64 field with the ring box of k_mom (36 x 10 for the
+// velocity, 36 x 11 for phi)
+int mom_field_map(CUtensorMap* map, const double* field, int nx, int ny, int nz, bool phi);
 
 // ---------------------------------------------------------------- projection + reductions
 struct CorrectArgs {

@@ -90,6 +90,8 @@ struct mhit_ctx {
   int zchunk_phase = 0, zchunk_mom = 0;  // z planes per block of k_phase / k_mom (0: default)
   long long label_bound = 0;              // test hook: union-find loop bound (0: the cell count)
   ZsolveTc* tcz = nullptr;                // tensor-core z solve (zsolve_tc = 1)
+  CUtensorMap tm_u[2], tm_v[2], tm_w[2], tm_phi[2];  // k_mom's ring boxes over U, V, W, PHI[0..1]
+  int mom_tma = 1;                        // k_mom fills its interior rings by TMA (test hook: 0)
   int graph_kernels = 0;                  // kernel nodes in a captured step graph
 };
 
@@ -244,6 +246,11 @@ static int enqueue_stage(mhit_ctx* c, int stage, double alpha, double beta, int 
       a.alpha = alpha;
       a.beta = beta;
       a.zchunk = c->zchunk_mom;
+      a.tma = c->mom_tma;
+      a.tmu = c->tm_u[cur];
+      a.tmv = c->tm_v[cur];
+      a.tmw = c->tm_w[cur];
+      if (p.phiflag) a.tmphi = c->tm_phi[nxt];
       MHIT_CUDA_TRY(launch_mom(a, c->st));
       return MHIT_OK;
     }
@@ -545,6 +552,7 @@ static int init_impl(const mhit_params* p, mhit_ctx* c) {
   const size_t n = (size_t)g.nx * g.ny * g.nz;
   c->n = n;
   const size_t fb = n * sizeof(double);
+  int rc0;
   for (int i = 0; i < 2; ++i) {
     MHIT_CUDA_TRY(cudaMalloc(&c->U[i], fb));
     MHIT_CUDA_TRY(cudaMalloc(&c->V[i], fb));
@@ -556,6 +564,12 @@ static int init_impl(const mhit_params* p, mhit_ctx* c) {
       MHIT_CUDA_TRY(cudaMalloc(&c->PHI[i], fb));
       MHIT_CUDA_TRY(cudaMemset(c->PHI[i], 0, fb));
     }
+  }
+  for (int i = 0; i < 2; ++i) {  // the momentum kernel's TMA boxes over each ping-pong buffer
+    if ((rc0 = mom_field_map(&c->tm_u[i], c->U[i], g.nx, g.ny, g.nz, false))) return rc0;
+    if ((rc0 = mom_field_map(&c->tm_v[i], c->V[i], g.nx, g.ny, g.nz, false))) return rc0;
+    if ((rc0 = mom_field_map(&c->tm_w[i], c->W[i], g.nx, g.ny, g.nz, false))) return rc0;
+    if (p->phiflag && (rc0 = mom_field_map(&c->tm_phi[i], c->PHI[i], g.nx, g.ny, g.nz, true))) return rc0;
   }
   MHIT_CUDA_TRY(cudaMalloc(&c->RU, fb));
   MHIT_CUDA_TRY(cudaMalloc(&c->RV, fb));
@@ -1406,6 +1420,21 @@ int mhit_debug_set_label_bound(mhit_ctx* c, long long bound) {
   if (!c) return set_error(MHIT_ERR_ARG, "null context");
   if (bound < 0) return set_error(MHIT_ERR_ARG, "bound must be >= 0");
   c->label_bound = bound;
+  return MHIT_OK;
+}
+
+int mhit_debug_set_mom_tma(mhit_ctx* c, int on) {
+  int rc;
+  if ((rc = check_ctx(c))) return rc;
+  if (on != 0 && on != 1) return set_error(MHIT_ERR_ARG, "on must be 0 or 1");
+  MHIT_CUDA_TRY(cudaStreamSynchronize(c->st));
+  c->mom_tma = on;
+  for (int i = 0; i < 2; ++i)  // the kernel arguments are baked into the captured graphs
+    if (c->gexec[i]) {
+      cudaGraphExecDestroy(c->gexec[i]);
+      c->gexec[i] = nullptr;
+    }
+  c->graph_built = false;
   return MHIT_OK;
 }
 
