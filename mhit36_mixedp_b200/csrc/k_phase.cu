@@ -26,6 +26,8 @@
 //
 // gamma = 1.0*gumax is read from the device scalars written by the previous projection
 // (:536, :998-1002); u, v, w are the stored fields minus the lazily removed mean.
+#include <type_traits>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -78,7 +80,6 @@ __global__ void __launch_bounds__(PNT, 1) k_phase(PhaseArgs a) {
   double* sph = sps + 2 * PNT;
   double* sfx = sph + 2 * PNT;
   double* sfy = sfx + 2 * PNT;
-  auto slot = [](int m) { return (m & 1) * PNT; };
 
   const Geo& g = a.g;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
@@ -144,10 +145,11 @@ __global__ void __launch_bounds__(PNT, 1) k_phase(PhaseArgs a) {
   double s_0 = 0.0, s_p1 = 0.0, z_m1 = 0.0, z_0 = 0.0;
   int o3 = pmodi(k0 - 1, nz) * plane + col;  // phi(k+3) of the first iteration
 
-  // four planes per unrolled body: 2.58 ms at 512^3 against 2.67 (two), 2.69 (none) and 2.60
-  // (eight, which spills); the same bits for every unroll factor
-#pragma unroll 4
-  for (int k = k0 - 4; k < k1; ++k) {
+  // One plane of the loop; P is the parity of k, so the double-buffer slots are compile-time
+  // offsets: slot(k) = slot(k + 2) = P PNT, slot(k + 1) = (1 - P) PNT.
+  auto plane_iter = [&](auto par, int k) {
+    constexpr int P = decltype(par)::value;
+    constexpr int SK = P * PNT, SK1 = (1 - P) * PNT;
     const bool out = orole && k >= k0;
     const double f_p3 = (k + 1 < k1) ? phig[o3] : 0.0;
     o3 += plane;
@@ -164,21 +166,21 @@ __global__ void __launch_bounds__(PNT, 1) k_phase(PhaseArgs a) {
     }
     // psi(k+2) of this position; phi(k+1) for the next plane's neighbours
     const double s_p2 = psi_of(f_p2);
-    sps[slot(k + 2)] = s_p2;
-    sph[slot(k + 1)] = f_p1;
+    sps[SK] = s_p2;
+    sph[SK1] = f_p1;
     // F(k+1) from the shared psi(k+1) (written last iteration) and the own psi(k+2) - psi(k)
     double z_p1 = 0.0;
     if (frole && k >= k0 - 2) {
       double fx, fy;
-      F_of(sps + slot(k + 1), s_p2 - s_0, f_p1, s_p1, fx, fy, z_p1);
-      sfx[slot(k + 1)] = fx;
-      sfy[slot(k + 1)] = fy;
+      F_of(sps + SK1, s_p2 - s_0, f_p1, s_p1, fx, fy, z_p1);
+      sfx[SK1] = fx;
+      sfy[SK1] = fy;
     }
     // output plane k from the shared phi(k), Fx/Fy(k) and the own column
     if (out) {
       const double u_0 = u0 - mu_, u_x = uxp - mu_, v_0 = v0 - mv_, v_y = vyp - mv_;
       const double w_0 = w0 - mw_, w_z = wzp - mw_;
-      const double* P0 = sph + slot(k);
+      const double* P0 = sph + SK;
       const double p0 = f_0;
       const double pxp = P0[1], pxm = P0[-1], pyp = P0[PHX], pym = P0[-PHX];
       const double pzp = f_p1, pzm = f_m1;
@@ -188,8 +190,8 @@ __global__ void __launch_bounds__(PNT, 1) k_phase(PhaseArgs a) {
       //   rhs = -dxi/2 sum_d (u_d+ (phi+ + phi) - u_d (phi + phi-))                 advection
       //         + gamma eps ddxi (sum of the six neighbours - 6 phi)                diffusion
       //         - gamma dxi/2 sum_d (F_d+ - F_d-)                                   sharpening
-      const double* Fx = sfx + slot(k);
-      const double* Fy = sfy + slot(k);
+      const double* Fx = sfx + SK;
+      const double* Fy = sfy + SK;
       const double adv = (__fma_rn(u_x, pxp + p0, -u_0 * (p0 + pxm)) + __fma_rn(v_y, pyp + p0, -v_0 * (p0 + pym))) +
                          __fma_rn(w_z, pzp + p0, -w_0 * (p0 + pzm));
       const double lap = ((pxp + pxm) + (pyp + pym)) + __fma_rn(-6.0, p0, pzp + pzm);
@@ -210,6 +212,15 @@ __global__ void __launch_bounds__(PNT, 1) k_phase(PhaseArgs a) {
     s_p1 = s_p2;
     z_m1 = z_0;
     z_0 = z_p1;
+  };
+  // k0 and the chunk are even (launch_phase), so k0 - 4 is even and the trip count too; two
+  // planes per iteration, four per unrolled body (2.58 ms at 512^3 with runtime slots, against
+  // 2.67 for two, 2.69 for one and 2.60 for eight planes, where it spills); the same bits for
+  // every unroll factor
+#pragma unroll 2
+  for (int k = k0 - 4; k < k1; k += 2) {
+    plane_iter(std::integral_constant<int, 0>{}, k);
+    plane_iter(std::integral_constant<int, 1>{}, k + 1);
   }
 }
 
@@ -235,6 +246,7 @@ cudaError_t launch_phase(const PhaseArgs& a, cudaStream_t st) {
     b.zchunk = cols * ((a.g.nz + 127) / 128) >= 8 * 148 ? 128 : PZC;
   }
   const int zc = b.zchunk;
+  if (zc % 2 || a.g.nz % 2) return cudaErrorInvalidValue;  // the plane loop runs two planes at a time
   dim3 grd((a.g.nx + PTX - 1) / PTX, (a.g.ny + PTY - 1) / PTY, (a.g.nz + zc - 1) / zc);
   kern<<<grd, PNT, smem, st>>>(b);
   return cudaGetLastError();

@@ -55,8 +55,9 @@ k_div_fftx(const double* __restrict__ u, const double* __restrict__ v, const dou
 
   // Element e of the tile: line e / M, complex point e % M.  The FP64 256-point tile (nx = 512)
   // loads in a loop of compile-time length unrolled twice (88 registers, twelve loads in flight
-  // per thread): 0.85 ms at 512^3 against 1.00 ms for the strided loop; the FP32 tile keeps the
-  // strided loop (0.707 against 0.715 ms), and so do the other lengths (not measured).
+  // per thread): 0.85 ms at 512^3 against 1.00 ms for the strided loop; so does the FP32 tile
+  // of the residual source (its 13 loads per pair); the FP32 divergence tile keeps the strided
+  // loop (0.707 against 0.715 ms), and so do the other lengths (not measured).
   auto load = [&](int e) {
     const int b = e / M, n = e - b * M;
     const int line = min(line0 + b, nlines - 1);  // a tail tile repeats the last line
@@ -113,7 +114,7 @@ k_div_fftx(const double* __restrict__ u, const double* __restrict__ v, const dou
     }
     s[sw<B>(n, b)] = z;
   };
-  if constexpr (sizeof(T) == 8 && M == 256 && (M * B) % NT == 0) {
+  if constexpr ((sizeof(T) == 8 || SRC == 3) && M == 256 && (M * B) % NT == 0) {
 #pragma unroll 2
     for (int it = 0; it < M * B / NT; ++it) load(threadIdx.x + it * NT);
   } else {
