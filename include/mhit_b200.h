@@ -235,9 +235,15 @@ int mhit_kernels_per_step(mhit_ctx* ctx, int* n);
  * the boxes advance together: mhit_ensemble_step runs each step after the first as ONE CUDA
  * graph launch whose graph forks the boxes' step sequences onto concurrent streams ("lanes")
  * and joins them.  All boxes must be at the same step (upload all, then step all).
+ * In the batched schedule (the default when every box has the same phiflag and acdi_clamp) the
+ * phase and momentum stages of all boxes run as one persistent launch each, whose blocks take
+ * (box, tile, z chunk) items from a device work queue; the Poisson passes and the projection of
+ * each box follow on the lanes.  Both schedules give the same bits.
  * mhit_ensemble_autotune times the z-chunk of the phase and momentum kernels per box size and
- * the number of lanes, keeps the fastest, and leaves every box zeroed: call it before the
- * uploads.  mhit_ensemble_tuning reports the choices (arrays of nbox ints, may be NULL). */
+ * the number of lanes, then the batched schedule with uniform z chunks, keeps the fastest, and
+ * leaves every box zeroed: call it before the uploads.  mhit_ensemble_tuning reports the choices
+ * (arrays of nbox ints, may be NULL); mhit_ensemble_batched reports the schedule and
+ * mhit_ensemble_set_batched chooses it (1: batched, 0: per-box lanes). */
 typedef struct mhit_ensemble mhit_ensemble;
 int mhit_ensemble_create(const mhit_params* params, int nbox, mhit_ensemble** out);
 void mhit_ensemble_destroy(mhit_ensemble* e);
@@ -246,6 +252,8 @@ int mhit_ensemble_step(mhit_ensemble* e, int nsteps);
 int mhit_ensemble_time_steps(mhit_ensemble* e, int nsteps, double* ms);
 int mhit_ensemble_autotune(mhit_ensemble* e, int trials, int* nlanes);
 int mhit_ensemble_tuning(mhit_ensemble* e, int* nlanes, int* zchunk_phase, int* zchunk_mom);
+int mhit_ensemble_batched(mhit_ensemble* e, int* on);
+int mhit_ensemble_set_batched(mhit_ensemble* e, int on);
 
 /* Test hooks (no reference counterpart): run one stage of the step pipeline on the current
  * buffers, read an internal buffer widened to float64, and commit the staged step.  They let

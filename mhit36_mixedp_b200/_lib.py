@@ -95,6 +95,8 @@ SIGNATURES = {
     "mhit_ensemble_time_steps": (_c.c_int, [_c.c_void_p, _c.c_int, _dp]),
     "mhit_ensemble_autotune": (_c.c_int, [_c.c_void_p, _c.c_int, _P(_c.c_int)]),
     "mhit_ensemble_tuning": (_c.c_int, [_c.c_void_p, _P(_c.c_int), _P(_c.c_int), _P(_c.c_int)]),
+    "mhit_ensemble_batched": (_c.c_int, [_c.c_void_p, _P(_c.c_int)]),
+    "mhit_ensemble_set_batched": (_c.c_int, [_c.c_void_p, _c.c_int]),
     "mhit_field_stats_noalloc": (_c.c_int, [_c.c_int, _c.c_int, _c.c_int, _c.c_double, _c.c_void_p, _c.c_void_p,
                                             _c.c_void_p, _c.c_void_p, _c.c_void_p]),
     "mhit_debug_run_stage": (_c.c_int, [_c.c_void_p, _c.c_int]),

@@ -426,7 +426,14 @@ class Ensemble:
         zp = (ctypes.c_int * nb)()
         zm = (ctypes.c_int * nb)()
         _check(self._lib.mhit_ensemble_tuning(self._e, ctypes.byref(lanes), zp, zm))
-        return {"lanes": lanes.value, "zchunk_phase": list(zp), "zchunk_mom": list(zm)}
+        on = ctypes.c_int()
+        _check(self._lib.mhit_ensemble_batched(self._e, ctypes.byref(on)))
+        return {"lanes": lanes.value, "zchunk_phase": list(zp), "zchunk_mom": list(zm), "batched": bool(on.value)}
+
+    def set_batched(self, on: bool):
+        """Batched schedule (phase and momentum of all boxes as one persistent launch each) or
+        per-box lanes."""
+        _check(self._lib.mhit_ensemble_set_batched(self._e, int(bool(on))))
 
 
 def abi_version() -> int:

@@ -96,16 +96,18 @@ __device__ __forceinline__ int pmod_int(int x, int n) {
   return x < 0 ? x + n : x;
 }
 
+// One z column of MTX x MTY cells, tile (bx, by), chunk bz, of the box a, with the step's
+// alpha, beta (AB2 weights).
 template <bool PHI>
-__global__ void __launch_bounds__(MNT, 3) k_mom(const __grid_constant__ MomArgs a) {
-  extern __shared__ __align__(128) unsigned char smraw[];
+__device__ __forceinline__ void mom_tile(const MomArgs& a, double alpha, double beta, int bx, int by, int bz,
+                                         unsigned char* smraw) {
   MomSmem<PHI>& S = *reinterpret_cast<MomSmem<PHI>*>(smraw);
   const Geo& g = a.g;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const size_t plane = (size_t)nx * ny;
-  const int i0 = blockIdx.x * MTX, j0 = blockIdx.y * MTY;
+  const int i0 = bx * MTX, j0 = by * MTY;
   const int zc = a.zchunk > 0 ? a.zchunk : MZC;
-  const int k0 = blockIdx.z * zc;
+  const int k0 = bz * zc;
   const int k1 = min(k0 + zc, nz);
   const int tid = threadIdx.x;
 
@@ -230,7 +232,7 @@ __global__ void __launch_bounds__(MNT, 3) k_mom(const __grid_constant__ MomArgs 
   const double c_adv = -0.25 * dxi;                    // -(h11 + h12 + h13) / 4 dxi
   const double c_vis = g.mu * ddxi * g.rhoi;           // mu lap(u) / rho
   const double c_st = 6.0 * g.sigma * 0.25 * dxi * g.rhoi;  // face average of the force / rho
-  const double dta = g.dt * a.alpha, dtb = g.dt * a.beta;
+  const double dta = g.dt * alpha, dtb = g.dt * beta;
   const int uq = (ty + 1) * UPX + (tx + 2);   // own cell in the u/v/w plane
   const int pq = (ty + 2) * PPX + (tx + 2);   // own cell in the phi plane
   const int cq = (ty + 1) * CPX + (tx + 1);   // own cell in the chempot plane
@@ -343,6 +345,55 @@ __global__ void __launch_bounds__(MNT, 3) k_mom(const __grid_constant__ MomArgs 
 }
 
 template <bool PHI>
+__global__ void __launch_bounds__(MNT, 3) k_mom(const __grid_constant__ MomArgs a) {
+  extern __shared__ __align__(128) unsigned char smraw[];
+  mom_tile<PHI>(a, a.alpha, a.beta, blockIdx.x, blockIdx.y, blockIdx.z, smraw);
+}
+
+// The momentum step of many boxes in one launch: persistent blocks (three per SM) take work items
+// (box, tile x, tile y, z chunk) from a device queue until it is empty.  The boxes' arguments live
+// in device memory, so their rings are filled by per-thread copies (no TMA).
+template <bool PHI>
+__global__ void __launch_bounds__(MNT, 3) k_mom_batch(const __grid_constant__ BatchArgs<MomArgs> b) {
+  extern __shared__ __align__(128) unsigned char smraw[];
+  __shared__ int s_item;
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(b.counter, 1);
+    __syncthreads();
+    const int it = s_item;
+    __syncthreads();  // every thread has the item before thread 0 takes the next one
+    if (it >= b.nitems) break;
+    const int4 w = b.items[it];
+    mom_tile<PHI>(b.args[w.x], b.alpha, b.beta, w.y, w.z, w.w, smraw);
+    __syncthreads();  // the rings are reused by the next item
+  }
+}
+
+int mom_zchunk(const Geo& g, int requested) {
+  // Default chunk: 64 planes where that still leaves eight waves of three blocks on each of the
+  // 148 SMs (2.896 against 2.928 ms at 512^3), otherwise MZC.  Results do not depend on it.
+  if (requested > 0) return requested;
+  const long long cols = (long long)((g.nx + MTX - 1) / MTX) * ((g.ny + MTY - 1) / MTY);
+  return cols * ((g.nz + 63) / 64) >= 8 * 148 * 3 ? 64 : MZC;
+}
+
+dim3 mom_grid(const Geo& g, int zc) {
+  return dim3((g.nx + MTX - 1) / MTX, (g.ny + MTY - 1) / MTY, (g.nz + zc - 1) / zc);
+}
+
+cudaError_t launch_mom_batch(const BatchArgs<MomArgs>& b, bool phi, int nsm, cudaStream_t st) {
+  const size_t smem = phi ? sizeof(MomSmem<true>) : sizeof(MomSmem<false>);
+  auto kern = phi ? k_mom_batch<true> : k_mom_batch<false>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(b.counter, 0, sizeof(int), st);
+  if (e != cudaSuccess) return e;
+  const int grid = b.nitems < 3 * nsm ? b.nitems : 3 * nsm;
+  kern<<<grid, MNT, smem, st>>>(b);
+  return cudaGetLastError();
+}
+
+template <bool PHI>
 static cudaError_t launch_mom_t(const MomArgs& a, cudaStream_t st) {
   const size_t smem = sizeof(MomSmem<PHI>);
   static int attr_set[64] = {0};
@@ -353,16 +404,9 @@ static cudaError_t launch_mom_t(const MomArgs& a, cudaStream_t st) {
     if (e != cudaSuccess) return e;
     attr_set[dev] = 1;
   }
-  // Default chunk: 64 planes where that still leaves eight waves of three blocks on each of the
-  // 148 SMs (2.896 against 2.928 ms at 512^3), otherwise MZC.  Results do not depend on it.
   MomArgs b = a;
-  if (b.zchunk <= 0) {
-    const long long cols = (long long)((a.g.nx + MTX - 1) / MTX) * ((a.g.ny + MTY - 1) / MTY);
-    b.zchunk = cols * ((a.g.nz + 63) / 64) >= 8 * 148 * 3 ? 64 : MZC;
-  }
-  const int zc = b.zchunk;
-  dim3 grd((a.g.nx + MTX - 1) / MTX, (a.g.ny + MTY - 1) / MTY, (a.g.nz + zc - 1) / zc);
-  k_mom<PHI><<<grd, MNT, smem, st>>>(b);
+  b.zchunk = mom_zchunk(a.g, a.zchunk);
+  k_mom<PHI><<<mom_grid(a.g, b.zchunk), MNT, smem, st>>>(b);
   return cudaGetLastError();
 }
 

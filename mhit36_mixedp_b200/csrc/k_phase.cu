@@ -60,9 +60,11 @@ __device__ __forceinline__ void ring_pos(int r, int x0, int y0, int w, int h, in
   y = y0 + 1 + r;
 }
 
+// One z column of PTX x PTY cells, tile (bx, by), chunk bz, of the box a; dta, dtb = dt alpha,
+// dt beta of the AB2 update.
 template <bool CLAMP>
-__global__ void __launch_bounds__(PNT, 1) k_phase(PhaseArgs a) {
-  extern __shared__ __align__(16) unsigned char smraw[];
+__device__ __forceinline__ void phase_tile(const PhaseArgs& a, double dta, double dtb, int bx, int by, int bz,
+                                           unsigned char* smraw) {
   // thread -> position (hx, hy) in the (PHX x PHY) grid of the tile with its halo
   const int tid = threadIdx.x;
   int hx, hy;
@@ -84,9 +86,9 @@ __global__ void __launch_bounds__(PNT, 1) k_phase(PhaseArgs a) {
   const Geo& g = a.g;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const int plane = nx * ny, ntot = plane * nz;
-  const int i0 = blockIdx.x * PTX, j0 = blockIdx.y * PTY;
+  const int i0 = bx * PTX, j0 = by * PTY;
   const int zc = a.zchunk > 0 ? a.zchunk : PZC;
-  const int k0 = blockIdx.z * zc, k1 = min(k0 + zc, nz);
+  const int k0 = bz * zc, k1 = min(k0 + zc, nz);
   const int i = i0 - 2 + hx, j = j0 - 2 + hy;
   const int col = pmodi(j, ny) * nx + pmodi(i, nx);
   const bool frole = tid < PNF;
@@ -198,7 +200,7 @@ __global__ void __launch_bounds__(PNT, 1) k_phase(PhaseArgs a) {
       const double shp = ((Fx[1] - Fx[-1]) + (Fy[PHX] - Fy[-PHX])) + (z_p1 - z_m1);
       const double rhs = __fma_rn(-hdxi, adv, __fma_rn(c_lap, lap, c_shp * shp));
       // :625-626
-      a.phin[c] = __fma_rn(a.dta, rhs, __fma_rn(-a.dtb, ro, p0));
+      a.phin[c] = __fma_rn(dta, rhs, __fma_rn(-dtb, ro, p0));
       a.rphio[c] = rhs;
       w0 = wzp;
       c += plane;
@@ -224,6 +226,56 @@ __global__ void __launch_bounds__(PNT, 1) k_phase(PhaseArgs a) {
   }
 }
 
+template <bool CLAMP>
+__global__ void __launch_bounds__(PNT, 1) k_phase(const __grid_constant__ PhaseArgs a) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  phase_tile<CLAMP>(a, a.dta, a.dtb, blockIdx.x, blockIdx.y, blockIdx.z, smraw);
+}
+
+// The phase step of many boxes in one launch: persistent blocks (one per SM) take work items
+// (box, tile x, tile y, z chunk) from a device queue until it is empty.  A box's arguments
+// (including its resolved z chunk) come from b.args; alpha, beta are the step's.  The boxes of
+// one launch share the psi clamp (CLAMP).
+template <bool CLAMP>
+__global__ void __launch_bounds__(PNT, 1) k_phase_batch(const __grid_constant__ BatchArgs<PhaseArgs> b) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  __shared__ int s_item;
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(b.counter, 1);
+    __syncthreads();
+    const int it = s_item;
+    __syncthreads();  // every thread has the item before thread 0 takes the next one
+    if (it >= b.nitems) break;
+    const int4 w = b.items[it];
+    const PhaseArgs& a = b.args[w.x];
+    phase_tile<CLAMP>(a, a.g.dt * b.alpha, a.g.dt * b.beta, w.y, w.z, w.w, smraw);
+  }
+}
+
+int phase_zchunk(const Geo& g, int requested) {
+  // Default chunk: 128 planes where that still leaves eight waves of one block on each of the
+  // 148 SMs (the four planes of warm-up below a chunk cost 3% instead of 6%: 2.667 against
+  // 2.723 ms at 512^3), otherwise PZC.  Results do not depend on the chunk.
+  if (requested > 0) return requested;
+  const long long cols = (long long)((g.nx + PTX - 1) / PTX) * ((g.ny + PTY - 1) / PTY);
+  return cols * ((g.nz + 127) / 128) >= 8 * 148 ? 128 : PZC;
+}
+
+dim3 phase_grid(const Geo& g, int zc) {
+  return dim3((g.nx + PTX - 1) / PTX, (g.ny + PTY - 1) / PTY, (g.nz + zc - 1) / zc);
+}
+
+cudaError_t launch_phase_batch(const BatchArgs<PhaseArgs>& b, bool clamp, int nsm, cudaStream_t st) {
+  constexpr size_t smem = 8 * sizeof(double) * PNT;
+  auto kern = clamp ? k_phase_batch<true> : k_phase_batch<false>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(b.counter, 0, sizeof(int), st);
+  if (e != cudaSuccess) return e;
+  kern<<<b.nitems < nsm ? b.nitems : nsm, PNT, smem, st>>>(b);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_phase(const PhaseArgs& a, cudaStream_t st) {
   constexpr size_t smem = 8 * sizeof(double) * PNT;  // psi, phi, Fx, Fy: two planes each
   auto kern = a.clamp ? k_phase<true> : k_phase<false>;
@@ -235,20 +287,13 @@ cudaError_t launch_phase(const PhaseArgs& a, cudaStream_t st) {
     if (e != cudaSuccess) return e;
     if (dev < 64) attr_set[dev][a.clamp ? 1 : 0] = 1;
   }
-  // Default chunk: 128 planes where that still leaves eight waves of one block on each of the
-  // 148 SMs (the four planes of warm-up below a chunk cost 3% instead of 6%: 2.667 against
-  // 2.723 ms at 512^3), otherwise PZC.  Results do not depend on the chunk.
   PhaseArgs b = a;
   b.dta = a.g.dt * a.alpha;
   b.dtb = a.g.dt * a.beta;
-  if (b.zchunk <= 0) {
-    const long long cols = (long long)((a.g.nx + PTX - 1) / PTX) * ((a.g.ny + PTY - 1) / PTY);
-    b.zchunk = cols * ((a.g.nz + 127) / 128) >= 8 * 148 ? 128 : PZC;
-  }
+  b.zchunk = phase_zchunk(a.g, a.zchunk);
   const int zc = b.zchunk;
   if (zc % 2 || a.g.nz % 2) return cudaErrorInvalidValue;  // the plane loop runs two planes at a time
-  dim3 grd((a.g.nx + PTX - 1) / PTX, (a.g.ny + PTY - 1) / PTY, (a.g.nz + zc - 1) / zc);
-  kern<<<grd, PNT, smem, st>>>(b);
+  kern<<<phase_grid(a.g, zc), PNT, smem, st>>>(b);
   return cudaGetLastError();
 }
 

@@ -71,6 +71,20 @@ struct PhaseArgs {
 };
 cudaError_t launch_phase(const PhaseArgs& a, cudaStream_t st);
 
+// A stage of many boxes in one launch: persistent blocks take work items (box, tile x, tile y,
+// z chunk) from a device queue (counter, reset by the launcher) and run the box's tile with
+// args[box] (device memory) and the step's alpha, beta.
+template <typename A> struct BatchArgs {
+  const A* args;
+  const int4* items;
+  int nitems;
+  int* counter;
+  double alpha, beta;
+};
+int phase_zchunk(const Geo& g, int requested);  // the z chunk launch_phase uses
+dim3 phase_grid(const Geo& g, int zc);           // its tiles: x, y, z chunk
+cudaError_t launch_phase_batch(const BatchArgs<PhaseArgs>& b, bool clamp, int nsm, cudaStream_t st);
+
 // ---------------------------------------------------------------- momentum
 struct MomArgs {
   Geo g;
@@ -88,6 +102,9 @@ struct MomArgs {
   CUtensorMap tmu, tmv, tmw, tmphi;
 };
 cudaError_t launch_mom(const MomArgs& a, cudaStream_t st);
+int mom_zchunk(const Geo& g, int requested);  // the z chunk launch_mom uses
+dim3 mom_grid(const Geo& g, int zc);           // its tiles: x, y, z chunk
+cudaError_t launch_mom_batch(const BatchArgs<MomArgs>& b, bool phi, int nsm, cudaStream_t st);
 // tensor map of an x-fastest nx*ny*nz float64 field with the ring box of k_mom (36 x 10 for the
 // velocity, 36 x 11 for phi)
 int mom_field_map(CUtensorMap* map, const double* field, int nx, int ny, int nz, bool phi);

@@ -187,6 +187,52 @@ static bool stage_runs(const mhit_ctx* c, int stage) {
   return true;
 }
 
+// Arguments of the phase and momentum stages of a step that reads buffer set `cur`.
+static PhaseArgs phase_args(const mhit_ctx* c, double alpha, double beta, int cur) {
+  const int nxt = cur ^ 1;
+  PhaseArgs a;
+  a.g = c->g;
+  a.phi = c->PHI[cur];
+  a.u = c->U[cur];
+  a.v = c->V[cur];
+  a.w = c->W[cur];
+  a.phin = c->PHI[nxt];
+  a.rphio = c->RPHI;
+  a.sc = c->sc;
+  a.alpha = alpha;
+  a.beta = beta;
+  a.clamp = c->prm.acdi_clamp;
+  a.zchunk = c->zchunk_phase;
+  return a;
+}
+
+static MomArgs mom_args(const mhit_ctx* c, double alpha, double beta, int cur) {
+  const int nxt = cur ^ 1;
+  MomArgs a;
+  a.g = c->g;
+  a.u = c->U[cur];
+  a.v = c->V[cur];
+  a.w = c->W[cur];
+  a.un = c->U[nxt];
+  a.vn = c->V[nxt];
+  a.wn = c->W[nxt];
+  a.ru = c->RU;
+  a.rv = c->RV;
+  a.rw = c->RW;
+  a.phi = c->prm.phiflag ? c->PHI[nxt] : nullptr;
+  a.tabs = c->tabs;
+  a.sc = c->sc;
+  a.alpha = alpha;
+  a.beta = beta;
+  a.zchunk = c->zchunk_mom;
+  a.tma = c->mom_tma;
+  a.tmu = c->tm_u[cur];
+  a.tmv = c->tm_v[cur];
+  a.tmw = c->tm_w[cur];
+  if (c->prm.phiflag) a.tmphi = c->tm_phi[nxt];
+  return a;
+}
+
 // Launch one stage of the step that reads buffer set `cur` and writes set `cur ^ 1`.
 static int enqueue_stage(mhit_ctx* c, int stage, double alpha, double beta, int cur) {
   const int nxt = cur ^ 1;
@@ -212,46 +258,11 @@ static int enqueue_stage(mhit_ctx* c, int stage, double alpha, double beta, int 
       return MHIT_OK;
     }
     case ST_PHASE: {
-      PhaseArgs a;
-      a.g = c->g;
-      a.phi = c->PHI[cur];
-      a.u = c->U[cur];
-      a.v = c->V[cur];
-      a.w = c->W[cur];
-      a.phin = c->PHI[nxt];
-      a.rphio = c->RPHI;
-      a.sc = c->sc;
-      a.alpha = alpha;
-      a.beta = beta;
-      a.clamp = p.acdi_clamp;
-      a.zchunk = c->zchunk_phase;
-      MHIT_CUDA_TRY(launch_phase(a, c->st));
+      MHIT_CUDA_TRY(launch_phase(phase_args(c, alpha, beta, cur), c->st));
       return MHIT_OK;
     }
     case ST_MOM: {
-      MomArgs a;
-      a.g = c->g;
-      a.u = c->U[cur];
-      a.v = c->V[cur];
-      a.w = c->W[cur];
-      a.un = c->U[nxt];
-      a.vn = c->V[nxt];
-      a.wn = c->W[nxt];
-      a.ru = c->RU;
-      a.rv = c->RV;
-      a.rw = c->RW;
-      a.phi = p.phiflag ? c->PHI[nxt] : nullptr;
-      a.tabs = c->tabs;
-      a.sc = c->sc;
-      a.alpha = alpha;
-      a.beta = beta;
-      a.zchunk = c->zchunk_mom;
-      a.tma = c->mom_tma;
-      a.tmu = c->tm_u[cur];
-      a.tmv = c->tm_v[cur];
-      a.tmw = c->tm_w[cur];
-      if (p.phiflag) a.tmphi = c->tm_phi[nxt];
-      MHIT_CUDA_TRY(launch_mom(a, c->st));
+      MHIT_CUDA_TRY(launch_mom(mom_args(c, alpha, beta, cur), c->st));
       return MHIT_OK;
     }
     case ST_XFWD:
@@ -1510,7 +1521,93 @@ struct mhit_ensemble {
   bool built = false;
   std::vector<unsigned> gen;  // the boxes' graph generations the ensemble graphs were built from
   cudaEvent_t ev[2] = {nullptr, nullptr};
+  // batched schedule: the phase and momentum stages of all boxes as one persistent launch each
+  // (device work queues of (box, tile x, tile y, z chunk) items), the Poisson passes and the
+  // projection per box on the lanes
+  bool batched = false;
+  bool batch_ready = false;   // device argument arrays and item lists match the boxes' tuning
+  int nsm = 148;
+  PhaseArgs* d_pargs[2] = {nullptr, nullptr};  // per parity of the ping-pong buffers
+  MomArgs* d_margs[2] = {nullptr, nullptr};
+  int4* d_pitems = nullptr;
+  int4* d_mitems = nullptr;
+  int npitems = 0, nmitems = 0;
+  int* d_counters = nullptr;  // the two queues' counters
 };
+
+// The batched schedule needs one phase variant (all boxes with the phase field share the psi
+// clamp) and one momentum variant (all boxes with or all without the phase field).
+static bool ens_batchable(const mhit_ensemble* e) {
+  for (const mhit_ctx* c : e->box)
+    if (c->prm.phiflag != e->box[0]->prm.phiflag || c->prm.acdi_clamp != e->box[0]->prm.acdi_clamp) return false;
+  return true;
+}
+
+static void ens_free_batch(mhit_ensemble* e) {
+  for (int i = 0; i < 2; ++i) {
+    cudaFree(e->d_pargs[i]);
+    cudaFree(e->d_margs[i]);
+    e->d_pargs[i] = nullptr;
+    e->d_margs[i] = nullptr;
+  }
+  cudaFree(e->d_pitems);
+  cudaFree(e->d_mitems);
+  cudaFree(e->d_counters);
+  e->d_pitems = e->d_mitems = nullptr;
+  e->d_counters = nullptr;
+  e->batch_ready = false;
+}
+
+// Device copies of every box's phase and momentum arguments (both parities; the step's alpha,
+// beta come with the launch) and the work items, largest boxes first so that the queue ends on
+// small items.
+static int ens_prepare_batch(mhit_ensemble* e) {
+  if (e->batch_ready) return MHIT_OK;
+  ens_free_batch(e);
+  std::vector<int> order(e->nbox);
+  for (int b = 0; b < e->nbox; ++b) order[b] = b;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return e->box[x]->n > e->box[y]->n; });
+  std::vector<int4> pit, mit;
+  std::vector<PhaseArgs> pa[2];
+  std::vector<MomArgs> ma[2];
+  for (int b = 0; b < e->nbox; ++b) {
+    mhit_ctx* c = e->box[b];
+    for (int par = 0; par < 2; ++par) {
+      PhaseArgs p = phase_args(c, 1.0, 0.0, par);
+      p.zchunk = phase_zchunk(c->g, c->zchunk_phase);
+      pa[par].push_back(p);
+      MomArgs m = mom_args(c, 1.0, 0.0, par);
+      m.zchunk = mom_zchunk(c->g, c->zchunk_mom);
+      m.tma = 0;  // the tensor maps would be read from device memory: per-thread ring copies
+      ma[par].push_back(m);
+    }
+  }
+  for (int b : order) {
+    const mhit_ctx* c = e->box[b];
+    if (c->prm.phiflag) {
+      const dim3 gp = phase_grid(c->g, pa[0][b].zchunk);
+      for (unsigned z = 0; z < gp.z; ++z)
+        for (unsigned y = 0; y < gp.y; ++y)
+          for (unsigned x = 0; x < gp.x; ++x) pit.push_back(make_int4(b, (int)x, (int)y, (int)z));
+    }
+    const dim3 gm = mom_grid(c->g, ma[0][b].zchunk);
+    for (unsigned z = 0; z < gm.z; ++z)
+      for (unsigned y = 0; y < gm.y; ++y)
+        for (unsigned x = 0; x < gm.x; ++x) mit.push_back(make_int4(b, (int)x, (int)y, (int)z));
+  }
+  int rc;
+  for (int par = 0; par < 2; ++par) {
+    if ((rc = upload_vec((void**)&e->d_pargs[par], pa[par]))) return rc;
+    if ((rc = upload_vec((void**)&e->d_margs[par], ma[par]))) return rc;
+  }
+  if (!pit.empty() && (rc = upload_vec((void**)&e->d_pitems, pit))) return rc;
+  if ((rc = upload_vec((void**)&e->d_mitems, mit))) return rc;
+  MHIT_CUDA_TRY(cudaMalloc(&e->d_counters, 2 * sizeof(int)));
+  e->npitems = (int)pit.size();
+  e->nmitems = (int)mit.size();
+  e->batch_ready = true;
+  return MHIT_OK;
+}
 
 static void ens_drop_graphs(mhit_ensemble* e) {
   for (int i = 0; i < 2; ++i)
@@ -1519,6 +1616,7 @@ static void ens_drop_graphs(mhit_ensemble* e) {
       e->gexec[i] = nullptr;
     }
   e->built = false;
+  e->batch_ready = false;  // z chunks or buffers may have changed
 }
 
 static int ens_set_lanes(mhit_ensemble* e, int nlanes) {
@@ -1538,15 +1636,38 @@ static int ens_set_lanes(mhit_ensemble* e, int nlanes) {
   return MHIT_OK;
 }
 
-// One ensemble step on e->st (captured or eager): fork, per-box sequences on lanes, join.
+// One ensemble step on e->st (captured or eager): fork, per-box sequences on lanes, join.  In the
+// batched schedule the tracer, phase and momentum stages of all boxes run first on e->st (the
+// phase and momentum stages as one persistent launch each), then the per-box Poisson passes and
+// projections fork onto the lanes.
 static int ens_enqueue(mhit_ensemble* e, double alpha, double beta, int cur) {
+  int first = 0;
+  if (e->batched) {
+    int rc;
+    if ((rc = ens_prepare_batch(e))) return rc;
+    for (mhit_ctx* c : e->box) {
+      cudaStream_t saved = c->st;
+      c->st = e->st;
+      rc = enqueue_stage(c, ST_TRACER, alpha, beta, cur);
+      c->st = saved;
+      if (rc) return rc;
+    }
+    if (e->npitems) {
+      BatchArgs<PhaseArgs> pb{e->d_pargs[cur], e->d_pitems, e->npitems, e->d_counters, alpha, beta};
+      MHIT_CUDA_TRY(launch_phase_batch(pb, e->box[0]->prm.acdi_clamp != 0, e->nsm, e->st));
+    }
+    BatchArgs<MomArgs> mb{e->d_margs[cur], e->d_mitems, e->nmitems, e->d_counters + 1, alpha, beta};
+    MHIT_CUDA_TRY(launch_mom_batch(mb, e->box[0]->prm.phiflag != 0, e->nsm, e->st));
+    first = ST_XFWD;
+  }
   MHIT_CUDA_TRY(cudaEventRecord(e->fork, e->st));
   for (int l = 0; l < e->nlanes; ++l) MHIT_CUDA_TRY(cudaStreamWaitEvent(e->lanes[l], e->fork, 0));
   for (int b = 0; b < e->nbox; ++b) {
     mhit_ctx* c = e->box[b];
     cudaStream_t saved = c->st;
     c->st = e->lanes[b % e->nlanes];
-    int rc = enqueue_step(c, alpha, beta, cur, false);
+    int rc = MHIT_OK;
+    for (int s = first; s < ST_COUNT && rc == MHIT_OK; ++s) rc = enqueue_stage(c, s, alpha, beta, cur);
     c->st = saved;
     if (rc) return rc;
   }
@@ -1651,6 +1772,10 @@ int mhit_ensemble_create(const mhit_params* params, int nbox, mhit_ensemble** ou
     if (err != cudaSuccess) rc = set_cuda_error(err, "ensemble stream/events", __FILE__, __LINE__);
   }
   if (rc == MHIT_OK) rc = ens_set_lanes(e, nbox);
+  if (rc == MHIT_OK) {
+    cudaDeviceGetAttribute(&e->nsm, cudaDevAttrMultiProcessorCount, e->dev);
+    e->batched = ens_batchable(e);  // the autotuner may switch back to per-box lanes
+  }
   if (rc) {
     std::string keep = g_err;
     mhit_ensemble_destroy(e);
@@ -1672,6 +1797,7 @@ void mhit_ensemble_destroy(mhit_ensemble* e) {
   for (int i = 0; i < 2; ++i)
     if (e->ev[i]) cudaEventDestroy(e->ev[i]);
   if (e->st) cudaStreamDestroy(e->st);
+  ens_free_batch(e);
   for (mhit_ctx* c : e->box) mhit_destroy(c);
   delete e;
 }
@@ -1710,8 +1836,10 @@ int mhit_ensemble_time_steps(mhit_ensemble* e, int nsteps, double* ms) {
 // Autotuner: for every class of equal boxes (grid, phase field on/off) time the z-chunk of
 // k_phase and k_mom over {8, 16, 32, 64} on the first box of the class (one profiled step per
 // candidate, best of `trials`), then time whole ensemble steps for 1, 2, 4, 8, ... lanes and
-// keep the fastest.  The timing steps run on zeroed fields and are thrown away: every box is
-// left zeroed with an empty history, so call this before uploading the initial fields.
+// keep the fastest; then time the batched schedule with uniform z chunks of 32, 64 and 128
+// planes on those lanes and keep it if it is faster.  The timing steps run on zeroed fields and
+// are thrown away: every box is left zeroed with an empty history, so call this before
+// uploading the initial fields.
 int mhit_ensemble_autotune(mhit_ensemble* e, int trials, int* nlanes_out) {
   if (!e) return set_error(MHIT_ERR_ARG, "null ensemble");
   if (trials < 1) trials = 1;
@@ -1774,9 +1902,62 @@ int mhit_ensemble_autotune(mhit_ensemble* e, int trials, int* nlanes_out) {
     if (lanes == e->nbox) break;
   }
   if ((rc = ens_set_lanes(e, best_l))) return rc;
+  // the batched schedule (phase and momentum of all boxes as one persistent launch each) with
+  // uniform z chunks and the same lanes for the Poisson passes; kept if it beats the lanes
+  if (ens_batchable(e)) {
+    std::vector<int> zp(e->nbox), zm(e->nbox);
+    for (int b = 0; b < e->nbox; ++b) {
+      zp[b] = e->box[b]->zchunk_phase;
+      zm[b] = e->box[b]->zchunk_mom;
+    }
+    const int bcand[3] = {32, 64, 128};
+    int best_z = 0;
+    double best_bt = 1e30;
+    e->batched = true;
+    for (int q = 0; q < 3; ++q) {
+      for (mhit_ctx* c : e->box) {
+        c->zchunk_phase = c->zchunk_mom = std::min(bcand[q], c->g.nz);
+        if ((rc = reset_state(c))) return rc;
+      }
+      ens_drop_graphs(e);
+      double ms = 0.0;
+      if ((rc = ens_enqueue_steps(e, 2))) return rc;
+      if ((rc = mhit_ensemble_time_steps(e, 2 * trials, &ms))) return rc;
+      if (ms < best_bt) {
+        best_bt = ms;
+        best_z = bcand[q];
+      }
+    }
+    e->batched = best_bt < best_t;
+    for (int b = 0; b < e->nbox; ++b) {
+      mhit_ctx* c = e->box[b];
+      c->zchunk_phase = e->batched ? std::min(best_z, c->g.nz) : zp[b];
+      c->zchunk_mom = e->batched ? std::min(best_z, c->g.nz) : zm[b];
+    }
+    ens_drop_graphs(e);
+  } else {
+    e->batched = false;
+  }
   for (mhit_ctx* c : e->box)
     if ((rc = reset_state(c))) return rc;
   if (nlanes_out) *nlanes_out = best_l;
+  return MHIT_OK;
+}
+
+int mhit_ensemble_set_batched(mhit_ensemble* e, int on) {
+  if (!e || (on != 0 && on != 1)) return set_error(MHIT_ERR_ARG, "on must be 0 or 1");
+  if (on && !ens_batchable(e))
+    return set_error(MHIT_ERR_ARG, "the batched schedule needs equal phiflag and acdi_clamp in every box");
+  MHIT_CUDA_TRY(cudaSetDevice(e->dev));
+  MHIT_CUDA_TRY(cudaStreamSynchronize(e->st));
+  e->batched = on != 0;
+  ens_drop_graphs(e);
+  return MHIT_OK;
+}
+
+int mhit_ensemble_batched(mhit_ensemble* e, int* on) {
+  if (!e || !on) return set_error(MHIT_ERR_ARG, "null argument");
+  *on = e->batched ? 1 : 0;
   return MHIT_OK;
 }
 

@@ -35,7 +35,7 @@ def test_ensemble_matches_standalone(gpu, tune):
         if tune:
             t = ens.autotune(trials=1)
             assert 1 <= t["lanes"] <= len(cases)
-            assert all(z in (8, 16, 32, 64) for z in t["zchunk_mom"])
+            assert all(z in (8, 16, 32, 64, 128) for z in t["zchunk_mom"])
         for box, (prm, u, v, w, phi) in zip(ens.boxes, cases):
             box.upload(u, v, w, phi)
         ens.step(6)
@@ -100,3 +100,40 @@ def test_ensemble_follows_a_tracer_reupload(gpu):
     for k in ref:
         np.testing.assert_array_equal(got[k], ref[k])
     np.testing.assert_array_equal(got_part, ref_part)
+
+
+def batchable_cases(phiflag):
+    out = []
+    for b, n in enumerate((32, 64, 128, 64)):
+        prm = Params(nx=n, dt=2e-4, mu=0.003 + 0.001 * b, radius=0.3, sigma=0.4, phiflag=phiflag, acdi_clamp=1,
+                     poisson="fp32" if b % 2 else "fp64")
+        u, v, w = synth.solenoidal_velocity(n, 300 + b)
+        phi = synth.drops_phi(n, synth.drop_centres(5 + b, 400 + b), 0.3, 2 * np.pi / n) if phiflag else None
+        out.append((prm, u, v, w, phi))
+    return out
+
+
+@pytest.mark.parametrize("phiflag", [1, 0])
+def test_batched_schedule_matches_lanes_and_standalone(gpu, phiflag):
+    """The batched schedule (phase and momentum of all boxes as one persistent launch each, work
+    items from a device queue, largest boxes first) gives every box the bits of the per-box
+    lanes and of a standalone box, with the default and with autotuned z chunks."""
+    cases = batchable_cases(phiflag)
+    got = {}
+    for mode in ("batched", "lanes", "tuned"):
+        with Ensemble([c[0] for c in cases]) as ens:
+            if mode == "tuned":
+                ens.autotune(trials=1)
+            else:
+                ens.set_batched(mode == "batched")
+            assert mode == "tuned" or ens.tuning()["batched"] == (mode == "batched")
+            for box, (prm, u, v, w, phi) in zip(ens.boxes, cases):
+                box.upload(u, v, w, phi)
+            ens.step(6)
+            got[mode] = [box.download() for box in ens.boxes]
+    for b, (prm, u, v, w, phi) in enumerate(cases):
+        ref = standalone(prm, u, v, w, phi, 6)
+        for mode in got:
+            for k in ref:
+                np.testing.assert_array_equal(got[mode][b][k], ref[k], err_msg=f"{mode} box {b} {k}")
+
