@@ -1544,6 +1544,7 @@ static bool ens_batchable(const mhit_ensemble* e) {
 }
 
 static void ens_free_batch(mhit_ensemble* e) {
+  if (e->st) cudaStreamSynchronize(e->st);  // no step in flight may still read the arrays
   for (int i = 0; i < 2; ++i) {
     cudaFree(e->d_pargs[i]);
     cudaFree(e->d_margs[i]);
@@ -1644,7 +1645,8 @@ static int ens_enqueue(mhit_ensemble* e, double alpha, double beta, int cur) {
   int first = 0;
   if (e->batched) {
     int rc;
-    if ((rc = ens_prepare_batch(e))) return rc;
+    // the device argument arrays are built before any capture (they allocate)
+    if (!e->batch_ready) return set_error(MHIT_ERR_STATE, "batched ensemble arguments not prepared");
     for (mhit_ctx* c : e->box) {
       cudaStream_t saved = c->st;
       c->st = e->st;
@@ -1679,6 +1681,8 @@ static int ens_enqueue(mhit_ensemble* e, double alpha, double beta, int cur) {
 }
 
 static int ens_build(mhit_ensemble* e) {
+  int rc0;
+  if (e->batched && (rc0 = ens_prepare_batch(e))) return rc0;
   for (int par = 0; par < 2; ++par) {
     cudaGraph_t graph;
     MHIT_CUDA_TRY(cudaStreamBeginCapture(e->st, cudaStreamCaptureModeThreadLocal));
@@ -1705,6 +1709,7 @@ static int ens_enqueue_steps(mhit_ensemble* e, int nsteps) {
         return set_error(MHIT_ERR_STATE, "ensemble boxes are at different steps (upload or step all of them together)");
     int rc;
     if (n0 == 0) {
+      if (e->batched && (rc = ens_prepare_batch(e))) return rc;
       rc = ens_enqueue(e, 1.0, 0.0, cur);  // Euler first step, multi/main.f90:440-441
     } else {
       // a box whose captured arguments changed (tracers uploaded) invalidates the ensemble graphs
