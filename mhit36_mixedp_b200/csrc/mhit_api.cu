@@ -1796,13 +1796,13 @@ void mhit_ensemble_destroy(mhit_ensemble* e) {
   cudaSetDevice(e->dev);
   if (e->st) cudaStreamSynchronize(e->st);
   ens_drop_graphs(e);
+  ens_free_batch(e);  // before its stream goes
   for (cudaStream_t s : e->lanes) cudaStreamDestroy(s);
   for (cudaEvent_t v : e->join) cudaEventDestroy(v);
   if (e->fork) cudaEventDestroy(e->fork);
   for (int i = 0; i < 2; ++i)
     if (e->ev[i]) cudaEventDestroy(e->ev[i]);
   if (e->st) cudaStreamDestroy(e->st);
-  ens_free_batch(e);
   for (mhit_ctx* c : e->box) mhit_destroy(c);
   delete e;
 }
