@@ -17,6 +17,7 @@
 #include <cstdlib>
 #include <algorithm>
 #include <cstring>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -1521,18 +1522,23 @@ struct mhit_ensemble {
   bool built = false;
   std::vector<unsigned> gen;  // the boxes' graph generations the ensemble graphs were built from
   cudaEvent_t ev[2] = {nullptr, nullptr};
-  // batched schedule: the phase and momentum stages of all boxes as one persistent launch each
-  // (device work queues of (box, tile x, tile y, z chunk) items), the Poisson passes and the
-  // projection per box on the lanes
+  // batched schedule: per class of equal-size boxes, the phase and momentum stages of the
+  // class's boxes as one persistent launch each (device work queues of (box, tile x, tile y,
+  // z chunk) items), then the Poisson passes and the projection of each box on the lanes
   bool batched = false;
   bool batch_ready = false;   // device argument arrays and item lists match the boxes' tuning
   int nsm = 148;
   PhaseArgs* d_pargs[2] = {nullptr, nullptr};  // per parity of the ping-pong buffers
   MomArgs* d_margs[2] = {nullptr, nullptr};
-  int4* d_pitems = nullptr;
-  int4* d_mitems = nullptr;
-  int npitems = 0, nmitems = 0;
-  int* d_counters = nullptr;  // the two queues' counters
+  int4* d_pitems = nullptr;   // the classes' phase items, one class after the other
+  int4* d_mitems = nullptr;   // the same for the momentum stage
+  int* d_counters = nullptr;  // two queue counters per class
+  struct Class {
+    int p0, np, m0, nm;       // offset and count of the class's phase and momentum items
+  };
+  std::vector<Class> cls;     // largest boxes first
+  std::vector<int> box_cls;   // class of each box
+  std::vector<cudaEvent_t> cls_done;  // the class's momentum launch has finished
 };
 
 // The batched schedule needs one phase variant (all boxes with the phase field share the psi
@@ -1556,18 +1562,26 @@ static void ens_free_batch(mhit_ensemble* e) {
   cudaFree(e->d_counters);
   e->d_pitems = e->d_mitems = nullptr;
   e->d_counters = nullptr;
+  for (cudaEvent_t v : e->cls_done) cudaEventDestroy(v);
+  e->cls_done.clear();
+  e->cls.clear();
+  e->box_cls.clear();
   e->batch_ready = false;
 }
 
 // Device copies of every box's phase and momentum arguments (both parities; the step's alpha,
-// beta come with the launch) and the work items, largest boxes first so that the queue ends on
-// small items.
+// beta come with the launch) and the work items of each class of equal-size boxes, the classes
+// largest boxes first.
 static int ens_prepare_batch(mhit_ensemble* e) {
   if (e->batch_ready) return MHIT_OK;
   ens_free_batch(e);
-  std::vector<int> order(e->nbox);
-  for (int b = 0; b < e->nbox; ++b) order[b] = b;
-  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return e->box[x]->n > e->box[y]->n; });
+  std::vector<size_t> sizes;
+  for (const mhit_ctx* c : e->box)
+    if (std::find(sizes.begin(), sizes.end(), c->n) == sizes.end()) sizes.push_back(c->n);
+  std::sort(sizes.begin(), sizes.end(), std::greater<size_t>());
+  e->box_cls.assign(e->nbox, 0);
+  for (int b = 0; b < e->nbox; ++b)
+    e->box_cls[b] = (int)(std::find(sizes.begin(), sizes.end(), e->box[b]->n) - sizes.begin());
   std::vector<int4> pit, mit;
   std::vector<PhaseArgs> pa[2];
   std::vector<MomArgs> ma[2];
@@ -1583,18 +1597,28 @@ static int ens_prepare_batch(mhit_ensemble* e) {
       ma[par].push_back(m);
     }
   }
-  for (int b : order) {
-    const mhit_ctx* c = e->box[b];
-    if (c->prm.phiflag) {
-      const dim3 gp = phase_grid(c->g, pa[0][b].zchunk);
-      for (unsigned z = 0; z < gp.z; ++z)
-        for (unsigned y = 0; y < gp.y; ++y)
-          for (unsigned x = 0; x < gp.x; ++x) pit.push_back(make_int4(b, (int)x, (int)y, (int)z));
+  for (size_t k = 0; k < sizes.size(); ++k) {
+    mhit_ensemble::Class cl{(int)pit.size(), 0, (int)mit.size(), 0};
+    for (int b = 0; b < e->nbox; ++b) {
+      if (e->box_cls[b] != (int)k) continue;
+      const mhit_ctx* c = e->box[b];
+      if (c->prm.phiflag) {
+        const dim3 gp = phase_grid(c->g, pa[0][b].zchunk);
+        for (unsigned z = 0; z < gp.z; ++z)
+          for (unsigned y = 0; y < gp.y; ++y)
+            for (unsigned x = 0; x < gp.x; ++x) pit.push_back(make_int4(b, (int)x, (int)y, (int)z));
+      }
+      const dim3 gm = mom_grid(c->g, ma[0][b].zchunk);
+      for (unsigned z = 0; z < gm.z; ++z)
+        for (unsigned y = 0; y < gm.y; ++y)
+          for (unsigned x = 0; x < gm.x; ++x) mit.push_back(make_int4(b, (int)x, (int)y, (int)z));
     }
-    const dim3 gm = mom_grid(c->g, ma[0][b].zchunk);
-    for (unsigned z = 0; z < gm.z; ++z)
-      for (unsigned y = 0; y < gm.y; ++y)
-        for (unsigned x = 0; x < gm.x; ++x) mit.push_back(make_int4(b, (int)x, (int)y, (int)z));
+    cl.np = (int)pit.size() - cl.p0;
+    cl.nm = (int)mit.size() - cl.m0;
+    e->cls.push_back(cl);
+    cudaEvent_t ev;
+    MHIT_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    e->cls_done.push_back(ev);
   }
   int rc;
   for (int par = 0; par < 2; ++par) {
@@ -1603,9 +1627,7 @@ static int ens_prepare_batch(mhit_ensemble* e) {
   }
   if (!pit.empty() && (rc = upload_vec((void**)&e->d_pitems, pit))) return rc;
   if ((rc = upload_vec((void**)&e->d_mitems, mit))) return rc;
-  MHIT_CUDA_TRY(cudaMalloc(&e->d_counters, 2 * sizeof(int)));
-  e->npitems = (int)pit.size();
-  e->nmitems = (int)mit.size();
+  MHIT_CUDA_TRY(cudaMalloc(&e->d_counters, 2 * e->cls.size() * sizeof(int)));
   e->batch_ready = true;
   return MHIT_OK;
 }
@@ -1638,9 +1660,11 @@ static int ens_set_lanes(mhit_ensemble* e, int nlanes) {
 }
 
 // One ensemble step on e->st (captured or eager): fork, per-box sequences on lanes, join.  In the
-// batched schedule the tracer, phase and momentum stages of all boxes run first on e->st (the
-// phase and momentum stages as one persistent launch each), then the per-box Poisson passes and
-// projections fork onto the lanes.
+// batched schedule the tracers of all boxes run first on e->st; then each class of equal-size
+// boxes runs its phase and momentum stages as one persistent launch each on a lane of its own
+// (the last lanes), and each box's Poisson passes and projection follow on its lane as soon as
+// its class's momentum launch is done, so small boxes start their Poisson solves while large
+// boxes are still in their stencils.
 static int ens_enqueue(mhit_ensemble* e, double alpha, double beta, int cur) {
   int first = 0;
   if (e->batched) {
@@ -1654,20 +1678,28 @@ static int ens_enqueue(mhit_ensemble* e, double alpha, double beta, int cur) {
       c->st = saved;
       if (rc) return rc;
     }
-    if (e->npitems) {
-      BatchArgs<PhaseArgs> pb{e->d_pargs[cur], e->d_pitems, e->npitems, e->d_counters, alpha, beta};
-      MHIT_CUDA_TRY(launch_phase_batch(pb, e->box[0]->prm.acdi_clamp != 0, e->nsm, e->st));
-    }
-    BatchArgs<MomArgs> mb{e->d_margs[cur], e->d_mitems, e->nmitems, e->d_counters + 1, alpha, beta};
-    MHIT_CUDA_TRY(launch_mom_batch(mb, e->box[0]->prm.phiflag != 0, e->nsm, e->st));
     first = ST_XFWD;
   }
   MHIT_CUDA_TRY(cudaEventRecord(e->fork, e->st));
   for (int l = 0; l < e->nlanes; ++l) MHIT_CUDA_TRY(cudaStreamWaitEvent(e->lanes[l], e->fork, 0));
+  if (e->batched) {
+    for (size_t k = 0; k < e->cls.size(); ++k) {
+      const mhit_ensemble::Class& cl = e->cls[k];
+      cudaStream_t lane = e->lanes[e->nlanes - 1 - (int)(k % e->nlanes)];
+      if (cl.np) {
+        BatchArgs<PhaseArgs> pb{e->d_pargs[cur], e->d_pitems + cl.p0, cl.np, e->d_counters + 2 * k, alpha, beta};
+        MHIT_CUDA_TRY(launch_phase_batch(pb, e->box[0]->prm.acdi_clamp != 0, e->nsm, lane));
+      }
+      BatchArgs<MomArgs> mb{e->d_margs[cur], e->d_mitems + cl.m0, cl.nm, e->d_counters + 2 * k + 1, alpha, beta};
+      MHIT_CUDA_TRY(launch_mom_batch(mb, e->box[0]->prm.phiflag != 0, e->nsm, lane));
+      MHIT_CUDA_TRY(cudaEventRecord(e->cls_done[k], lane));
+    }
+  }
   for (int b = 0; b < e->nbox; ++b) {
     mhit_ctx* c = e->box[b];
     cudaStream_t saved = c->st;
     c->st = e->lanes[b % e->nlanes];
+    if (e->batched) MHIT_CUDA_TRY(cudaStreamWaitEvent(c->st, e->cls_done[e->box_cls[b]], 0));
     int rc = MHIT_OK;
     for (int s = first; s < ST_COUNT && rc == MHIT_OK; ++s) rc = enqueue_stage(c, s, alpha, beta, cur);
     c->st = saved;
