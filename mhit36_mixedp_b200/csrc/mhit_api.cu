@@ -1874,9 +1874,9 @@ int mhit_ensemble_time_steps(mhit_ensemble* e, int nsteps, double* ms) {
 // k_phase and k_mom over {8, 16, 32, 64} on the first box of the class (one profiled step per
 // candidate, best of `trials`), then time whole ensemble steps for 1, 2, 4, 8, ... lanes and
 // keep the fastest; then time the batched schedule with uniform z chunks of 32, 64 and 128
-// planes on those lanes and keep it if it is faster.  The timing steps run on zeroed fields and
-// are thrown away: every box is left zeroed with an empty history, so call this before
-// uploading the initial fields.
+// planes on those lanes and on one lane per box, and keep it if it is faster.  The timing
+// steps run on zeroed fields and are thrown away: every box is left zeroed with an empty
+// history, so call this before uploading the initial fields.
 int mhit_ensemble_autotune(mhit_ensemble* e, int trials, int* nlanes_out) {
   if (!e) return set_error(MHIT_ERR_ARG, "null ensemble");
   if (trials < 1) trials = 1;
@@ -1948,24 +1948,31 @@ int mhit_ensemble_autotune(mhit_ensemble* e, int trials, int* nlanes_out) {
       zm[b] = e->box[b]->zchunk_mom;
     }
     const int bcand[3] = {32, 64, 128};
-    int best_z = 0;
+    const int lcand[2] = {best_l, e->nbox};
+    int best_z = 0, best_bl = best_l;
     double best_bt = 1e30;
     e->batched = true;
-    for (int q = 0; q < 3; ++q) {
-      for (mhit_ctx* c : e->box) {
-        c->zchunk_phase = c->zchunk_mom = std::min(bcand[q], c->g.nz);
-        if ((rc = reset_state(c))) return rc;
-      }
-      ens_drop_graphs(e);
-      double ms = 0.0;
-      if ((rc = ens_enqueue_steps(e, 2))) return rc;
-      if ((rc = mhit_ensemble_time_steps(e, 2 * trials, &ms))) return rc;
-      if (ms < best_bt) {
-        best_bt = ms;
-        best_z = bcand[q];
+    for (int li = 0; li < (best_l == e->nbox ? 1 : 2); ++li) {
+      if ((rc = ens_set_lanes(e, lcand[li]))) return rc;
+      for (int q = 0; q < 3; ++q) {
+        for (mhit_ctx* c : e->box) {
+          c->zchunk_phase = c->zchunk_mom = std::min(bcand[q], c->g.nz);
+          if ((rc = reset_state(c))) return rc;
+        }
+        ens_drop_graphs(e);
+        double ms = 0.0;
+        if ((rc = ens_enqueue_steps(e, 2))) return rc;
+        if ((rc = mhit_ensemble_time_steps(e, 2 * trials, &ms))) return rc;
+        if (ms < best_bt) {
+          best_bt = ms;
+          best_z = bcand[q];
+          best_bl = lcand[li];
+        }
       }
     }
     e->batched = best_bt < best_t;
+    if ((rc = ens_set_lanes(e, e->batched ? best_bl : best_l))) return rc;
+    if (nlanes_out) *nlanes_out = e->nlanes;
     for (int b = 0; b < e->nbox; ++b) {
       mhit_ctx* c = e->box[b];
       c->zchunk_phase = e->batched ? std::min(best_z, c->g.nz) : zp[b];
@@ -1977,7 +1984,7 @@ int mhit_ensemble_autotune(mhit_ensemble* e, int trials, int* nlanes_out) {
   }
   for (mhit_ctx* c : e->box)
     if ((rc = reset_state(c))) return rc;
-  if (nlanes_out) *nlanes_out = best_l;
+  if (nlanes_out && !e->batched) *nlanes_out = best_l;
   return MHIT_OK;
 }
 
