@@ -50,9 +50,9 @@ METRIC = "ms/timestep 512^3 NS+ACDI, 1 B200: mixed-prec Poisson vs FP64, at matc
 # algorithmic HBM bytes per grid point and launch (compulsory traffic of each kernel)
 BYTES_PER_POINT = {
     "fp32": {"k_phase": 56, "k_mom": 104, "k_div_fftx": 28, "k_fft_cols_yfwd": 8, "k_fft_cols_zsolve": 8,
-             "k_fft_cols_yinv": 8, "k_fftx_inv": 8, "k_correct+k_finalize": 52},
+             "k_fft_cols_yinv": 8, "k_fftx_inv": 8, "k_correct+k_finalize": 52, "k_xinv_correct+k_finalize": 52},
     "fp64": {"k_phase": 56, "k_mom": 104, "k_div_fftx": 32, "k_fft_cols_yfwd": 16, "k_fft_cols_zsolve": 16,
-             "k_fft_cols_yinv": 16, "k_fftx_inv": 16, "k_correct+k_finalize": 56},
+             "k_fft_cols_yinv": 16, "k_fftx_inv": 16, "k_correct+k_finalize": 56, "k_xinv_correct+k_finalize": 56},
 }
 # DRAM bytes per grid point and launch measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum
 # of one launch / cells): k_phase and k_mom from a 256^3 capture, the Poisson and projection kernels
@@ -63,11 +63,11 @@ TRAFFIC_PER_POINT = {"k_phase": 55.1, "k_mom": 104.4, "k_div_fftx": 28.4, "k_fft
                      "k_correct+k_finalize": 51.2}
 TRAFFIC_SOURCE = {"k_phase": "256^3", "k_mom": "256^3"}
 BYTES_PER_POINT["fp32_incremental"] = dict(BYTES_PER_POINT["fp32"], k_div_fftx=32, k_fftx_inv=20,
-                                           **{"k_correct+k_finalize": 56})
-# the step-level model: NS+ACDI 256 B/pt (FP32 Poisson), 280 B/pt (FP64); the incremental FP32
-# solve adds the predictor's read in the x pass (4), the predictor's read and rewrite and the
-# FP64 pressure's write in the x-inverse (12) and the FP64 pressure in the projection (4): 276 B/pt
-STEP_BYTES = {"fp32": 256, "fp64": 280, "fp32_incremental": 276}
+                                           **{"k_correct+k_finalize": 56, "k_xinv_correct+k_finalize": 60})
+# the step-level model (the x-inverse fused with the projection, the y/z passes as two spectrum
+# round trips): NS+ACDI 256 B/pt (FP32 Poisson), 280 B/pt (FP64); the incremental FP32 solve adds
+# the predictor's read in the x pass (4) and its read and write in the fused projection (8): 268
+STEP_BYTES = {"fp32": 256, "fp64": 280, "fp32_incremental": 268}
 
 
 def peaks():

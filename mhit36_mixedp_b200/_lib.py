@@ -103,6 +103,7 @@ SIGNATURES = {
     "mhit_debug_commit_step": (_c.c_int, [_c.c_void_p]),
     "mhit_debug_set_label_bound": (_c.c_int, [_c.c_void_p, _c.c_longlong]),
     "mhit_debug_set_mom_tma": (_c.c_int, [_c.c_void_p, _c.c_int]),
+    "mhit_debug_set_fused_projection": (_c.c_int, [_c.c_void_p, _c.c_int]),
     "mhit_debug_buffer_len": (_c.c_longlong, [_c.c_void_p, _c.c_int]),
     "mhit_debug_get_buffer": (_c.c_int, [_c.c_void_p, _c.c_int, _dp]),
 }

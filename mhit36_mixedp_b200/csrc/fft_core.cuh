@@ -26,6 +26,13 @@ template <> struct Radix<256>  { static constexpr int ns = 2; static constexpr i
 template <> struct Radix<512>  { static constexpr int ns = 3; static constexpr int r[3] = {8, 8, 8}; };
 template <> struct Radix<1024> { static constexpr int ns = 3; static constexpr int r[3] = {8, 8, 16}; };
 
+// Schedule of the inverse x transforms fused with the projection (and of the pressure they
+// leave in the spectrum, transformed on demand with the same arithmetic): at most radix 8, since
+// 16-point butterflies hold 32 complex values per thread on top of the carried pressures.
+template <int N> struct XcRadix : Radix<N> {};
+template <> struct XcRadix<128> { static constexpr int ns = 3; static constexpr int r[3] = {8, 4, 4}; };
+template <> struct XcRadix<256> { static constexpr int ns = 3; static constexpr int r[3] = {8, 8, 4}; };
+
 template <int N> __host__ __device__ constexpr int max_radix() {
   int m = 0;
   for (int s = 0; s < Radix<N>::ns; ++s) m = Radix<N>::r[s] > m ? Radix<N>::r[s] : m;
@@ -175,28 +182,59 @@ __device__ __forceinline__ void stockham_stage(Cx<T>* s, const Cx<T>* __restrict
   __syncthreads();
 }
 
-// Full transform of the N x B tile in s (unnormalised in both directions, as cuFFT).
-// Caller must __syncthreads() before (tile loaded); returns after a barrier.
-template <typename T, int N, int B, int NT, bool INV>
+// Full transform of the N x B tile in s (unnormalised in both directions, as cuFFT), in the
+// radix schedule S (default Radix<N>).  Caller must __syncthreads() before (tile loaded); returns
+// after a barrier.
+template <typename T, int N, int B, int NT, bool INV, typename S = Radix<N>>
 __device__ __forceinline__ void fft_tile(Cx<T>* s, const Cx<T>* __restrict__ tw, int twstride) {
-  constexpr int NS = Radix<N>::ns;
+  constexpr int NS = S::ns;
   int p = 1;
   if constexpr (NS >= 1) {
-    constexpr int R = Radix<N>::r[0];
+    constexpr int R = S::r[0];
     stockham_stage<T, N, B, NT, R, INV>(s, tw, twstride, p);
     p *= R;
   }
   if constexpr (NS >= 2) {
-    constexpr int R = Radix<N>::r[1];
+    constexpr int R = S::r[1];
     stockham_stage<T, N, B, NT, R, INV>(s, tw, twstride, p);
     p *= R;
   }
   if constexpr (NS >= 3) {
-    constexpr int R = Radix<N>::r[2];
+    constexpr int R = S::r[2];
     stockham_stage<T, N, B, NT, R, INV>(s, tw, twstride, p);
   }
 }
 
+
+// C2R preparation of B half spectra of length M+1 (kx = 0..M) in the tile s, in place: the
+// packed half-length sequence Z[k] = (X[k] + X*[M-k]) + i W^-k (X[k] - X*[M-k]), W = exp(-2 pi
+// i/(2M)), whose inverse transform gives the real line as (even + i odd) pairs; the imaginary
+// parts of X[0] and X[M] are ignored.  Caller synchronises before (tile loaded) and after.
+template <typename T, int M, int B, int NT>
+__device__ __forceinline__ void c2r_untangle(Cx<T>* s, const Cx<T>* __restrict__ twx) {
+  for (int e = threadIdx.x; e < (M / 2 + 1) * B; e += NT) {
+    const int kk = e / B, b = e - kk * B;
+    if (kk == 0) {
+      const T a = s[sw<B>(0, b)].x, c = s[sw<B>(M, b)].x;
+      s[sw<B>(0, b)] = cx<T>(a + c, a - c);
+    } else {
+      const Cx<T> xk = s[sw<B>(kk, b)];
+      const Cx<T> xm = s[sw<B>(M - kk, b)];
+      {
+        const Cx<T> a = xk + conj(xm);
+        const Cx<T> d = xk - conj(xm);
+        const Cx<T> t = cmul(conj(twx[kk]), d);
+        s[sw<B>(kk, b)] = cx<T>(a.x - t.y, a.y + t.x);
+      }
+      if (kk != M - kk) {
+        const Cx<T> a = xm + conj(xk);
+        const Cx<T> d = xm - conj(xk);
+        const Cx<T> t = cmul(conj(twx[M - kk]), d);
+        s[sw<B>(M - kk, b)] = cx<T>(a.x - t.y, a.y + t.x);
+      }
+    }
+  }
+}
 
 // ---------------------------------------------------------------- stages with register I/O
 // Stage s of the transform in radix order REV (false: Radix<N>::r[0..ns-1], true: reversed).

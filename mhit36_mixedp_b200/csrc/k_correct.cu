@@ -207,7 +207,11 @@ cudaError_t launch_correct(const CorrectArgs& a, cudaStream_t st) {
   else k_correct<<<grd, blk, 0, st>>>(a, PDouble{static_cast<const double*>(a.p)}, zc);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  k_finalize<<<1, 1024, 0, st>>>(a.partials, a.nblocks, a.g, a.sc);
+  return launch_finalize(a.partials, a.nblocks, a.g, a.sc, st);
+}
+
+cudaError_t launch_finalize(const double* partials, int nblocks, const Geo& g, DevScalars* sc, cudaStream_t st) {
+  k_finalize<<<1, 1024, 0, st>>>(partials, nblocks, g, sc);
   return cudaGetLastError();
 }
 

@@ -159,12 +159,14 @@ k_div_fftx(const double* __restrict__ u, const double* __restrict__ v, const dou
 
 // ------------------------------------------------------------------ inverse x -> pressure
 // INC (incremental FP32 solve): the transform is the correction delta; with q the FP32 predictor
-// in `pred`, the pressure s = q + delta is formed in FP64 and written to `p64` (what the
-// projection reads), and hi = fl32(s) over q (the next step's predictor).
-template <typename T, int M, bool INC>
+// in `qin`, the pressure s = q + delta is formed in FP64 and written to `p64` (what the
+// projection reads), and fl32(s) to `qout` (the next step's predictor; skipped when null).
+// S: the radix schedule (XcRadix<M> for the pressure the fused projection left in the spectrum,
+// so it is transformed with the projection's arithmetic).
+template <typename T, int M, bool INC, typename S = Radix<M>>
 __global__ void __launch_bounds__(xpass_threads<T, M>())
 k_fftx_inv(const Cx<T>* __restrict__ spec, T* __restrict__ p, const Cx<T>* __restrict__ twx, Geo g,
-           float* __restrict__ pred, double* __restrict__ p64) {
+           const float* __restrict__ qin, float* __restrict__ qout, double* __restrict__ p64) {
   constexpr int B = Tile<T>::B;
   constexpr int NT = xpass_threads<T, M>();
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -181,31 +183,9 @@ k_fftx_inv(const Cx<T>* __restrict__ spec, T* __restrict__ p, const Cx<T>* __res
   __pipeline_commit();
   __pipeline_wait_prior(0);
   __syncthreads();
-  // Z[k] = (X[k] + X*[M-k]) + i W^-k (X[k] - X*[M-k]); imaginary parts of X[0], X[M] ignored
-  for (int e = threadIdx.x; e < (M / 2 + 1) * B; e += NT) {
-    const int kk = e / B, b = e - kk * B;
-    if (kk == 0) {
-      const T a = s[sw<B>(0, b)].x, c = s[sw<B>(M, b)].x;
-      s[sw<B>(0, b)] = cx<T>(a + c, a - c);
-    } else {
-      const Cx<T> xk = s[sw<B>(kk, b)];
-      const Cx<T> xm = s[sw<B>(M - kk, b)];
-      {
-        const Cx<T> a = xk + conj(xm);
-        const Cx<T> d = xk - conj(xm);
-        const Cx<T> t = cmul(conj(twx[kk]), d);
-        s[sw<B>(kk, b)] = cx<T>(a.x - t.y, a.y + t.x);
-      }
-      if (kk != M - kk) {
-        const Cx<T> a = xm + conj(xk);
-        const Cx<T> d = xm - conj(xk);
-        const Cx<T> t = cmul(conj(twx[M - kk]), d);
-        s[sw<B>(M - kk, b)] = cx<T>(a.x - t.y, a.y + t.x);
-      }
-    }
-  }
+  c2r_untangle<T, M, B, NT>(s, twx);
   __syncthreads();
-  fft_tile<T, M, B, NT, true>(s, twx, 2);
+  fft_tile<T, M, B, NT, true, S>(s, twx, 2);
   for (int e = threadIdx.x; e < M * B; e += NT) {
     const int b = e / M, n = e - b * M;
     const int line = line0 + b;
@@ -213,10 +193,9 @@ k_fftx_inv(const Cx<T>* __restrict__ spec, T* __restrict__ p, const Cx<T>* __res
       const Cx<T> z = s[sw<B>(n, b)];
       if constexpr (INC) {
         const size_t o = (size_t)line * nx + 2 * n;
-        float2* q = reinterpret_cast<float2*>(pred + o);
-        const float2 q2 = *q;
+        const float2 q2 = *reinterpret_cast<const float2*>(qin + o);
         const double s0 = (double)q2.x + (double)z.x, s1 = (double)q2.y + (double)z.y;
-        *q = make_float2((float)s0, (float)s1);
+        if (qout) *reinterpret_cast<float2*>(qout + o) = make_float2((float)s0, (float)s1);
         *reinterpret_cast<double2*>(p64 + o) = make_double2(s0, s1);
       } else {
         store2<T>(p + (size_t)line * nx + 2 * n, z.x, z.y);
@@ -400,12 +379,13 @@ template <typename T, int M>
 static cudaError_t launch_xinv_m(const PoissonArgs& a, cudaStream_t st) {
   constexpr int B = Tile<T>::B;
   const size_t smem = (size_t)(M + 1) * B * sizeof(Cx<T>);
-  auto kern = a.pinc ? k_fftx_inv<T, M, true> : k_fftx_inv<T, M, false>;
+  auto kern = a.xc_sched ? (a.qin ? k_fftx_inv<T, M, true, XcRadix<M>> : k_fftx_inv<T, M, false, XcRadix<M>>)
+                         : (a.qin ? k_fftx_inv<T, M, true> : k_fftx_inv<T, M, false>);
   cudaError_t e = prep_smem(kern, smem);
   if (e != cudaSuccess) return e;
   const int nlines = a.g.ny * a.g.nz;
   kern<<<(nlines + B - 1) / B, xpass_threads<T, M>(), smem, st>>>((const Cx<T>*)a.spec, (T*)a.p, (const Cx<T>*)a.twx,
-                                                                  a.g, a.pinc, a.p64);
+                                                                  a.g, a.qin, a.qout, a.p64);
   return cudaGetLastError();
 }
 

@@ -40,10 +40,12 @@ struct PoissonArgs {
   // pressure (refinement sweep, incremental solve)
   const float* presid = nullptr;
   // non-null: x-inverse adds its transform to this FP32 predictor in FP64, writes the sum to p64
-  // and its FP32 rounding back here (incremental solve)
-  float* pinc = nullptr;
+  // and its FP32 rounding to qout (incremental solve; qout null: p64 only)
+  const float* qin = nullptr;
+  float* qout = nullptr;
   double* p64 = nullptr;
   bool real64 = false;           // x-forward transforms the FP64 field u (energy spectrum)
+  bool xc_sched = false;         // x-inverse in the radix schedule of the fused projection
   const ZsolveTc* tcz = nullptr;  // non-null (FP32, nz = 512): the z solve runs on the tensor cores
   DevScalars* sc = nullptr;       // flag word for the tensor-core z solve's bounded waits
 };
@@ -122,6 +124,27 @@ struct CorrectArgs {
 };
 cudaError_t launch_correct(const CorrectArgs& a, cudaStream_t st);
 int correct_blocks(const Geo& g);
+// k_finalize: the projection's partial sums/maxima -> mean, gumax, cfl, flags (fixed order)
+cudaError_t launch_finalize(const double* partials, int nblocks, const Geo& g, DevScalars* sc, cudaStream_t st);
+
+// the inverse x transform fused with the projection (the pressure stays on chip): u*, v*, w*
+// projected in place from the y-inverted spectrum, partial sums/maxima as k_correct, then
+// k_finalize.  The FP32 modes transform in FP32; qold non-null selects the incremental solve
+// (pressure = qold + delta in FP64, fl32 of it to qnew).
+struct XcArgs {
+  Geo g;
+  bool fp32;
+  const void* spec;           // Cx<T>[nz][ny][pitch] after the y inverse
+  const void* twx;            // exp(-2 pi i m/nx) in T
+  double *u, *v, *w;          // u* in, u** out
+  const float* qold = nullptr;
+  float* qnew = nullptr;
+  double* partials;           // [xc_blocks(g)][6]
+  DevScalars* sc;
+  int zc = 0;                 // z planes per block (0: default)
+};
+cudaError_t launch_xinv_correct(const XcArgs& a, cudaStream_t st);
+int xc_blocks(const Geo& g, int zc);
 
 // on-demand diagnostics of the current velocity: max|div|, KE, dissipation
 struct DiagArgs {

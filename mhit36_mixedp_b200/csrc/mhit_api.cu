@@ -51,6 +51,7 @@ enum {
 static const char* kStageNames[ST_COUNT] = {"k_tracer", "k_phase", "k_mom", "k_div_fftx", "k_fft_cols_yfwd",
                                             "k_fft_cols_zsolve", "k_fft_cols_yinv", "k_fftx_inv",
                                             "refine(5 passes)", "k_correct+k_finalize"};
+static const char* kFusedCorrectName = "k_xinv_correct+k_finalize";
 
 struct mhit_ctx {
   mhit_params prm;
@@ -62,6 +63,7 @@ struct mhit_ctx {
   double *RU = nullptr, *RV = nullptr, *RW = nullptr;
   double *PHI[2] = {}, *RPHI = nullptr;
   void* P = nullptr;
+  float* Q[2] = {};       // incremental: the FP32 predictor, ping-pong (the step reading set k reads Q[k])
   float* P2 = nullptr;    // refinement: the pressure correction (FP32)
   double* P64 = nullptr;  // refinement: corrected pressure for a download; incremental: the pressure (FP64)
   double* Pw = nullptr;   // FP32 modes: the pressure widened to FP64 for a download (lazy)
@@ -94,12 +96,22 @@ struct mhit_ctx {
   CUtensorMap tm_u[2], tm_v[2], tm_w[2], tm_phi[2];  // k_mom's ring boxes over U, V, W, PHI[0..1]
   int mom_tma = 1;                        // k_mom fills its interior rings by TMA (test hook: 0)
   int graph_kernels = 0;                  // kernel nodes in a captured step graph
+  // 1: the inverse x transform runs fused with the projection (k_xinv_correct); 0 (the default,
+  // the faster today): k_fftx_inv + k_correct.  The fused pass leaves the pressure in the spectrum
+  // only: after such a step p_lazy is set, and whatever reads the pressure or reuses the spectrum
+  // first materialises it (materialise_pressure).
+  int fuse_xc = 0;
+  bool p_lazy = false;
+  int nblk_xc = 0;                        // blocks of k_xinv_correct (partials rows)
 };
 
 // ------------------------------------------------------------------ helpers
 static size_t tsize(const mhit_ctx* c) { return c->prm.poisson == MHIT_POISSON_FP64 ? 8 : 4; }
 static bool refined(const mhit_ctx* c) { return c->prm.poisson == MHIT_POISSON_FP32_REFINED; }
 static bool incremental(const mhit_ctx* c) { return c->prm.poisson == MHIT_POISSON_FP32_INCREMENTAL; }
+// the step's inverse x transform runs inside the projection (every mode but the refinement sweep,
+// whose projection reads the sum of two pressures)
+static bool fused_xc(const mhit_ctx* c) { return c->fuse_xc && !refined(c); }
 
 static int check_ctx(mhit_ctx* c) {
   if (!c) return set_error(MHIT_ERR_ARG, "null context");
@@ -144,9 +156,10 @@ static int reset_history(mhit_ctx* c, bool keep_pressure = false) {
   MHIT_CUDA_TRY(cudaMemsetAsync(c->RV, 0, bytes, c->st));
   MHIT_CUDA_TRY(cudaMemsetAsync(c->RW, 0, bytes, c->st));
   if (c->RPHI) MHIT_CUDA_TRY(cudaMemsetAsync(c->RPHI, 0, bytes, c->st));
-  if (incremental(c) && !keep_pressure) {  // the pressure restarts at 0
-    MHIT_CUDA_TRY(cudaMemsetAsync(c->P, 0, c->n * sizeof(float), c->st));
+  if (incremental(c) && !keep_pressure) {  // the pressure restarts at 0 (both predictor buffers)
+    MHIT_CUDA_TRY(cudaMemsetAsync(c->P, 0, 2 * c->n * sizeof(float), c->st));
     MHIT_CUDA_TRY(cudaMemsetAsync(c->P64, 0, c->n * sizeof(double), c->st));
+    c->p_lazy = false;
   }
   DevScalars s;
   memset(&s, 0, sizeof(s));
@@ -181,10 +194,11 @@ __global__ void k_clear_mean(DevScalars* sc) {
 }
 
 // ------------------------------------------------------------------ one step
-static bool stage_runs(const mhit_ctx* c, int stage) {
+static bool stage_runs(const mhit_ctx* c, int stage, bool fz) {
   if (stage == ST_TRACER) return c->prm.partflag && c->np > 0;
   if (stage == ST_PHASE) return c->prm.phiflag != 0;
   if (stage == ST_REFINE) return c->prm.poisson == MHIT_POISSON_FP32_REFINED;
+  if (stage == ST_XINV) return !fz;  // fused into the projection
   return true;
 }
 
@@ -234,11 +248,12 @@ static MomArgs mom_args(const mhit_ctx* c, double alpha, double beta, int cur) {
   return a;
 }
 
-// Launch one stage of the step that reads buffer set `cur` and writes set `cur ^ 1`.
-static int enqueue_stage(mhit_ctx* c, int stage, double alpha, double beta, int cur) {
+// Launch one stage of the step that reads buffer set `cur` and writes set `cur ^ 1`; fz: the
+// inverse x transform runs inside the projection stage.
+static int enqueue_stage(mhit_ctx* c, int stage, double alpha, double beta, int cur, bool fz) {
   const int nxt = cur ^ 1;
   const mhit_params& p = c->prm;
-  if (!stage_runs(c, stage)) return MHIT_OK;
+  if (!stage_runs(c, stage, fz)) return MHIT_OK;
   switch (stage) {
     case ST_TRACER: {
       TracerArgs a;
@@ -291,11 +306,12 @@ static int enqueue_stage(mhit_ctx* c, int stage, double alpha, double beta, int 
       a.tcz = c->tcz;
       a.sc = c->sc;
       if (incremental(c)) {
-        // the residual of the predictor P in the x pass; the x-inverse writes the pressure
-        // P + delta to P64 in FP64 and its FP32 rounding to P
-        if (stage == ST_XFWD) a.presid = static_cast<const float*>(c->P);
+        // the residual of the predictor Q[cur] in the x pass; the x-inverse writes the pressure
+        // Q[cur] + delta to P64 in FP64 and its FP32 rounding to Q[nxt]
+        if (stage == ST_XFWD) a.presid = c->Q[cur];
         if (stage == ST_XINV) {
-          a.pinc = static_cast<float*>(c->P);
+          a.qin = c->Q[cur];
+          a.qout = c->Q[nxt];
           a.p64 = c->P64;
         }
       }
@@ -311,6 +327,24 @@ static int enqueue_stage(mhit_ctx* c, int stage, double alpha, double beta, int 
       return MHIT_OK;
     }
     case ST_CORRECT: {
+      if (fz) {
+        XcArgs x;
+        x.g = c->g;
+        x.fp32 = p.poisson != MHIT_POISSON_FP64;
+        x.spec = c->spec;
+        x.twx = c->twx;
+        x.u = c->U[nxt];
+        x.v = c->V[nxt];
+        x.w = c->W[nxt];
+        if (incremental(c)) {
+          x.qold = c->Q[cur];
+          x.qnew = c->Q[nxt];
+        }
+        x.partials = c->partials;
+        x.sc = c->sc;
+        MHIT_CUDA_TRY(launch_xinv_correct(x, c->st));
+        return MHIT_OK;
+      }
       CorrectArgs a;
       a.g = c->g;
       a.u = c->U[nxt];
@@ -330,13 +364,43 @@ static int enqueue_stage(mhit_ctx* c, int stage, double alpha, double beta, int 
 }
 
 static int enqueue_step(mhit_ctx* c, double alpha, double beta, int cur, bool profile) {
+  const bool fz = fused_xc(c);
   for (int s = 0; s < ST_COUNT; ++s) {
-    const bool ran = stage_runs(c, s);
+    const bool ran = stage_runs(c, s, fz);
     if (profile && ran) MHIT_CUDA_TRY(cudaEventRecord(c->ev[2 * s], c->st));
-    int rc = enqueue_stage(c, s, alpha, beta, cur);
+    int rc = enqueue_stage(c, s, alpha, beta, cur, fz);
     if (rc) return rc;
     if (profile && ran) MHIT_CUDA_TRY(cudaEventRecord(c->ev[2 * s + 1], c->st));
   }
+  return MHIT_OK;
+}
+
+// The pressure of the last step into P (P64 in the incremental solve) when the fused projection
+// left it in the spectrum: the inverse x transform of the y-inverted spectrum, which no kernel
+// touches between steps until this runs; in the incremental solve added to the predictor that
+// step read, Q[cur ^ 1] (the one it wrote, Q[cur], already holds fl32 of the sum).
+static int materialise_pressure(mhit_ctx* c) {
+  if (!c->p_lazy) return MHIT_OK;
+  PoissonArgs a;
+  a.g = c->g;
+  a.fp32 = c->prm.poisson != MHIT_POISSON_FP64;
+  a.u = a.v = a.w = nullptr;
+  a.spec = c->spec;
+  a.p = c->P;
+  a.twx = c->twx;
+  a.twy = c->twy;
+  a.twz = c->twz;
+  a.k2x = a.k2y = a.k2z = nullptr;
+  a.cdiv = 0.0;
+  a.ntot = (double)c->n;
+  a.xc_sched = true;  // the arithmetic of the fused pass: the pressure the projection used
+  if (incremental(c)) {
+    a.qin = c->Q[c->cur ^ 1];
+    a.qout = nullptr;
+    a.p64 = c->P64;
+  }
+  MHIT_CUDA_TRY(poisson_stage(a, PSTAGE_XINV, c->st));
+  c->p_lazy = false;
   return MHIT_OK;
 }
 
@@ -388,6 +452,7 @@ static int enqueue_steps(mhit_ctx* c, int nsteps) {
     if (rc) return rc;
     c->cur ^= 1;
     c->nstep++;
+    c->p_lazy = fused_xc(c);
   }
   return MHIT_OK;
 }
@@ -588,7 +653,12 @@ static int init_impl(const mhit_params* p, mhit_ctx* c) {
   MHIT_CUDA_TRY(cudaMalloc(&c->RW, fb));
   if (p->phiflag) MHIT_CUDA_TRY(cudaMalloc(&c->RPHI, fb));
   const size_t ts = tsize(c);
-  MHIT_CUDA_TRY(cudaMalloc(&c->P, n * ts));
+  // the incremental solve keeps two FP32 predictors (read one, write the other), in one block
+  MHIT_CUDA_TRY(cudaMalloc(&c->P, (incremental(c) ? 2 : 1) * n * ts));
+  if (incremental(c)) {
+    c->Q[0] = static_cast<float*>(c->P);
+    c->Q[1] = c->Q[0] + n;
+  }
   if (refined(c)) {
     MHIT_CUDA_TRY(cudaMalloc(&c->P2, n * sizeof(float)));
     MHIT_CUDA_TRY(cudaMemset(c->P2, 0, n * sizeof(float)));
@@ -597,7 +667,7 @@ static int init_impl(const mhit_params* p, mhit_ctx* c) {
     MHIT_CUDA_TRY(cudaMalloc(&c->P64, n * sizeof(double)));
     MHIT_CUDA_TRY(cudaMemset(c->P64, 0, n * sizeof(double)));
   }
-  MHIT_CUDA_TRY(cudaMemset(c->P, 0, n * ts));
+  MHIT_CUDA_TRY(cudaMemset(c->P, 0, (incremental(c) ? 2 : 1) * n * ts));
   MHIT_CUDA_TRY(cudaMalloc(&c->spec, (size_t)g.pitch * g.ny * g.nz * 2 * ts));
   MHIT_CUDA_TRY(cudaMemset(c->spec, 0, (size_t)g.pitch * g.ny * g.nz * 2 * ts));
   int rc;
@@ -647,7 +717,8 @@ static int init_impl(const mhit_params* p, mhit_ctx* c) {
     if ((rc = upload_vec((void**)&c->tabs, t))) return rc;
   }
   c->nblk = correct_blocks(g);
-  MHIT_CUDA_TRY(cudaMalloc(&c->partials, (size_t)c->nblk * 6 * sizeof(double)));
+  c->nblk_xc = xc_blocks(g, 0);
+  MHIT_CUDA_TRY(cudaMalloc(&c->partials, (size_t)std::max(c->nblk, c->nblk_xc) * 6 * sizeof(double)));
   MHIT_CUDA_TRY(cudaMalloc(&c->sc, sizeof(DevScalars)));
   MHIT_CUDA_TRY(cudaMallocHost(&c->sc_host, sizeof(DevScalars)));
   return reset_history(c);
@@ -813,21 +884,24 @@ int mhit_profile_step(mhit_ctx* c, double* ms, const char** names, int* nstages)
   if (!ms || !nstages || *nstages < ST_COUNT) return set_error(MHIT_ERR_ARG, "need room for all stages");
   const bool first = c->nstep == 0;
   MHIT_CUDA_TRY(cudaStreamSynchronize(c->st));
+  if ((rc = materialise_pressure(c))) return rc;  // not needed by the step; keeps the flag exact
   // mark stages that do not run
   for (int i = 0; i < ST_COUNT; ++i) ms[i] = -1.0;
   if ((rc = enqueue_step(c, first ? 1.0 : 1.5, first ? 0.0 : 0.5, c->cur, true))) return rc;
   MHIT_CUDA_TRY(cudaStreamSynchronize(c->st));
+  const bool fz = fused_xc(c);
   for (int i = 0; i < ST_COUNT; ++i) {
-    if (stage_runs(c, i)) {
+    if (stage_runs(c, i, fz)) {
       float f = 0.f;
       MHIT_CUDA_TRY(cudaEventElapsedTime(&f, c->ev[2 * i], c->ev[2 * i + 1]));
       ms[i] = f;
     }
-    if (names) names[i] = kStageNames[i];
+    if (names) names[i] = (i == ST_CORRECT && fz) ? kFusedCorrectName : kStageNames[i];
   }
   *nstages = ST_COUNT;
   c->cur ^= 1;
   c->nstep++;
+  c->p_lazy = fz;
   return MHIT_OK;
 }
 
@@ -853,6 +927,7 @@ int mhit_download_fields(mhit_ctx* c, double* u, double* v, double* w, double* p
   }
   if (phi) MHIT_CUDA_TRY(cudaMemcpyAsync(phi, c->PHI[c->cur], fb, cudaMemcpyDeviceToHost, c->st));
   if (p) {
+    if ((rc = materialise_pressure(c))) return rc;
     const double* src = static_cast<const double*>(c->P);
     if (incremental(c)) {  // the FP64 pressure of the last projection
       src = c->P64;
@@ -949,12 +1024,14 @@ int mhit_read_field(mhit_ctx* c, const char* path, int fieldn) {
       // mode also keeps the file's FP64 values
       std::vector<float> pf(c->n);
       for (size_t i = 0; i < c->n; ++i) pf[i] = (float)buf[i];
-      MHIT_CUDA_TRY(cudaMemcpyAsync(c->P, pf.data(), c->n * 4, cudaMemcpyHostToDevice, c->st));
+      void* dst = incremental(c) ? static_cast<void*>(c->Q[c->cur]) : c->P;
+      MHIT_CUDA_TRY(cudaMemcpyAsync(dst, pf.data(), c->n * 4, cudaMemcpyHostToDevice, c->st));
       if (incremental(c)) MHIT_CUDA_TRY(cudaMemcpyAsync(c->P64, buf.data(), fb, cudaMemcpyHostToDevice, c->st));
       MHIT_CUDA_TRY(cudaStreamSynchronize(c->st));
     } else {
       MHIT_CUDA_TRY(cudaMemcpyAsync(c->P, buf.data(), fb, cudaMemcpyHostToDevice, c->st));
     }
+    c->p_lazy = false;
   }
   MHIT_CUDA_TRY(cudaStreamSynchronize(c->st));
   // a field read happens at setup: the next step is an Euler step with empty history
@@ -987,7 +1064,8 @@ std::vector<CkptArray> ckpt_arrays(mhit_ctx* c) {
     a.push_back({c->PHI[k], fb});
     a.push_back({c->RPHI, fb});
   }
-  a.push_back({c->P, c->n * tsize(c)});
+  // the pressure in the Poisson precision (incremental: the predictor the next step reads)
+  a.push_back({incremental(c) ? static_cast<void*>(c->Q[k]) : c->P, c->n * tsize(c)});
   if (c->P2) a.push_back({c->P2, c->n * sizeof(float)});  // refinement: the correction
   if (incremental(c)) a.push_back({c->P64, c->n * sizeof(double)});  // incremental: the FP64 pressure
   return a;
@@ -1005,6 +1083,7 @@ int mhit_write_checkpoint(mhit_ctx* c, const char* path) {
   int rc;
   if ((rc = check_ctx(c))) return rc;
   if (!path) return set_error(MHIT_ERR_ARG, "null path");
+  if ((rc = materialise_pressure(c))) return rc;
   if ((rc = fetch_scalars(c))) return rc;
   FileCloser fc{fopen(path, "wb")};
   if (!fc.f) return set_error(MHIT_ERR_IO, std::string("cannot create ") + path);
@@ -1089,6 +1168,7 @@ int mhit_read_checkpoint(mhit_ctx* c, const char* path) {
   *c->sc_host = s;
   MHIT_CUDA_TRY(cudaMemcpy(c->sc, c->sc_host, sizeof(DevScalars), cudaMemcpyHostToDevice));
   c->nstep = h.nstep;
+  c->p_lazy = false;
   return MHIT_OK;
 }
 
@@ -1123,6 +1203,7 @@ int mhit_label_drops(mhit_ctx* c, double thresh, int connectivity, mhit_drop* dr
   const int nx = c->prm.nx, ny = c->prm.ny, nz = c->prm.nz;
   const int n = (int)c->n;
   const int nch = label_chunks(n);
+  if ((rc = materialise_pressure(c))) return rc;  // the spectrum becomes scratch
   // scratch: the spectrum buffer (at least 4 bytes per cell, unused between steps) holds the
   // parents; the chunk counts, the error flag and the trig tables share one allocation
   const size_t trig_n = 2 * (size_t)(nx + ny + nz);
@@ -1370,6 +1451,7 @@ int mhit_energy_spectrum(mhit_ctx* c, double* E, int nbins) {
   void* spec;
   const void *tx, *ty, *tz;
   if (c->prm.poisson == MHIT_POISSON_FP64) {  // the Poisson spectrum is scratch between steps
+    if ((rc = materialise_pressure(c))) return rc;
     spec = c->spec;
     tx = c->twx;
     ty = c->twy;
@@ -1422,8 +1504,10 @@ int mhit_debug_run_stage(mhit_ctx* c, int stage) {
   int rc;
   if ((rc = check_ctx(c))) return rc;
   if (stage < 0 || stage >= ST_COUNT) return set_error(MHIT_ERR_ARG, "stage out of range");
+  if ((rc = materialise_pressure(c))) return rc;
   const bool first = c->nstep == 0;
-  if ((rc = enqueue_stage(c, stage, first ? 1.0 : 1.5, first ? 0.0 : 0.5, c->cur))) return rc;
+  // the staged step runs every stage on its own (the x-inverse writes the pressure)
+  if ((rc = enqueue_stage(c, stage, first ? 1.0 : 1.5, first ? 0.0 : 0.5, c->cur, false))) return rc;
   MHIT_CUDA_TRY(cudaStreamSynchronize(c->st));
   return MHIT_OK;
 }
@@ -1455,6 +1539,23 @@ int mhit_debug_commit_step(mhit_ctx* c) {
   if ((rc = check_ctx(c))) return rc;
   c->cur ^= 1;
   c->nstep++;
+  c->p_lazy = false;
+  return MHIT_OK;
+}
+
+int mhit_debug_set_fused_projection(mhit_ctx* c, int on) {
+  int rc;
+  if ((rc = check_ctx(c))) return rc;
+  if (on != 0 && on != 1) return set_error(MHIT_ERR_ARG, "on must be 0 or 1");
+  MHIT_CUDA_TRY(cudaStreamSynchronize(c->st));
+  c->fuse_xc = on;
+  c->gen++;  // the stage sequence is baked into captured graphs (also the ensemble's)
+  for (int i = 0; i < 2; ++i)
+    if (c->gexec[i]) {
+      cudaGraphExecDestroy(c->gexec[i]);
+      c->gexec[i] = nullptr;
+    }
+  c->graph_built = false;
   return MHIT_OK;
 }
 
@@ -1473,6 +1574,7 @@ int mhit_debug_get_buffer(mhit_ctx* c, int which, double* out) {
   const void* src = nullptr;
   bool typed = false;  // buffer in the Poisson precision
   size_t len = c->n;
+  if (which == MHIT_BUF_P && (rc = materialise_pressure(c))) return rc;
   switch (which) {
     case MHIT_BUF_U: src = c->U[cur]; break;
     case MHIT_BUF_V: src = c->V[cur]; break;
@@ -1480,7 +1582,13 @@ int mhit_debug_get_buffer(mhit_ctx* c, int which, double* out) {
     case MHIT_BUF_UN: src = c->U[nxt]; break;
     case MHIT_BUF_VN: src = c->V[nxt]; break;
     case MHIT_BUF_WN: src = c->W[nxt]; break;
-    case MHIT_BUF_P: src = c->P; typed = true; break;
+    case MHIT_BUF_P:  // incremental: the FP64 pressure of the last projection
+      if (incremental(c)) src = c->P64;
+      else {
+        src = c->P;
+        typed = true;
+      }
+      break;
     case MHIT_BUF_PHI: src = c->PHI[cur]; break;
     case MHIT_BUF_PHIN: src = c->PHI[nxt]; break;
     case MHIT_BUF_RU: src = c->RU; break;
@@ -1674,7 +1782,7 @@ static int ens_enqueue(mhit_ensemble* e, double alpha, double beta, int cur) {
     for (mhit_ctx* c : e->box) {
       cudaStream_t saved = c->st;
       c->st = e->st;
-      rc = enqueue_stage(c, ST_TRACER, alpha, beta, cur);
+      rc = enqueue_stage(c, ST_TRACER, alpha, beta, cur, fused_xc(c));
       c->st = saved;
       if (rc) return rc;
     }
@@ -1701,7 +1809,7 @@ static int ens_enqueue(mhit_ensemble* e, double alpha, double beta, int cur) {
     c->st = e->lanes[b % e->nlanes];
     if (e->batched) MHIT_CUDA_TRY(cudaStreamWaitEvent(c->st, e->cls_done[e->box_cls[b]], 0));
     int rc = MHIT_OK;
-    for (int s = first; s < ST_COUNT && rc == MHIT_OK; ++s) rc = enqueue_stage(c, s, alpha, beta, cur);
+    for (int s = first; s < ST_COUNT && rc == MHIT_OK; ++s) rc = enqueue_stage(c, s, alpha, beta, cur, fused_xc(c));
     c->st = saved;
     if (rc) return rc;
   }
@@ -1755,6 +1863,7 @@ static int ens_enqueue_steps(mhit_ensemble* e, int nsteps) {
     for (mhit_ctx* c : e->box) {
       c->cur ^= 1;
       c->nstep++;
+      c->p_lazy = fused_xc(c);
     }
   }
   return MHIT_OK;

@@ -16,7 +16,7 @@ pytestmark = pytest.mark.gpu
 
 
 def case(n=32, poisson="fp64", **kw):
-    lap = "modified" if poisson == "fp32_refined" else "exact"
+    lap = "modified" if poisson in ("fp32_refined", "fp32_incremental") else "exact"
     prm = Params(nx=n, dt=5e-4, mu=0.006, phiflag=1, partflag=1, radius=0.3, sigma=0.5, poisson=poisson,
                  laplacian=lap, **kw)
     u, v, w = synth.solenoidal_velocity(n, 0)
@@ -33,7 +33,7 @@ def run_straight(prm, u, v, w, phi, part, nsteps):
         return s.download(), s.download_particles(), s.diagnostics()
 
 
-@pytest.mark.parametrize("poisson", ["fp64", "fp32", "fp32_refined"])
+@pytest.mark.parametrize("poisson", ["fp64", "fp32", "fp32_refined", "fp32_incremental"])
 def test_checkpoint_resume_is_bit_exact(gpu, tmp_path, poisson):
     prm, u, v, w, phi, part = case(poisson=poisson)
     ref, ref_part, ref_dg = run_straight(prm, u, v, w, phi, part, 7)
