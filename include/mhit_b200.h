@@ -320,9 +320,10 @@ int mhit_debug_set_label_bound(mhit_ctx* ctx, long long bound);
 int mhit_debug_set_mom_tma(mhit_ctx* ctx, int on);
 /* 1: the inverse x transform runs inside the projection (one pass; the pressure of a step is
  * transformed into its array only when something reads it: a download, a field file, a
- * checkpoint, a debug read, or a call that reuses the spectrum buffer); 0 (the default): the two
- * passes of multi/main.f90:909-912 and :942-1003 run apart.  The refinement sweep always runs
- * them apart.  The results agree to rounding (a test compares). */
+ * checkpoint, a debug read, or a call that reuses the spectrum buffer); 0: the two passes of
+ * multi/main.f90:909-912 and :942-1003 run apart; -1 (the default): fused where it is the faster
+ * (nx = 512).  The refinement sweep always runs them apart.  The results agree to rounding (a
+ * test compares). */
 int mhit_debug_set_fused_projection(mhit_ctx* ctx, int on);
 long long mhit_debug_buffer_len(mhit_ctx* ctx, int which);
 int mhit_debug_get_buffer(mhit_ctx* ctx, int which, double* out);

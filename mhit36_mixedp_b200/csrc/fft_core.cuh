@@ -139,9 +139,18 @@ template <typename T, bool INV, int R> __device__ __forceinline__ void dftR(Cx<T
   else if constexpr (R == 16) dft16<T, INV>(a);
 }
 
+// Barrier of the threads that run a tile transform: the whole block by default; a named
+// barrier (id, count) when only some warps of the block transform (warp-specialised kernels).
+struct SyncBlock {
+  __device__ __forceinline__ static void sync() { __syncthreads(); }
+};
+template <int ID, int COUNT> struct SyncNamed {
+  __device__ __forceinline__ static void sync() { asm volatile("bar.sync %0, %1;" ::"n"(ID), "n"(COUNT) : "memory"); }
+};
+
 // ---------------------------------------------------------------- one Stockham stage
-// tw: table of exp(-2 pi i m / L) for m in [0, L); twstride = L / N.
-template <typename T, int N, int B, int NT, int R, bool INV>
+// tw: table of exp(-2 pi i m / L) for m in [0, L); twstride = L / N.  Threads 0..NT-1 take part.
+template <typename T, int N, int B, int NT, int R, bool INV, typename SY = SyncBlock>
 __device__ __forceinline__ void stockham_stage(Cx<T>* s, const Cx<T>* __restrict__ tw, int twstride, int p) {
   constexpr int NB = N / R * B;
   constexpr int BPT = (NB + NT - 1) / NT;
@@ -156,7 +165,7 @@ __device__ __forceinline__ void stockham_stage(Cx<T>* s, const Cx<T>* __restrict
       for (int r = 0; r < R; ++r) a[m][r] = s[sw<B>(t + r * (N / R), b)];
     }
   }
-  __syncthreads();
+  SY::sync();
 #pragma unroll
   for (int m = 0; m < BPT; ++m) {
     const int q = tid + m * NT;
@@ -179,29 +188,29 @@ __device__ __forceinline__ void stockham_stage(Cx<T>* s, const Cx<T>* __restrict
       for (int r = 0; r < R; ++r) s[sw<B>(j + r * p, b)] = a[m][r];
     }
   }
-  __syncthreads();
+  SY::sync();
 }
 
 // Full transform of the N x B tile in s (unnormalised in both directions, as cuFFT), in the
-// radix schedule S (default Radix<N>).  Caller must __syncthreads() before (tile loaded); returns
-// after a barrier.
-template <typename T, int N, int B, int NT, bool INV, typename S = Radix<N>>
+// radix schedule S (default Radix<N>), by threads 0..NT-1 synchronising with SY.  Caller
+// synchronises before (tile loaded); returns after a barrier.
+template <typename T, int N, int B, int NT, bool INV, typename S = Radix<N>, typename SY = SyncBlock>
 __device__ __forceinline__ void fft_tile(Cx<T>* s, const Cx<T>* __restrict__ tw, int twstride) {
   constexpr int NS = S::ns;
   int p = 1;
   if constexpr (NS >= 1) {
     constexpr int R = S::r[0];
-    stockham_stage<T, N, B, NT, R, INV>(s, tw, twstride, p);
+    stockham_stage<T, N, B, NT, R, INV, SY>(s, tw, twstride, p);
     p *= R;
   }
   if constexpr (NS >= 2) {
     constexpr int R = S::r[1];
-    stockham_stage<T, N, B, NT, R, INV>(s, tw, twstride, p);
+    stockham_stage<T, N, B, NT, R, INV, SY>(s, tw, twstride, p);
     p *= R;
   }
   if constexpr (NS >= 3) {
     constexpr int R = S::r[2];
-    stockham_stage<T, N, B, NT, R, INV>(s, tw, twstride, p);
+    stockham_stage<T, N, B, NT, R, INV, SY>(s, tw, twstride, p);
   }
 }
 

@@ -3,26 +3,37 @@
 //
 // Apart, k_fftx_inv writes the pressure and k_correct reads it back beside u*, v*, w* (the
 // pressure's -x, -y and -z neighbours of each cell).  Here a block owns XO = 7 consecutive y
-// lines of a chunk of z planes and marches up z.  Per plane it
-//   1. has the plane's 8 half-spectrum rows in shared memory (its 7 lines and the line below
-//      them, j0 - 1, the -y neighbour of its first line), fetched by cp.async one plane ahead
-//      into the other of two tile buffers;
-//   2. C2R-transforms the 8 rows in place (the untangle and Stockham stages of k_fftx_inv, so
-//      the pressure values are the same doubles);
+// lines of a chunk of z planes and marches up z.  Per plane the block
+//   1. fetches the plane's 8 half-spectrum rows (its 7 lines and the line below them, j0 - 1,
+//      the -y neighbour of its first line) with cp.async, two planes ahead, into a ring of three
+//      tile buffers in shared memory;
+//   2. C2R-transforms the 8 rows in place (the untangle of k_fftx_inv and Stockham stages in the
+//      XcRadix schedule: the on-demand transform of the same spectrum, k_fftx_inv with that
+//      schedule, gives the same doubles);
 //   3. projects its 7 lines (u -= dt/rho (p - p(i-1)) dxi, and v, w along y, z: :953-955) with
-//      p(i-1) and p(j-1) from the tile and p(k-1) from the thread's registers, which hold the
-//      pressure of its own x pairs at the plane below (the loop starts one plane below the
-//      chunk for them), and accumulates the per-block sums and maxima of k_correct.
-// The pressure never goes to HBM: the library materialises it from the spectrum, which stays
-// intact until the next step's x pass, when something reads it.  Per cell this moves the spectrum
-// once (8/7 of it: the halo line) and u, v, w in and out: 48 + 8 (FP64) or 48 + 4 (FP32) bytes
-// of the 72 / 60 of the two passes.
+//      p(i-1) and p(j-1) from the tile and p(k-1) from registers that hold the pressure of the
+//      thread's own x pairs at the plane below (the loop starts one plane below the chunk for
+//      them), and accumulates the per-block sums and maxima of k_correct.
+// The warps are specialised so the two kinds of work overlap: the transform warps (steps 1-2,
+// synchronising among themselves on named barrier 1) transform plane i while the stream warps
+// (step 3: the u, v, w traffic, deep in loads) project plane i - 1.  A tile buffer passes between
+// them by named barriers: "ready" (2 + buffer: transform warps arrive, stream warps wait) and
+// "free" (5 + buffer: stream warps arrive, transform warps wait before fetching plane i + 2 into
+// the buffer of plane i - 1).  Hardware barriers, no spin loops; every arrival has its matching
+// wait, and a barrier's next phase starts only after its last one completed.
+//
+// The pressure never goes to HBM: the library transforms it from the spectrum, which stays intact
+// until the next step's x pass, when something reads it.  Per cell this moves the spectrum once
+// (8/7 of it, the halo line) and u, v, w in and out: 48 + 8 (FP64) or 48 + 4 (FP32) bytes of the
+// 72 / 60 of the two passes.
 //
 // INC (incremental FP32 solve): the transform is the correction delta; the pressure is
 // qold + delta formed in FP64 (qold, the FP32 predictor, read at the cell and its -x and -y
 // neighbours), and fl32 of it goes to qnew, the next step's predictor (a second buffer, so no
 // block overwrites a predictor another block still reads).
 #include <cuda_pipeline.h>
+
+#include <algorithm>
 
 #include "common.cuh"
 #include "fft_core.cuh"
@@ -32,139 +43,217 @@ namespace mhit {
 
 constexpr int XL = 8;       // lines transformed per plane (a power of two: the tile swizzle)
 constexpr int XO = XL - 1;  // lines projected per plane: tile line 0 is the -y halo
-constexpr int XZC = 16;     // default z planes per block
+constexpr int XZC_MIN = 8;  // fewest z planes per block of the default chunking
+constexpr int XNB = 3;      // tile buffers: loading, transforming, being projected
 
-template <int M> __host__ __device__ constexpr int xc_max_radix() {
-  int m = 0;
-  for (int s = 0; s < XcRadix<M>::ns; ++s) m = XcRadix<M>::r[s] > m ? XcRadix<M>::r[s] : m;
-  return m;
+// transform threads: one radix-8 butterfly each (at most 256: larger tiles loop), at least 64
+template <int M> __host__ __device__ constexpr int xc_nf() { return M >= 256 ? 256 : (M < 64 ? 64 : M); }
+// stream threads: 7 x pairs of the 7 lines each at nx = 512 (all their loads in flight at once:
+// ~86 KB per SM), 14 at nx = 1024
+template <int M> __host__ __device__ constexpr int xc_ns() { return M >= 256 ? 256 : 128; }
+template <int M> __host__ __device__ constexpr int xc_ppt() { return (XO * M + xc_ns<M>() - 1) / xc_ns<M>(); }
+template <typename T, int M> __host__ __device__ constexpr size_t xc_spec_bytes() {
+  return (size_t)XNB * (M + 1) * XL * sizeof(Cx<T>);
+}
+// incremental solve: beside each spectrum tile, the 8 lines of the FP32 predictor (row-major)
+template <typename T, int M, bool INC> __host__ __device__ constexpr size_t xc_tile_bytes() {
+  return xc_spec_bytes<T, M>() + (INC ? (size_t)XNB * XL * 2 * M * sizeof(float) : 0);
+}
+// The pressure each stream thread carries to the next plane (the -z neighbour) lives in shared
+// memory where it fits beside the tiles (in registers it would crowd out the loads in flight),
+// else in registers (FP64 at nx = 1024).
+template <typename T, int M, bool INC> __host__ __device__ constexpr bool xc_pz_shared() {
+  return xc_tile_bytes<T, M, INC>() + (size_t)xc_ns<M>() * xc_ppt<M>() * 16 <= 227 * 1024;
+}
+template <typename T, int M, bool INC> __host__ __device__ constexpr size_t xc_smem() {
+  return xc_tile_bytes<T, M, INC>() + (xc_pz_shared<T, M, INC>() ? (size_t)xc_ns<M>() * xc_ppt<M>() * 16 : 0);
+}
+// x pairs a stream thread loads before computing any of them
+template <typename T, int M, bool INC> __host__ __device__ constexpr int xc_pb() {
+  return xc_pz_shared<T, M, INC>() ? 7 : 2;
 }
 
-// threads: one per x pair of a line (coalesced 16-byte rows), at least one butterfly each
-template <int M> __host__ __device__ constexpr int xc_threads() {
-  return M / xc_max_radix<M>() * XL > M ? M / xc_max_radix<M>() * XL : (M < 64 ? 64 : M);
+__device__ __forceinline__ void bar_sync(int id, int count) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
 }
-
-// resident blocks per SM the register budget is sized for (the tile buffers allow 3 of 256
-// threads in FP64 at nx = 512)
-#ifndef XC_MINB
-#define XC_MINB 2
-#endif
-template <typename T, int M> __host__ __device__ constexpr int xc_minb() {
-  return xc_threads<M>() >= 512 ? 1 : (xc_threads<M>() >= 256 ? XC_MINB : 4);
+__device__ __forceinline__ void bar_arrive(int id, int count) {
+  asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(count) : "memory");
 }
 
 template <typename T, int M, bool INC>
-__global__ void __launch_bounds__(xc_threads<M>(), (xc_minb<T, M>())) k_xinv_correct(const XcArgs a) {
-  constexpr int NT = xc_threads<M>();
+__global__ void __launch_bounds__(xc_nf<M>() + xc_ns<M>(), 1) k_xinv_correct(const XcArgs a) {
+  constexpr int NF = xc_nf<M>(), NS = xc_ns<M>(), NT = NF + NS;
   constexpr int TL = (M + 1) * XL;         // elements of one tile buffer
   constexpr int NP = XO * M;               // x pairs projected per plane
-  constexpr int PPT = (NP + NT - 1) / NT;  // ... per thread
+  constexpr int PPT = xc_ppt<M>();         // ... per stream thread
+  constexpr int XPB = xc_pb<T, M, INC>();
+  constexpr bool PZS = xc_pz_shared<T, M, INC>();
   constexpr int nx = 2 * M;
+  constexpr int QL = XL * nx;              // floats of one predictor tile
   extern __shared__ __align__(16) unsigned char smraw[];
   Cx<T>* tiles = reinterpret_cast<Cx<T>*>(smraw);
+  float* qtiles = reinterpret_cast<float*>(smraw + xc_spec_bytes<T, M>());
   const Geo& g = a.g;
   const int ny = g.ny, nz = g.nz;
-  const size_t plane = (size_t)nx * ny;
-  const int pitch = g.pitch;
   const int j0 = blockIdx.x * XO;
-  const int zc = a.zc;
-  const int k0 = blockIdx.y * zc, k1 = min(k0 + zc, nz);
-  const Cx<T>* __restrict__ spec = static_cast<const Cx<T>*>(a.spec);
-  const Cx<T>* __restrict__ twx = static_cast<const Cx<T>*>(a.twx);
-  double* __restrict__ U = a.u;
-  double* __restrict__ V = a.v;
-  double* __restrict__ W = a.w;
-  const double cc = g.dt / g.rho, dxi = g.dxi;
-
-  // rows j0-1 .. j0+6 of plane k (periodic in y and z; rows past ny in a tail tile wrap and
-  // are transformed but not projected)
-  auto fetch = [&](int k, Cx<T>* s) {
-    const int kk = k < 0 ? k + nz : k;
-    const Cx<T>* src = spec + (size_t)kk * ny * pitch;
-    for (int e = threadIdx.x; e < TL; e += NT) {
-      const int b = e / (M + 1), kx = e - b * (M + 1);
-      int j = j0 - 1 + b;
-      j = j < 0 ? j + ny : (j >= ny ? j - ny : j);
-      __pipeline_memcpy_async(&s[sw<XL>(kx, b)], &src[(size_t)j * pitch + kx], sizeof(Cx<T>));
-    }
-    __pipeline_commit();
-  };
-
-  double pz[PPT][2];  // pressure of the thread's x pairs at the plane below
+  const int k0 = blockIdx.y * a.zc, k1 = min(k0 + a.zc, nz);
+  const int nplanes = k1 - k0 + 1;  // with the plane below the chunk
+  const int tid = threadIdx.x;
   double su = 0.0, sv = 0.0, sw_ = 0.0;
   double mu = -INFINITY, mv = -INFINITY, mw = -INFINITY;
-  fetch(k0 - 1, tiles);
-  int it = 0;
-  for (int k = k0 - 1; k < k1; ++k, ++it) {
-    Cx<T>* s = tiles + (it & 1) * TL;
-    __pipeline_wait_prior(0);
-    __syncthreads();  // plane k's tile is complete; no thread still reads the other buffer
-    if (k + 1 < k1) fetch(k + 1, tiles + ((it + 1) & 1) * TL);
-    c2r_untangle<T, M, XL, NT>(s, twx);
-    __syncthreads();
-    fft_tile<T, M, XL, NT, true, XcRadix<M>>(s, twx, 2);  // returns after a barrier
-    const int kk = k < 0 ? k + nz : k;
-    const bool out = k >= k0;
-#pragma unroll
-    for (int m = 0; m < PPT; ++m) {
-      const int e = threadIdx.x + m * NT;
-      if (NP % NT == 0 || e < NP) {
-        const int l = e / M, n = e - l * M;  // output line l = tile line l + 1
-        const int j = j0 + l;
-        const Cx<T> z = s[sw<XL>(n, l + 1)];
-        const T zxm = s[sw<XL>(n == 0 ? M - 1 : n - 1, l + 1)].y;
-        const Cx<T> zy = s[sw<XL>(n, l)];
-        double p0, p1, pxm, py0, py1;
-        if constexpr (INC) {
-          const int jj = j < ny ? j : j - ny;
-          const int jm = jj == 0 ? ny - 1 : jj - 1;
-          const float* q = a.qold + (size_t)kk * plane;
-          const float2 qc = __ldg(reinterpret_cast<const float2*>(q + (size_t)jj * nx + 2 * n));
-          const float qx = __ldg(q + (size_t)jj * nx + (n == 0 ? nx - 1 : 2 * n - 1));
-          const float2 qy = __ldg(reinterpret_cast<const float2*>(q + (size_t)jm * nx + 2 * n));
-          // the sums k_fftx_inv forms for the FP64 pressure (same doubles)
-          p0 = (double)qc.x + (double)z.x;
-          p1 = (double)qc.y + (double)z.y;
-          pxm = (double)qx + (double)zxm;
-          py0 = (double)qy.x + (double)zy.x;
-          py1 = (double)qy.y + (double)zy.y;
-        } else {
-          p0 = (double)z.x;
-          p1 = (double)z.y;
-          pxm = (double)zxm;
-          py0 = (double)zy.x;
-          py1 = (double)zy.y;
+
+  if (tid < NF) {
+    // ---------------------------------------------------------- transform warps
+    const Cx<T>* __restrict__ spec = static_cast<const Cx<T>*>(a.spec);
+    const Cx<T>* __restrict__ twx = static_cast<const Cx<T>*>(a.twx);
+    const int pitch = g.pitch;
+    // rows j0-1 .. j0+6 of plane index i (plane k0 - 1 + i, periodic in y and z; rows past ny in
+    // a tail tile wrap and are transformed but not projected)
+    auto fetch = [&](int i) {
+      int kk = k0 - 1 + i;
+      kk = kk < 0 ? kk + nz : kk;
+      const Cx<T>* src = spec + (size_t)kk * ny * pitch;
+      Cx<T>* s = tiles + (i % XNB) * TL;
+      for (int e = tid; e < TL; e += NF) {
+        const int b = e / (M + 1), kx = e - b * (M + 1);
+        int j = j0 - 1 + b;
+        j = j < 0 ? j + ny : (j >= ny ? j - ny : j);
+        __pipeline_memcpy_async(&s[sw<XL>(kx, b)], &src[(size_t)j * pitch + kx], sizeof(Cx<T>));
+      }
+      if constexpr (INC) {
+        // the same 8 lines of the predictor, 16-byte chunks (a line is nx floats, nx % 4 == 0)
+        const float* qsrc = a.qold + (size_t)kk * ny * nx;
+        float* qs = qtiles + (i % XNB) * QL;
+        for (int e = tid; e < QL / 4; e += NF) {
+          const int b = e / (nx / 4), c4 = e - b * (nx / 4);
+          int j = j0 - 1 + b;
+          j = j < 0 ? j + ny : (j >= ny ? j - ny : j);
+          __pipeline_memcpy_async(&qs[b * nx + 4 * c4], &qsrc[(size_t)j * nx + 4 * c4], 16);
         }
-        if (out && j < ny) {
-          const size_t o = (size_t)kk * plane + (size_t)j * nx + 2 * n;
-          const double2 uo = *reinterpret_cast<const double2*>(U + o);
-          const double2 vo = *reinterpret_cast<const double2*>(V + o);
-          const double2 wo = *reinterpret_cast<const double2*>(W + o);
-          // multi/main.f90:953-955, the expressions of k_correct
-          const double u0 = uo.x - cc * (p0 - pxm) * dxi, u1 = uo.y - cc * (p1 - p0) * dxi;
-          const double v0 = vo.x - cc * (p0 - py0) * dxi, v1 = vo.y - cc * (p1 - py1) * dxi;
-          const double w0 = wo.x - cc * (p0 - pz[m][0]) * dxi, w1 = wo.y - cc * (p1 - pz[m][1]) * dxi;
-          *reinterpret_cast<double2*>(U + o) = make_double2(u0, u1);
-          *reinterpret_cast<double2*>(V + o) = make_double2(v0, v1);
-          *reinterpret_cast<double2*>(W + o) = make_double2(w0, w1);
-          if constexpr (INC) *reinterpret_cast<float2*>(a.qnew + o) = make_float2((float)p0, (float)p1);
-          su += u0 + u1;
-          sv += v0 + v1;
-          sw_ += w0 + w1;
-          mu = fmax(mu, fmax(u0, u1));
-          mv = fmax(mv, fmax(v0, v1));
-          mw = fmax(mw, fmax(w0, w1));
-        }
-        pz[m][0] = p0;
-        pz[m][1] = p1;
+      }
+      __pipeline_commit();
+    };
+    fetch(0);
+    if (nplanes > 1) fetch(1);
+    for (int i = 0; i < nplanes; ++i) {
+      Cx<T>* s = tiles + (i % XNB) * TL;
+      if (i + 1 < nplanes) __pipeline_wait_prior(1);  // plane i's rows (plane i+1's may still fly)
+      else __pipeline_wait_prior(0);
+      bar_sync(1, NF);
+      c2r_untangle<T, M, XL, NF>(s, twx);
+      bar_sync(1, NF);
+      fft_tile<T, M, XL, NF, true, XcRadix<M>, SyncNamed<1, NF>>(s, twx, 2);
+      bar_arrive(2 + i % XNB, NT);  // plane i's pressure is in its buffer
+      if (i + 2 < nplanes) {
+        // the buffer of plane i + 2 held plane i - 1: wait until the stream warps are done with it
+        if (i >= 1) bar_sync(5 + (i - 1) % XNB, NT);
+        fetch(i + 2);
       }
     }
+  } else {
+    // ---------------------------------------------------------- stream warps
+    const int st = tid - NF;
+    const size_t plane = (size_t)nx * ny;
+    double* __restrict__ U = a.u;
+    double* __restrict__ V = a.v;
+    double* __restrict__ W = a.w;
+    const double cc = g.dt / g.rho, dxi = g.dxi;
+    // pressure of the thread's x pairs at the plane below: [pair][stream thread] in shared memory
+    // after the tiles (each thread its own 16-byte slots: conflict-free), or in registers
+    double2* pzs = reinterpret_cast<double2*>(smraw + xc_tile_bytes<T, M, INC>()) + st;
+    double2 pzr[PZS ? 1 : PPT] = {};
+    auto pz_get = [&](int m) -> double2 {
+      if constexpr (PZS) return pzs[m * NS];
+      else return pzr[m];
+    };
+    auto pz_set = [&](int m, double2 v) {
+      if constexpr (PZS) pzs[m * NS] = v;
+      else pzr[m] = v;
+    };
+    for (int i = 0; i < nplanes; ++i) {
+      const Cx<T>* s = tiles + (i % XNB) * TL;
+      const float* qs = qtiles + (i % XNB) * QL;
+      const int k = k0 - 1 + i;
+      const int kk = k < 0 ? k + nz : k;
+      bar_sync(2 + i % XNB, NT);  // plane i's pressure (and predictor rows) are ready
+#pragma unroll
+      for (int m0 = 0; m0 < PPT; m0 += XPB) {
+        // the batch's loads first (u, v, w of up to XPB pairs in flight per thread), then the math
+        double2 uo[XPB], vo[XPB], wo[XPB];
+#pragma unroll
+        for (int mb = 0; mb < XPB && m0 + mb < PPT; ++mb) {
+          const int e = st + (m0 + mb) * NS;
+          if (NP % NS == 0 || e < NP) {
+            const int l = e / M, n = e - l * M;
+            const int j = j0 + l;
+            if (i > 0 && j < ny) {
+              const size_t o = (size_t)kk * plane + (size_t)j * nx + 2 * n;
+              uo[mb] = *reinterpret_cast<const double2*>(U + o);
+              vo[mb] = *reinterpret_cast<const double2*>(V + o);
+              wo[mb] = *reinterpret_cast<const double2*>(W + o);
+            }
+          }
+        }
+#pragma unroll
+        for (int mb = 0; mb < XPB && m0 + mb < PPT; ++mb) {
+          const int m = m0 + mb;
+          const int e = st + m * NS;
+          if (NP % NS == 0 || e < NP) {
+            const int l = e / M, n = e - l * M;  // output line l = tile line l + 1
+            const int j = j0 + l;
+            const Cx<T> z = s[sw<XL>(n, l + 1)];
+            const T zxm = s[sw<XL>(n == 0 ? M - 1 : n - 1, l + 1)].y;
+            const Cx<T> zy = s[sw<XL>(n, l)];
+            double p0, p1, pxm, py0, py1;
+            if constexpr (INC) {
+              // the sums k_fftx_inv forms for the FP64 pressure (same doubles), the predictor at the
+              // cell pair and its -x and -y neighbours from the tile's predictor rows
+              const float2 qc = *reinterpret_cast<const float2*>(qs + (l + 1) * nx + 2 * n);
+              const float qx = qs[(l + 1) * nx + (n == 0 ? nx - 1 : 2 * n - 1)];
+              const float2 qy = *reinterpret_cast<const float2*>(qs + l * nx + 2 * n);
+              p0 = (double)qc.x + (double)z.x;
+              p1 = (double)qc.y + (double)z.y;
+              pxm = (double)qx + (double)zxm;
+              py0 = (double)qy.x + (double)zy.x;
+              py1 = (double)qy.y + (double)zy.y;
+            } else {
+              p0 = (double)z.x;
+              p1 = (double)z.y;
+              pxm = (double)zxm;
+              py0 = (double)zy.x;
+              py1 = (double)zy.y;
+            }
+            if (i > 0 && j < ny) {
+              const size_t o = (size_t)kk * plane + (size_t)j * nx + 2 * n;
+              // multi/main.f90:953-955, the expressions of k_correct
+              const double u0 = uo[mb].x - cc * (p0 - pxm) * dxi, u1 = uo[mb].y - cc * (p1 - p0) * dxi;
+              const double v0 = vo[mb].x - cc * (p0 - py0) * dxi, v1 = vo[mb].y - cc * (p1 - py1) * dxi;
+              const double2 pk = pz_get(m);
+              const double w0 = wo[mb].x - cc * (p0 - pk.x) * dxi, w1 = wo[mb].y - cc * (p1 - pk.y) * dxi;
+              *reinterpret_cast<double2*>(U + o) = make_double2(u0, u1);
+              *reinterpret_cast<double2*>(V + o) = make_double2(v0, v1);
+              *reinterpret_cast<double2*>(W + o) = make_double2(w0, w1);
+              if constexpr (INC) *reinterpret_cast<float2*>(a.qnew + o) = make_float2((float)p0, (float)p1);
+              su += u0 + u1;
+              sv += v0 + v1;
+              sw_ += w0 + w1;
+              mu = fmax(mu, fmax(u0, u1));
+              mv = fmax(mv, fmax(v0, v1));
+              mw = fmax(mw, fmax(w0, w1));
+            }
+            pz_set(m, make_double2(p0, p1));
+          }
+        }
+      }
+      // the transform warps wait for this buffer only if they fetch plane i + 3 into it
+      if (i + 3 < nplanes) bar_arrive(5 + i % XNB, NT);
+    }
   }
-  // block reduction (fixed tree, as k_correct)
+  // block reduction (fixed tree, as k_correct; the transform warps add the identities)
+  __syncthreads();
   __shared__ double red[6][NT / 32];
   double vals[6] = {su, sv, sw_, mu, mv, mw};
-  const int t = threadIdx.x, lane = t & 31;
+  const int lane = tid & 31;
 #pragma unroll
   for (int q = 0; q < 6; ++q) {
     double x = vals[q];
@@ -173,20 +262,27 @@ __global__ void __launch_bounds__(xc_threads<M>(), (xc_minb<T, M>())) k_xinv_cor
       const double y = __shfl_down_sync(0xffffffffu, x, o);
       x = q < 3 ? x + y : fmax(x, y);
     }
-    if (lane == 0) red[q][t >> 5] = x;
+    if (lane == 0) red[q][tid >> 5] = x;
   }
   __syncthreads();
-  if (t < 6) {
-    double x = red[t][0];
-    for (int wv = 1; wv < NT / 32; ++wv) x = t < 3 ? x + red[t][wv] : fmax(x, red[t][wv]);
+  if (tid < 6) {
+    double x = red[tid][0];
+    for (int wv = 1; wv < NT / 32; ++wv) x = tid < 3 ? x + red[tid][wv] : fmax(x, red[tid][wv]);
     const size_t bid = (size_t)blockIdx.y * gridDim.x + blockIdx.x;
-    a.partials[bid * 6 + t] = x;
+    a.partials[bid * 6 + tid] = x;
   }
 }
 
+// z planes per block: by default as many as make the grid one wave of one block per SM (148 on
+// a B200; at 512^3 the 74 columns of 7 lines times 2 halves of z), so each block fills its
+// transform-to-stream pipeline once for a long run of planes
 static int xc_chunk(const Geo& g, int zc) {
-  const int c = zc > 0 ? zc : XZC;
-  return c < g.nz ? c : g.nz;
+  if (zc <= 0) {
+    const int ncols = (g.ny + XO - 1) / XO;
+    const int per = std::max(1, 148 / ncols);
+    zc = std::max(XZC_MIN, (g.nz + per - 1) / per);
+  }
+  return zc < g.nz ? zc : g.nz;
 }
 
 static dim3 xc_grid(const Geo& g, int zc) {
@@ -201,9 +297,13 @@ int xc_blocks(const Geo& g, int zc) {
 
 template <typename T, int M>
 static cudaError_t launch_xc_m(const XcArgs& a, cudaStream_t st) {
-  constexpr int NT = xc_threads<M>();
-  const size_t smem = 2 * (size_t)(M + 1) * XL * sizeof(Cx<T>);
-  auto kern = a.qold ? k_xinv_correct<T, M, true> : k_xinv_correct<T, M, false>;
+  constexpr int NT = xc_nf<M>() + xc_ns<M>();
+  // the incremental solve is an FP32 mode: its variant exists for float tiles only
+  constexpr bool HAS_INC = sizeof(T) == 4;
+  static_assert(xc_smem<T, M, false>() <= 227 * 1024 && (!HAS_INC || xc_smem<T, M, HAS_INC>() <= 227 * 1024),
+                "tiles exceed the shared memory of a block");
+  const size_t smem = a.qold ? xc_smem<T, M, HAS_INC>() : xc_smem<T, M, false>();
+  auto kern = a.qold ? k_xinv_correct<T, M, HAS_INC> : k_xinv_correct<T, M, false>;
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;

@@ -96,11 +96,13 @@ struct mhit_ctx {
   CUtensorMap tm_u[2], tm_v[2], tm_w[2], tm_phi[2];  // k_mom's ring boxes over U, V, W, PHI[0..1]
   int mom_tma = 1;                        // k_mom fills its interior rings by TMA (test hook: 0)
   int graph_kernels = 0;                  // kernel nodes in a captured step graph
-  // 1: the inverse x transform runs fused with the projection (k_xinv_correct); 0 (the default,
-  // the faster today): k_fftx_inv + k_correct.  The fused pass leaves the pressure in the spectrum
-  // only: after such a step p_lazy is set, and whatever reads the pressure or reuses the spectrum
-  // first materialises it (materialise_pressure).
-  int fuse_xc = 0;
+  // 1: the inverse x transform runs fused with the projection (k_xinv_correct); 0: k_fftx_inv +
+  // k_correct; -1 (the default): fused where that is the faster, nx = 512 (measured at 512^3:
+  // FP64 pass pair 1.63 against 1.77 ms; at 1024^3, where k_correct streams at 96% of the copy
+  // peak, and on the small boxes of the ensemble the separate passes are faster).  The fused
+  // pass leaves the pressure in the spectrum only: after such a step p_lazy is set, and whatever
+  // reads the pressure or reuses the spectrum first materialises it (materialise_pressure).
+  int fuse_xc = -1;
   bool p_lazy = false;
   int nblk_xc = 0;                        // blocks of k_xinv_correct (partials rows)
 };
@@ -111,7 +113,10 @@ static bool refined(const mhit_ctx* c) { return c->prm.poisson == MHIT_POISSON_F
 static bool incremental(const mhit_ctx* c) { return c->prm.poisson == MHIT_POISSON_FP32_INCREMENTAL; }
 // the step's inverse x transform runs inside the projection (every mode but the refinement sweep,
 // whose projection reads the sum of two pressures)
-static bool fused_xc(const mhit_ctx* c) { return c->fuse_xc && !refined(c); }
+static bool fused_xc(const mhit_ctx* c) {
+  if (refined(c)) return false;
+  return c->fuse_xc >= 0 ? c->fuse_xc != 0 : c->g.nx == 512;
+}
 
 static int check_ctx(mhit_ctx* c) {
   if (!c) return set_error(MHIT_ERR_ARG, "null context");
@@ -1546,7 +1551,7 @@ int mhit_debug_commit_step(mhit_ctx* c) {
 int mhit_debug_set_fused_projection(mhit_ctx* c, int on) {
   int rc;
   if ((rc = check_ctx(c))) return rc;
-  if (on != 0 && on != 1) return set_error(MHIT_ERR_ARG, "on must be 0 or 1");
+  if (on < -1 || on > 1) return set_error(MHIT_ERR_ARG, "on must be -1, 0 or 1");
   MHIT_CUDA_TRY(cudaStreamSynchronize(c->st));
   c->fuse_xc = on;
   c->gen++;  // the stage sequence is baked into captured graphs (also the ensemble's)
