@@ -33,7 +33,13 @@
 
 namespace mhit {
 
-constexpr int PTX = 32, PTY = 16;            // output cells per block in x, y
+#ifndef MHIT_PHASE_TX
+#define MHIT_PHASE_TX 32
+#define MHIT_PHASE_TY 16
+#define MHIT_PHASE_MINB 1
+#endif
+constexpr int PTX = MHIT_PHASE_TX, PTY = MHIT_PHASE_TY;  // output cells per block in x, y
+constexpr int PMINB = MHIT_PHASE_MINB;                   // resident blocks per SM
 constexpr int PHX = PTX + 4, PHY = PTY + 4;  // positions with the halo of 2
 constexpr int PNT = PHX * PHY;               // threads per block = positions
 constexpr int PNI = PTX * PTY;               // output cells
@@ -227,7 +233,7 @@ __device__ __forceinline__ void phase_tile(const PhaseArgs& a, double dta, doubl
 }
 
 template <bool CLAMP>
-__global__ void __launch_bounds__(PNT, 1) k_phase(const __grid_constant__ PhaseArgs a) {
+__global__ void __launch_bounds__(PNT, PMINB) k_phase(const __grid_constant__ PhaseArgs a) {
   extern __shared__ __align__(16) unsigned char smraw[];
   phase_tile<CLAMP>(a, a.dta, a.dtb, blockIdx.x, blockIdx.y, blockIdx.z, smraw);
 }
@@ -237,7 +243,7 @@ __global__ void __launch_bounds__(PNT, 1) k_phase(const __grid_constant__ PhaseA
 // (including its resolved z chunk) come from b.args; alpha, beta are the step's.  The boxes of
 // one launch share the psi clamp (CLAMP).
 template <bool CLAMP>
-__global__ void __launch_bounds__(PNT, 1) k_phase_batch(const __grid_constant__ BatchArgs<PhaseArgs> b) {
+__global__ void __launch_bounds__(PNT, PMINB) k_phase_batch(const __grid_constant__ BatchArgs<PhaseArgs> b) {
   extern __shared__ __align__(16) unsigned char smraw[];
   __shared__ int s_item;
   for (;;) {
