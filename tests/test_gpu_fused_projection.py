@@ -14,8 +14,9 @@ it.  The test hook ``mhit_debug_set_fused_projection(ctx, 0)`` runs the two pass
   against the oracle: the first steps' FP32 solves carry rounding of the whole pressure).  The
   projected divergence must be as small either way.
   For every Poisson mode that fuses (FP64, FP32, incremental FP32), on cubic and non-cubic boxes
-  whose ny is not a multiple of the fused pass's 7 lines per block (tail blocks), and at 256^3,
-  the production tile shapes.
+  whose ny is not a multiple of the fused pass's 7 lines per block (tail blocks), at nx = 192 (the
+  radix-3 schedule) and nx = 1024 (the pressure carried in registers instead of shared memory),
+  and at 256^3, the production tile shapes.
 * The pressure must be the one the projection used: a download after a step equals a download
   after a call that reuses the spectrum (droplet labelling, energy spectrum) and after a second
   download, bit for bit.
@@ -67,7 +68,7 @@ def run(shape, poisson, fused, nsteps=4):
 
 
 @pytest.mark.parametrize("poisson", ["fp64", "fp32", "fp32_incremental"])
-@pytest.mark.parametrize("shape", [(64, 64, 64), (32, 16, 64), (64, 192, 32)])
+@pytest.mark.parametrize("shape", [(64, 64, 64), (32, 16, 64), (64, 192, 32), (192, 32, 16), (1024, 16, 16)])
 def test_fused_matches_separate_passes(gpu, shape, poisson):
     check(shape, poisson, 4)
 
