@@ -131,12 +131,46 @@ template <typename T, bool INV> __device__ __forceinline__ void dft16(Cx<T>* a) 
   }
 }
 
+template <typename T, bool INV> __device__ __forceinline__ void dft32(Cx<T>* a) {
+  // 32 = 2 x 16: the 16-point DFTs of the even and odd elements, the odd half times
+  // w32^k = exp(-+ 2 pi i k/32) = cos(pi k/16) -+ i sin(pi k/16), then one radix-2 step
+  constexpr double C1 = 0.980785280403230449126182236134, C2 = 0.923879532511286756128183189397,
+                   C3 = 0.831469612302545237078788377618, C4 = 0.707106781186547524400844362105,
+                   C5 = 0.555570233019602224742830813949, C6 = 0.382683432365089771728459984030,
+                   C7 = 0.195090322016128267848284868477;
+  const T cs[16] = {(T)1.0, (T)C1, (T)C2, (T)C3, (T)C4, (T)C5, (T)C6, (T)C7,
+                    (T)0.0, (T)-C7, (T)-C6, (T)-C5, (T)-C4, (T)-C3, (T)-C2, (T)-C1};
+  const T sn[16] = {(T)0.0, (T)C7, (T)C6, (T)C5, (T)C4, (T)C3, (T)C2, (T)C1,
+                    (T)1.0, (T)C1, (T)C2, (T)C3, (T)C4, (T)C5, (T)C6, (T)C7};
+  Cx<T> e[16], o[16];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    e[k] = a[2 * k];
+    o[k] = a[2 * k + 1];
+  }
+  dft16<T, INV>(e);
+  dft16<T, INV>(o);
+  const T sg = INV ? (T)1 : (T)-1;
+#pragma unroll
+  for (int k = 1; k < 16; ++k) {
+    const T ck = cs[k], sk = sg * sn[k];
+    o[k] = cx<T>(o[k].x * ck - o[k].y * sk, o[k].x * sk + o[k].y * ck);
+  }
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    const Cx<T> t = o[k];
+    a[k] = e[k] + t;
+    a[k + 16] = e[k] - t;
+  }
+}
+
 template <typename T, bool INV, int R> __device__ __forceinline__ void dftR(Cx<T>* a) {
   if constexpr (R == 2) dft2<T, INV>(a);
   else if constexpr (R == 3) dft3<T, INV>(a);
   else if constexpr (R == 4) dft4<T, INV>(a);
   else if constexpr (R == 8) dft8<T, INV>(a);
   else if constexpr (R == 16) dft16<T, INV>(a);
+  else if constexpr (R == 32) dft32<T, INV>(a);
 }
 
 // Barrier of the threads that run a tile transform: the whole block by default; a named
@@ -252,14 +286,17 @@ __device__ __forceinline__ void c2r_untangle(Cx<T>* s, const Cx<T>* __restrict__
 // The first stage (p = 1) therefore reads, and the last stage (p = N/R) writes, the strided
 // set t + r N/R: those two stages can take their operands from, and leave their results in,
 // registers, so a tile loaded from (stored to) global memory skips a shared-memory pass.
-template <int N, bool REV> __host__ __device__ constexpr int rad(int s) {
-  return REV ? Radix<N>::r[Radix<N>::ns - 1 - s] : Radix<N>::r[s];
+// Radix of stage s, and the product of the earlier radices, of the schedule S (Radix<N>-like)
+template <typename S, bool REV> __host__ __device__ constexpr int srad(int s) {
+  return REV ? S::r[S::ns - 1 - s] : S::r[s];
 }
-template <int N, bool REV> __host__ __device__ constexpr int pbefore(int s) {
+template <typename S, bool REV> __host__ __device__ constexpr int spbefore(int s) {
   int p = 1;
-  for (int i = 0; i < s; ++i) p *= rad<N, REV>(i);
+  for (int i = 0; i < s; ++i) p *= srad<S, REV>(i);
   return p;
 }
+template <int N, bool REV> __host__ __device__ constexpr int rad(int s) { return srad<Radix<N>, REV>(s); }
+template <int N, bool REV> __host__ __device__ constexpr int pbefore(int s) { return spbefore<Radix<N>, REV>(s); }
 template <int N, int B, int NT, int R> struct StageShape {
   static constexpr int NB = N / R * B;
   static constexpr int BPT = (NB + NT - 1) / NT;
@@ -319,13 +356,13 @@ __device__ __forceinline__ void st_write(Cx<T>* s, const Cx<T> (&a)[StageShape<N
 // t + r N/R0), `out` receives the last stage's results (elements t + r N/R_last).  s is used
 // between stages; on entry no thread may still be reading s, and on return threads may still
 // be reading it (the caller synchronises before writing s again).
-template <typename T, int N, int B, int NT, bool INV, bool REV>
+template <typename T, int N, int B, int NT, bool INV, bool REV, typename S = Radix<N>>
 __device__ __forceinline__ void fft_regs(
     Cx<T>* s, const Cx<T>* __restrict__ tw, int twstride,
-    Cx<T> (&in)[StageShape<N, B, NT, rad<N, REV>(0)>::BPT][rad<N, REV>(0)],
-    Cx<T> (&out)[StageShape<N, B, NT, rad<N, REV>(Radix<N>::ns - 1)>::BPT][rad<N, REV>(Radix<N>::ns - 1)]) {
-  constexpr int NS = Radix<N>::ns;
-  constexpr int R0 = rad<N, REV>(0);
+    Cx<T> (&in)[StageShape<N, B, NT, srad<S, REV>(0)>::BPT][srad<S, REV>(0)],
+    Cx<T> (&out)[StageShape<N, B, NT, srad<S, REV>(S::ns - 1)>::BPT][srad<S, REV>(S::ns - 1)]) {
+  constexpr int NS = S::ns;
+  constexpr int R0 = srad<S, REV>(0);
   st_compute<T, N, B, NT, R0, INV>(in, tw, twstride, 1);
   if constexpr (NS == 1) {
 #pragma unroll
@@ -336,17 +373,17 @@ __device__ __forceinline__ void fft_regs(
     st_write<T, N, B, NT, R0>(s, in, 1);
     __syncthreads();
     if constexpr (NS == 3) {
-      constexpr int R1 = rad<N, REV>(1);
+      constexpr int R1 = srad<S, REV>(1);
       Cx<T> a1[StageShape<N, B, NT, R1>::BPT][R1];
       st_read<T, N, B, NT, R1>(s, a1);
       __syncthreads();
-      st_compute<T, N, B, NT, R1, INV>(a1, tw, twstride, pbefore<N, REV>(1));
-      st_write<T, N, B, NT, R1>(s, a1, pbefore<N, REV>(1));
+      st_compute<T, N, B, NT, R1, INV>(a1, tw, twstride, spbefore<S, REV>(1));
+      st_write<T, N, B, NT, R1>(s, a1, spbefore<S, REV>(1));
       __syncthreads();
     }
-    constexpr int RL = rad<N, REV>(NS - 1);
+    constexpr int RL = srad<S, REV>(NS - 1);
     st_read<T, N, B, NT, RL>(s, out);
-    st_compute<T, N, B, NT, RL, INV>(out, tw, twstride, pbefore<N, REV>(NS - 1));
+    st_compute<T, N, B, NT, RL, INV>(out, tw, twstride, spbefore<S, REV>(NS - 1));
   }
 }
 

@@ -14,6 +14,8 @@
 // exp(-2 pi i k/nx) twiddles (and the mirror image for C2R).
 #include <cuda_pipeline.h>
 
+#include <type_traits>
+
 #include "common.cuh"
 #include "fft_core.cuh"
 #include "kernels.h"
@@ -220,21 +222,52 @@ k_fftx_inv(const Cx<T>* __restrict__ spec, T* __restrict__ p, const Cx<T>* __res
 // 0.551 ms, 4 columns 0.68 ms.  The FP64 512-point z solve runs 4-column tiles (64-byte rows)
 // of 256 threads, two blocks per SM, so one block's loads overlap the other's butterflies:
 // 0.865 ms against 0.97 ms for one 8-column block of 512 threads per SM (2 columns: 1.24 ms).
+// Radix schedule of the FP32 512-point y passes: 16 x 32 with 128 threads (two radix-16 and one
+// radix-32 butterfly per thread, four blocks per SM), one shared-memory round trip per transform
+// instead of two for 8 x 8 x 8: y passes 0.222 / 0.231 against 0.269 / 0.271 ms at 512^3 (with
+// 256 threads, half of them idle in the 32-point stage: 0.237 / 0.246).  The z solve keeps
+// 8 x 8 x 8: 16 x 32 holds two transforms' registers across the divide and spills (0.63 against
+// 0.57 ms with 128 threads; 0.81 ms with 256, half of them idle in the 32-point stages).
+#ifndef MHIT_COL32_NT
+#define MHIT_COL32_NT 128
+#endif
+#ifndef MHIT_COL32_Z
+#define MHIT_COL32_Z 0
+#endif
+struct ColRadix512f { static constexpr int ns = 2; static constexpr int r[3] = {16, 32, 0}; };
+template <typename T, int N, int MODE> struct ColSched {
+  using S = Radix<N>;
+  static constexpr int NT = fft_threads<N, 8>();
+  static constexpr int MINB = 2;
+};
+#if MHIT_COL32_NT
+template <int MODE> struct ColSched<float, 512, MODE> {
+  static constexpr bool Y = MODE != 2 || MHIT_COL32_Z;
+  using S = std::conditional_t<Y, ColRadix512f, Radix<512>>;
+  static constexpr int NT = Y ? MHIT_COL32_NT : fft_threads<512, 8>();
+  static constexpr int MINB = Y ? 1024 / (2 * MHIT_COL32_NT) : 2;
+};
+#endif
+
 template <typename T, int N, int MODE> struct ColTile {
   static constexpr bool Z64 = MODE == 2 && N == 512 && sizeof(T) == 8;
   static constexpr int B = Z64 ? 4 : 8;
-  static constexpr int MINB = Z64 ? 2 : ((N >= 1024 || (MODE == 2 && sizeof(T) == 8)) ? 1 : 2);
+  static constexpr int NT = Z64 ? fft_threads<N, 4>() : ColSched<T, N, MODE>::NT;
+  static constexpr int MINB =
+      Z64 ? 2 : ((N >= 1024 || (MODE == 2 && sizeof(T) == 8)) ? 1 : ColSched<T, N, MODE>::MINB);
+  using S = typename ColSched<T, N, MODE>::S;
 };
 
 template <typename T, int N, int MODE>
-__global__ void __launch_bounds__(fft_threads<N, ColTile<T, N, MODE>::B>(), ColTile<T, N, MODE>::MINB)
+__global__ void __launch_bounds__(ColTile<T, N, MODE>::NT, ColTile<T, N, MODE>::MINB)
 k_fft_cols(Cx<T>* __restrict__ spec, const Cx<T>* __restrict__ tw, Geo g, size_t stride_n,
            size_t stride_outer, const double* __restrict__ k2x, const double* __restrict__ k2y,
            const double* __restrict__ k2z, double ntot) {
   constexpr int B = ColTile<T, N, MODE>::B;
-  constexpr int NT = fft_threads<N, B>();
-  constexpr int NS = Radix<N>::ns;
-  constexpr int RA = rad<N, false>(0), RL = rad<N, false>(NS - 1);
+  constexpr int NT = ColTile<T, N, MODE>::NT;
+  using S = typename ColTile<T, N, MODE>::S;
+  constexpr int NS = S::ns;
+  constexpr int RA = srad<S, false>(0), RL = srad<S, false>(NS - 1);
   constexpr int BA = StageShape<N, B, NT, RA>::BPT, BL = StageShape<N, B, NT, RL>::BPT;
   extern __shared__ __align__(16) unsigned char smraw[];
   Cx<T>* s = reinterpret_cast<Cx<T>*>(smraw);
@@ -254,7 +287,7 @@ k_fft_cols(Cx<T>* __restrict__ spec, const Cx<T>* __restrict__ tw, Geo g, size_t
     }
   }
   Cx<T> z[BL][RL];
-  fft_regs<T, N, B, NT, MODE == 1, false>(s, tw, 1, a, z);
+  fft_regs<T, N, B, NT, MODE == 1, false, S>(s, tw, 1, a, z);
   if constexpr (MODE == 2) {
     // multi/main.f90:889-895: phi3d = -phi3d/k2/(nx*ny*nz) in FP64, phi3d(1,1,1) = 0.
     // One reciprocal of k2*N per element (within 2 ulp of the reference's two divides).
@@ -279,7 +312,7 @@ k_fft_cols(Cx<T>* __restrict__ spec, const Cx<T>* __restrict__ tw, Geo g, size_t
       }
     }
     __syncthreads();  // every thread has read the forward transform's last stage
-    fft_regs<T, N, B, NT, true, true>(s, tw, 1, z, a);
+    fft_regs<T, N, B, NT, true, true, S>(s, tw, 1, z, a);
 #pragma unroll
     for (int m = 0; m < BA; ++m) {
       if (st_valid<N, B, NT, RA>(m)) {
@@ -395,7 +428,7 @@ static cudaError_t launch_cols_n(const PoissonArgs& a, int axis, cudaStream_t st
   // 0.072 ms FP32, 0.105 vs 0.117 ms FP64); every other pass and size register-staged
   constexpr bool staged = MODE == 2 && N == 256;
   constexpr int B = staged ? Tile<T>::B : ColTile<T, N, MODE>::B;
-  constexpr int NT = fft_threads<N, B>();
+  constexpr int NT = staged ? fft_threads<N, B>() : ColTile<T, N, MODE>::NT;
   const size_t smem = (size_t)N * B * sizeof(Cx<T>);
   auto kern = staged ? k_fft_cols_smem<T, N, MODE> : k_fft_cols<T, N, MODE>;
   cudaError_t e = prep_smem(kern, smem);
