@@ -238,7 +238,7 @@ struct ColRadix512f { static constexpr int ns = 2; static constexpr int r[3] = {
 template <typename T, int N, int MODE> struct ColSched {
   using S = Radix<N>;
   static constexpr int NT = fft_threads<N, 8>();
-  static constexpr int MINB = 2;
+  static constexpr int MINB = N >= 1024 ? 1 : 2;
 };
 #if MHIT_COL32_NT
 template <int MODE> struct ColSched<float, 512, MODE> {
@@ -248,13 +248,21 @@ template <int MODE> struct ColSched<float, 512, MODE> {
   static constexpr int MINB = Y ? 1024 / (2 * MHIT_COL32_NT) : 2;
 };
 #endif
+// The FP32 1024-point y passes (1024^3) in radix 32 x 32: two stages instead of three, one radix-32
+// butterfly per thread and stage (256 threads per 8-column tile, two tiles per SM).
+struct ColRadix1024f { static constexpr int ns = 2; static constexpr int r[3] = {32, 32, 0}; };
+template <int MODE> struct ColSched<float, 1024, MODE> {
+  static constexpr bool Y = MODE != 2;
+  using S = std::conditional_t<Y, ColRadix1024f, Radix<1024>>;
+  static constexpr int NT = Y ? 256 : fft_threads<1024, 8>();
+  static constexpr int MINB = Y ? 2 : 1;
+};
 
 template <typename T, int N, int MODE> struct ColTile {
   static constexpr bool Z64 = MODE == 2 && N == 512 && sizeof(T) == 8;
   static constexpr int B = Z64 ? 4 : 8;
   static constexpr int NT = Z64 ? fft_threads<N, 4>() : ColSched<T, N, MODE>::NT;
-  static constexpr int MINB =
-      Z64 ? 2 : ((N >= 1024 || (MODE == 2 && sizeof(T) == 8)) ? 1 : ColSched<T, N, MODE>::MINB);
+  static constexpr int MINB = Z64 ? 2 : ((MODE == 2 && sizeof(T) == 8) ? 1 : ColSched<T, N, MODE>::MINB);
   using S = typename ColSched<T, N, MODE>::S;
 };
 
