@@ -7,16 +7,18 @@
 //   1. fetches the plane's 8 half-spectrum rows (its 7 lines and the line below them, j0 - 1,
 //      the -y neighbour of its first line) with cp.async, two planes ahead, into a ring of three
 //      tile buffers in shared memory;
-//   2. C2R-transforms the 8 rows in place (the untangle of k_fftx_inv and Stockham stages in the
-//      XcRadix schedule: the on-demand transform of the same spectrum, k_fftx_inv with that
-//      schedule, gives the same doubles);
+//   2. C2R-transforms the 8 rows in place (the untangle and the Stockham stages of k_fftx_inv in
+//      the XcRadix schedule, so the on-demand transform of the same spectrum gives the same
+//      doubles);
 //   3. projects its 7 lines (u -= dt/rho (p - p(i-1)) dxi, and v, w along y, z: :953-955) with
 //      p(i-1) and p(j-1) from the tile and p(k-1) from registers that hold the pressure of the
 //      thread's own x pairs at the plane below (the loop starts one plane below the chunk for
 //      them), and accumulates the per-block sums and maxima of k_correct.
 // The warps are specialised so the two kinds of work overlap: the transform warps (steps 1-2,
 // synchronising among themselves on named barrier 1) transform plane i while the stream warps
-// (step 3: the u, v, w traffic, deep in loads) project plane i - 1.  A tile buffer passes between
+// (step 3: the u, v, w traffic) project plane i - 1.  At nx = 512 each stream thread stages its
+// u, v, w pairs of the next plane in shared memory by cp.async as it finishes each pair of the
+// current one, so a whole plane's loads are in flight without holding registers.  A tile buffer passes between
 // them by named barriers: "ready" (2 + buffer: transform warps arrive, stream warps wait) and
 // "free" (5 + buffer: stream warps arrive, transform warps wait before fetching plane i + 2 into
 // the buffer of plane i - 1).  Hardware barriers, no spin loops; every arrival has its matching
@@ -46,8 +48,16 @@ constexpr int XO = XL - 1;  // lines projected per plane: tile line 0 is the -y 
 constexpr int XZC_MIN = 8;  // fewest z planes per block of the default chunking
 constexpr int XNB = 3;      // tile buffers: loading, transforming, being projected
 
-// transform threads: one radix-8 butterfly each (at most 256: larger tiles loop), at least 64
-template <int M> __host__ __device__ constexpr int xc_nf() { return M >= 256 ? 256 : (M < 64 ? 64 : M); }
+// transform threads: one butterfly of the schedule's largest radix each (at most 256: larger tiles
+// loop), at least 64
+template <int M> __host__ __device__ constexpr int xc_maxr() {
+  int m = 0;
+  for (int s = 0; s < XcRadix<M>::ns; ++s) m = XcRadix<M>::r[s] > m ? XcRadix<M>::r[s] : m;
+  return m;
+}
+template <int M> __host__ __device__ constexpr int xc_nf() {
+  return M / xc_maxr<M>() * XL > 256 ? 256 : (M / xc_maxr<M>() * XL < 64 ? 64 : M / xc_maxr<M>() * XL);
+}
 // stream threads: 7 x pairs of the 7 lines each at nx = 512 (all their loads in flight at once:
 // ~86 KB per SM), 14 at nx = 1024
 template <int M> __host__ __device__ constexpr int xc_ns() { return M >= 256 ? 256 : 128; }
@@ -72,6 +82,19 @@ template <typename T, int M, bool INC> __host__ __device__ constexpr size_t xc_s
 template <typename T, int M, bool INC> __host__ __device__ constexpr int xc_pb() {
   return xc_pz_shared<T, M, INC>() ? 7 : 2;
 }
+// Where it fits as well (nx = 512), each stream thread stages its u, v, w pairs of the NEXT plane
+// in shared memory with cp.async, pair by pair as it finishes the current plane's pair (one
+// commit group per pair), so a whole plane's loads (~86 KB per SM) are in flight while the
+// current plane is projected and no registers hold them.
+template <typename T, int M, bool INC> __host__ __device__ constexpr size_t xc_uvw_bytes() {
+  return (size_t)3 * xc_ns<M>() * xc_ppt<M>() * 16;
+}
+template <typename T, int M, bool INC> __host__ __device__ constexpr bool xc_uvw_shared() {
+  return xc_pz_shared<T, M, INC>() && xc_smem<T, M, INC>() + xc_uvw_bytes<T, M, INC>() <= 227 * 1024;
+}
+template <typename T, int M, bool INC> __host__ __device__ constexpr size_t xc_smem_all() {
+  return xc_smem<T, M, INC>() + (xc_uvw_shared<T, M, INC>() ? xc_uvw_bytes<T, M, INC>() : 0);
+}
 
 __device__ __forceinline__ void bar_sync(int id, int count) {
   asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
@@ -88,6 +111,7 @@ __global__ void __launch_bounds__(xc_nf<M>() + xc_ns<M>(), 1) k_xinv_correct(con
   constexpr int PPT = xc_ppt<M>();         // ... per stream thread
   constexpr int XPB = xc_pb<T, M, INC>();
   constexpr bool PZS = xc_pz_shared<T, M, INC>();
+  constexpr bool UVS = xc_uvw_shared<T, M, INC>();
   constexpr int nx = 2 * M;
   constexpr int QL = XL * nx;              // floats of one predictor tile
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -170,33 +194,35 @@ __global__ void __launch_bounds__(xc_nf<M>() + xc_ns<M>(), 1) k_xinv_correct(con
       if constexpr (PZS) pzs[m * NS] = v;
       else pzr[m] = v;
     };
+    // staged u, v, w of pair m, field f: uvs[(f * PPT + m) * NS] (each thread its own slots)
+    double2* uvs = reinterpret_cast<double2*>(smraw + xc_smem<T, M, INC>()) + st;
+    // pair m of plane index ip into its slots, as one commit group (empty for pairs without a cell,
+    // and past the last plane, so every thread commits PPT groups per plane)
+    auto stage_pair = [&](int ip, int m) {
+      if constexpr (UVS) {
+        const int e = st + m * NS;
+        if (ip < nplanes && (NP % NS == 0 || e < NP)) {
+          const int l = e / M, n = e - l * M;
+          const int j = j0 + l;
+          if (j < ny) {
+            const size_t o = (size_t)(k0 - 1 + ip) * plane + (size_t)j * nx + 2 * n;  // ip >= 1: no wrap
+            __pipeline_memcpy_async(&uvs[(0 * PPT + m) * NS], U + o, 16);
+            __pipeline_memcpy_async(&uvs[(1 * PPT + m) * NS], V + o, 16);
+            __pipeline_memcpy_async(&uvs[(2 * PPT + m) * NS], W + o, 16);
+          }
+        }
+        __pipeline_commit();
+      }
+    };
     for (int i = 0; i < nplanes; ++i) {
       const Cx<T>* s = tiles + (i % XNB) * TL;
       const float* qs = qtiles + (i % XNB) * QL;
       const int k = k0 - 1 + i;
       const int kk = k < 0 ? k + nz : k;
       bar_sync(2 + i % XNB, NT);  // plane i's pressure (and predictor rows) are ready
+      if constexpr (UVS) {
 #pragma unroll
-      for (int m0 = 0; m0 < PPT; m0 += XPB) {
-        // the batch's loads first (u, v, w of up to XPB pairs in flight per thread), then the math
-        double2 uo[XPB], vo[XPB], wo[XPB];
-#pragma unroll
-        for (int mb = 0; mb < XPB && m0 + mb < PPT; ++mb) {
-          const int e = st + (m0 + mb) * NS;
-          if (NP % NS == 0 || e < NP) {
-            const int l = e / M, n = e - l * M;
-            const int j = j0 + l;
-            if (i > 0 && j < ny) {
-              const size_t o = (size_t)kk * plane + (size_t)j * nx + 2 * n;
-              uo[mb] = *reinterpret_cast<const double2*>(U + o);
-              vo[mb] = *reinterpret_cast<const double2*>(V + o);
-              wo[mb] = *reinterpret_cast<const double2*>(W + o);
-            }
-          }
-        }
-#pragma unroll
-        for (int mb = 0; mb < XPB && m0 + mb < PPT; ++mb) {
-          const int m = m0 + mb;
+        for (int m = 0; m < PPT; ++m) {
           const int e = st + m * NS;
           if (NP % NS == 0 || e < NP) {
             const int l = e / M, n = e - l * M;  // output line l = tile line l + 1
@@ -206,10 +232,10 @@ __global__ void __launch_bounds__(xc_nf<M>() + xc_ns<M>(), 1) k_xinv_correct(con
             const Cx<T> zy = s[sw<XL>(n, l)];
             double p0, p1, pxm, py0, py1;
             if constexpr (INC) {
-              // the sums k_fftx_inv forms for the FP64 pressure (same doubles), the predictor at the
-              // cell pair and its -x and -y neighbours from the tile's predictor rows
               const float2 qc = *reinterpret_cast<const float2*>(qs + (l + 1) * nx + 2 * n);
-              const float qx = qs[(l + 1) * nx + (n == 0 ? nx - 1 : 2 * n - 1)];
+              // the -x neighbour as the odd half of the aligned pair below (8-byte loads at an
+              // 8-byte stride: no bank conflict)
+              const float qx = reinterpret_cast<const float2*>(qs + (l + 1) * nx)[n == 0 ? M - 1 : n - 1].y;
               const float2 qy = *reinterpret_cast<const float2*>(qs + l * nx + 2 * n);
               p0 = (double)qc.x + (double)z.x;
               p1 = (double)qc.y + (double)z.y;
@@ -224,12 +250,16 @@ __global__ void __launch_bounds__(xc_nf<M>() + xc_ns<M>(), 1) k_xinv_correct(con
               py1 = (double)zy.y;
             }
             if (i > 0 && j < ny) {
+              // this pair's staged plane: every group but the newest PPT - 1 (the plane's later
+              // pairs, the next plane's earlier ones) is complete
+              __pipeline_wait_prior(PPT - 1);
+              const double2 uo = uvs[(0 * PPT + m) * NS], vo = uvs[(1 * PPT + m) * NS], wo = uvs[(2 * PPT + m) * NS];
               const size_t o = (size_t)kk * plane + (size_t)j * nx + 2 * n;
               // multi/main.f90:953-955, the expressions of k_correct
-              const double u0 = uo[mb].x - cc * (p0 - pxm) * dxi, u1 = uo[mb].y - cc * (p1 - p0) * dxi;
-              const double v0 = vo[mb].x - cc * (p0 - py0) * dxi, v1 = vo[mb].y - cc * (p1 - py1) * dxi;
+              const double u0 = uo.x - cc * (p0 - pxm) * dxi, u1 = uo.y - cc * (p1 - p0) * dxi;
+              const double v0 = vo.x - cc * (p0 - py0) * dxi, v1 = vo.y - cc * (p1 - py1) * dxi;
               const double2 pk = pz_get(m);
-              const double w0 = wo[mb].x - cc * (p0 - pk.x) * dxi, w1 = wo[mb].y - cc * (p1 - pk.y) * dxi;
+              const double w0 = wo.x - cc * (p0 - pk.x) * dxi, w1 = wo.y - cc * (p1 - pk.y) * dxi;
               *reinterpret_cast<double2*>(U + o) = make_double2(u0, u1);
               *reinterpret_cast<double2*>(V + o) = make_double2(v0, v1);
               *reinterpret_cast<double2*>(W + o) = make_double2(w0, w1);
@@ -243,11 +273,86 @@ __global__ void __launch_bounds__(xc_nf<M>() + xc_ns<M>(), 1) k_xinv_correct(con
             }
             pz_set(m, make_double2(p0, p1));
           }
+          // the slots are free (their values consumed above): the next plane's pair goes in
+          stage_pair(i + 1, m);
+        }
+      } else {
+#pragma unroll
+        for (int m0 = 0; m0 < PPT; m0 += XPB) {
+          // the batch's loads first (u, v, w of up to XPB pairs in flight per thread), then the math
+          double2 uo[XPB], vo[XPB], wo[XPB];
+#pragma unroll
+          for (int mb = 0; mb < XPB && m0 + mb < PPT; ++mb) {
+            const int e = st + (m0 + mb) * NS;
+            if (NP % NS == 0 || e < NP) {
+              const int l = e / M, n = e - l * M;
+              const int j = j0 + l;
+              if (i > 0 && j < ny) {
+                const size_t o = (size_t)kk * plane + (size_t)j * nx + 2 * n;
+                uo[mb] = *reinterpret_cast<const double2*>(U + o);
+                vo[mb] = *reinterpret_cast<const double2*>(V + o);
+                wo[mb] = *reinterpret_cast<const double2*>(W + o);
+              }
+            }
+          }
+#pragma unroll
+          for (int mb = 0; mb < XPB && m0 + mb < PPT; ++mb) {
+            const int m = m0 + mb;
+            const int e = st + m * NS;
+            if (NP % NS == 0 || e < NP) {
+              const int l = e / M, n = e - l * M;  // output line l = tile line l + 1
+              const int j = j0 + l;
+              const Cx<T> z = s[sw<XL>(n, l + 1)];
+              const T zxm = s[sw<XL>(n == 0 ? M - 1 : n - 1, l + 1)].y;
+              const Cx<T> zy = s[sw<XL>(n, l)];
+              double p0, p1, pxm, py0, py1;
+              if constexpr (INC) {
+                // the sums k_fftx_inv forms for the FP64 pressure (same doubles), the predictor at the
+                // cell pair and its -x and -y neighbours from the tile's predictor rows
+                const float2 qc = *reinterpret_cast<const float2*>(qs + (l + 1) * nx + 2 * n);
+                // the -x neighbour as the odd half of the aligned pair below (8-byte loads at an
+                // 8-byte stride: no bank conflict)
+                const float qx = reinterpret_cast<const float2*>(qs + (l + 1) * nx)[n == 0 ? M - 1 : n - 1].y;
+                const float2 qy = *reinterpret_cast<const float2*>(qs + l * nx + 2 * n);
+                p0 = (double)qc.x + (double)z.x;
+                p1 = (double)qc.y + (double)z.y;
+                pxm = (double)qx + (double)zxm;
+                py0 = (double)qy.x + (double)zy.x;
+                py1 = (double)qy.y + (double)zy.y;
+              } else {
+                p0 = (double)z.x;
+                p1 = (double)z.y;
+                pxm = (double)zxm;
+                py0 = (double)zy.x;
+                py1 = (double)zy.y;
+              }
+              if (i > 0 && j < ny) {
+                const size_t o = (size_t)kk * plane + (size_t)j * nx + 2 * n;
+                // multi/main.f90:953-955, the expressions of k_correct
+                const double u0 = uo[mb].x - cc * (p0 - pxm) * dxi, u1 = uo[mb].y - cc * (p1 - p0) * dxi;
+                const double v0 = vo[mb].x - cc * (p0 - py0) * dxi, v1 = vo[mb].y - cc * (p1 - py1) * dxi;
+                const double2 pk = pz_get(m);
+                const double w0 = wo[mb].x - cc * (p0 - pk.x) * dxi, w1 = wo[mb].y - cc * (p1 - pk.y) * dxi;
+                *reinterpret_cast<double2*>(U + o) = make_double2(u0, u1);
+                *reinterpret_cast<double2*>(V + o) = make_double2(v0, v1);
+                *reinterpret_cast<double2*>(W + o) = make_double2(w0, w1);
+                if constexpr (INC) *reinterpret_cast<float2*>(a.qnew + o) = make_float2((float)p0, (float)p1);
+                su += u0 + u1;
+                sv += v0 + v1;
+                sw_ += w0 + w1;
+                mu = fmax(mu, fmax(u0, u1));
+                mv = fmax(mv, fmax(v0, v1));
+                mw = fmax(mw, fmax(w0, w1));
+              }
+              pz_set(m, make_double2(p0, p1));
+            }
+          }
         }
       }
       // the transform warps wait for this buffer only if they fetch plane i + 3 into it
       if (i + 3 < nplanes) bar_arrive(5 + i % XNB, NT);
     }
+    if constexpr (UVS) __pipeline_wait_prior(0);  // no copy into the block's shared memory outlives it
   }
   // block reduction (fixed tree, as k_correct; the transform warps add the identities)
   __syncthreads();
@@ -300,9 +405,9 @@ static cudaError_t launch_xc_m(const XcArgs& a, cudaStream_t st) {
   constexpr int NT = xc_nf<M>() + xc_ns<M>();
   // the incremental solve is an FP32 mode: its variant exists for float tiles only
   constexpr bool HAS_INC = sizeof(T) == 4;
-  static_assert(xc_smem<T, M, false>() <= 227 * 1024 && (!HAS_INC || xc_smem<T, M, HAS_INC>() <= 227 * 1024),
+  static_assert(xc_smem_all<T, M, false>() <= 227 * 1024 && (!HAS_INC || xc_smem_all<T, M, HAS_INC>() <= 227 * 1024),
                 "tiles exceed the shared memory of a block");
-  const size_t smem = a.qold ? xc_smem<T, M, HAS_INC>() : xc_smem<T, M, false>();
+  const size_t smem = a.qold ? xc_smem_all<T, M, HAS_INC>() : xc_smem_all<T, M, false>();
   auto kern = a.qold ? k_xinv_correct<T, M, HAS_INC> : k_xinv_correct<T, M, false>;
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
