@@ -26,17 +26,6 @@ template <> struct Radix<256>  { static constexpr int ns = 2; static constexpr i
 template <> struct Radix<512>  { static constexpr int ns = 3; static constexpr int r[3] = {8, 8, 8}; };
 template <> struct Radix<1024> { static constexpr int ns = 3; static constexpr int r[3] = {8, 8, 16}; };
 
-// Schedule of the inverse x transforms fused with the projection (and of the pressure they
-// leave in the spectrum, transformed on demand with the same arithmetic).
-#ifndef MHIT_XC_SCHED16
-#define MHIT_XC_SCHED16 1
-#endif
-template <int N> struct XcRadix : Radix<N> {};
-#if !MHIT_XC_SCHED16
-template <> struct XcRadix<128> { static constexpr int ns = 3; static constexpr int r[3] = {8, 4, 4}; };
-template <> struct XcRadix<256> { static constexpr int ns = 3; static constexpr int r[3] = {8, 8, 4}; };
-#endif
-
 template <int N> __host__ __device__ constexpr int max_radix() {
   int m = 0;
   for (int s = 0; s < Radix<N>::ns; ++s) m = Radix<N>::r[s] > m ? Radix<N>::r[s] : m;

@@ -163,9 +163,7 @@ k_div_fftx(const double* __restrict__ u, const double* __restrict__ v, const dou
 // INC (incremental FP32 solve): the transform is the correction delta; with q the FP32 predictor
 // in `qin`, the pressure s = q + delta is formed in FP64 and written to `p64` (what the
 // projection reads), and fl32(s) to `qout` (the next step's predictor; skipped when null).
-// S: the radix schedule (XcRadix<M> for the pressure the fused projection left in the spectrum,
-// so it is transformed with the projection's arithmetic).
-template <typename T, int M, bool INC, typename S = Radix<M>>
+template <typename T, int M, bool INC>
 __global__ void __launch_bounds__(xpass_threads<T, M>())
 k_fftx_inv(const Cx<T>* __restrict__ spec, T* __restrict__ p, const Cx<T>* __restrict__ twx, Geo g,
            const float* __restrict__ qin, float* __restrict__ qout, double* __restrict__ p64) {
@@ -187,7 +185,7 @@ k_fftx_inv(const Cx<T>* __restrict__ spec, T* __restrict__ p, const Cx<T>* __res
   __syncthreads();
   c2r_untangle<T, M, B, NT>(s, twx);
   __syncthreads();
-  fft_tile<T, M, B, NT, true, S>(s, twx, 2);
+  fft_tile<T, M, B, NT, true>(s, twx, 2);
   for (int e = threadIdx.x; e < M * B; e += NT) {
     const int b = e / M, n = e - b * M;
     const int line = line0 + b;
@@ -228,26 +226,18 @@ k_fftx_inv(const Cx<T>* __restrict__ spec, T* __restrict__ p, const Cx<T>* __res
 // 256 threads, half of them idle in the 32-point stage: 0.237 / 0.246).  The z solve keeps
 // 8 x 8 x 8: 16 x 32 holds two transforms' registers across the divide and spills (0.63 against
 // 0.57 ms with 128 threads; 0.81 ms with 256, half of them idle in the 32-point stages).
-#ifndef MHIT_COL32_NT
-#define MHIT_COL32_NT 128
-#endif
-#ifndef MHIT_COL32_Z
-#define MHIT_COL32_Z 0
-#endif
 struct ColRadix512f { static constexpr int ns = 2; static constexpr int r[3] = {16, 32, 0}; };
 template <typename T, int N, int MODE> struct ColSched {
   using S = Radix<N>;
   static constexpr int NT = fft_threads<N, 8>();
   static constexpr int MINB = N >= 1024 ? 1 : 2;
 };
-#if MHIT_COL32_NT
 template <int MODE> struct ColSched<float, 512, MODE> {
-  static constexpr bool Y = MODE != 2 || MHIT_COL32_Z;
+  static constexpr bool Y = MODE != 2;
   using S = std::conditional_t<Y, ColRadix512f, Radix<512>>;
-  static constexpr int NT = Y ? MHIT_COL32_NT : fft_threads<512, 8>();
-  static constexpr int MINB = Y ? 1024 / (2 * MHIT_COL32_NT) : 2;
+  static constexpr int NT = Y ? 128 : fft_threads<512, 8>();
+  static constexpr int MINB = Y ? 4 : 2;
 };
-#endif
 // The FP32 1024-point y passes (1024^3) in radix 32 x 32: two stages instead of three, one radix-32
 // butterfly per thread and stage (256 threads per 8-column tile, two tiles per SM).
 struct ColRadix1024f { static constexpr int ns = 2; static constexpr int r[3] = {32, 32, 0}; };
@@ -420,8 +410,7 @@ template <typename T, int M>
 static cudaError_t launch_xinv_m(const PoissonArgs& a, cudaStream_t st) {
   constexpr int B = Tile<T>::B;
   const size_t smem = (size_t)(M + 1) * B * sizeof(Cx<T>);
-  auto kern = a.xc_sched ? (a.qin ? k_fftx_inv<T, M, true, XcRadix<M>> : k_fftx_inv<T, M, false, XcRadix<M>>)
-                         : (a.qin ? k_fftx_inv<T, M, true> : k_fftx_inv<T, M, false>);
+  auto kern = a.qin ? k_fftx_inv<T, M, true> : k_fftx_inv<T, M, false>;
   cudaError_t e = prep_smem(kern, smem);
   if (e != cudaSuccess) return e;
   const int nlines = a.g.ny * a.g.nz;

@@ -7,9 +7,8 @@
 //   1. fetches the plane's 8 half-spectrum rows (its 7 lines and the line below them, j0 - 1,
 //      the -y neighbour of its first line) with cp.async, two planes ahead, into a ring of three
 //      tile buffers in shared memory;
-//   2. C2R-transforms the 8 rows in place (the untangle and the Stockham stages of k_fftx_inv in
-//      the XcRadix schedule, so the on-demand transform of the same spectrum gives the same
-//      doubles);
+//   2. C2R-transforms the 8 rows in place (the untangle and the Stockham stages of k_fftx_inv, so
+//      the on-demand transform of the same spectrum gives the same doubles);
 //   3. projects its 7 lines (u -= dt/rho (p - p(i-1)) dxi, and v, w along y, z: :953-955) with
 //      p(i-1) and p(j-1) from the tile and p(k-1) from registers that hold the pressure of the
 //      thread's own x pairs at the plane below (the loop starts one plane below the chunk for
@@ -52,7 +51,7 @@ constexpr int XNB = 3;      // tile buffers: loading, transforming, being projec
 // loop), at least 64
 template <int M> __host__ __device__ constexpr int xc_maxr() {
   int m = 0;
-  for (int s = 0; s < XcRadix<M>::ns; ++s) m = XcRadix<M>::r[s] > m ? XcRadix<M>::r[s] : m;
+  for (int s = 0; s < Radix<M>::ns; ++s) m = Radix<M>::r[s] > m ? Radix<M>::r[s] : m;
   return m;
 }
 template <int M> __host__ __device__ constexpr int xc_nf() {
@@ -166,7 +165,7 @@ __global__ void __launch_bounds__(xc_nf<M>() + xc_ns<M>(), 1) k_xinv_correct(con
       bar_sync(1, NF);
       c2r_untangle<T, M, XL, NF>(s, twx);
       bar_sync(1, NF);
-      fft_tile<T, M, XL, NF, true, XcRadix<M>, SyncNamed<1, NF>>(s, twx, 2);
+      fft_tile<T, M, XL, NF, true, Radix<M>, SyncNamed<1, NF>>(s, twx, 2);
       bar_arrive(2 + i % XNB, NT);  // plane i's pressure is in its buffer
       if (i + 2 < nplanes) {
         // the buffer of plane i + 2 held plane i - 1: wait until the stream warps are done with it

@@ -45,7 +45,6 @@ struct PoissonArgs {
   float* qout = nullptr;
   double* p64 = nullptr;
   bool real64 = false;           // x-forward transforms the FP64 field u (energy spectrum)
-  bool xc_sched = false;         // x-inverse in the radix schedule of the fused projection
   const ZsolveTc* tcz = nullptr;  // non-null (FP32, nz = 512): the z solve runs on the tensor cores
   DevScalars* sc = nullptr;       // flag word for the tensor-core z solve's bounded waits
 };

@@ -398,7 +398,6 @@ static int materialise_pressure(mhit_ctx* c) {
   a.k2x = a.k2y = a.k2z = nullptr;
   a.cdiv = 0.0;
   a.ntot = (double)c->n;
-  a.xc_sched = true;  // the arithmetic of the fused pass: the pressure the projection used
   if (incremental(c)) {
     a.qin = c->Q[c->cur ^ 1];
     a.qout = nullptr;
