@@ -10,18 +10,18 @@
 //   2. C2R-transforms the 8 rows in place (the untangle and the Stockham stages of k_fftx_inv, so
 //      the on-demand transform of the same spectrum gives the same doubles);
 //   3. projects its 7 lines (u -= dt/rho (p - p(i-1)) dxi, and v, w along y, z: :953-955) with
-//      p(i-1) and p(j-1) from the tile and p(k-1) from registers that hold the pressure of the
-//      thread's own x pairs at the plane below (the loop starts one plane below the chunk for
-//      them), and accumulates the per-block sums and maxima of k_correct.
+//      p(i-1) and p(j-1) from the tile and p(k-1) carried by each thread for its own x pairs from
+//      the plane below (the loop starts one plane below the chunk for them), and accumulates the
+//      per-block sums and maxima of k_correct.
 // The warps are specialised so the two kinds of work overlap: the transform warps (steps 1-2,
 // synchronising among themselves on named barrier 1) transform plane i while the stream warps
 // (step 3: the u, v, w traffic) project plane i - 1.  At nx = 512 each stream thread stages its
 // u, v, w pairs of the next plane in shared memory by cp.async as it finishes each pair of the
-// current one, so a whole plane's loads are in flight without holding registers.  A tile buffer passes between
-// them by named barriers: "ready" (2 + buffer: transform warps arrive, stream warps wait) and
-// "free" (5 + buffer: stream warps arrive, transform warps wait before fetching plane i + 2 into
-// the buffer of plane i - 1).  Hardware barriers, no spin loops; every arrival has its matching
-// wait, and a barrier's next phase starts only after its last one completed.
+// current one, so a whole plane's loads are in flight without holding registers.  A tile buffer
+// passes between them by named barriers: "ready" (2 + buffer: transform warps arrive, stream
+// warps wait) and "free" (5 + buffer: stream warps arrive, transform warps wait before fetching
+// plane i + 2 into the buffer of plane i - 1).  Hardware barriers, no spin loops; every arrival
+// has its matching wait, and a barrier's next phase starts only after its last one completed.
 //
 // The pressure never goes to HBM: the library transforms it from the spectrum, which stays intact
 // until the next step's x pass, when something reads it.  Per cell this moves the spectrum once
@@ -57,8 +57,7 @@ template <int M> __host__ __device__ constexpr int xc_maxr() {
 template <int M> __host__ __device__ constexpr int xc_nf() {
   return M / xc_maxr<M>() * XL > 256 ? 256 : (M / xc_maxr<M>() * XL < 64 ? 64 : M / xc_maxr<M>() * XL);
 }
-// stream threads: 7 x pairs of the 7 lines each at nx = 512 (all their loads in flight at once:
-// ~86 KB per SM), 14 at nx = 1024
+// stream threads: 7 x pairs of the 7 lines each at nx = 512, 14 at nx = 1024
 template <int M> __host__ __device__ constexpr int xc_ns() { return M >= 256 ? 256 : 128; }
 template <int M> __host__ __device__ constexpr int xc_ppt() { return (XO * M + xc_ns<M>() - 1) / xc_ns<M>(); }
 template <typename T, int M> __host__ __device__ constexpr size_t xc_spec_bytes() {
@@ -69,15 +68,15 @@ template <typename T, int M, bool INC> __host__ __device__ constexpr size_t xc_t
   return xc_spec_bytes<T, M>() + (INC ? (size_t)XNB * XL * 2 * M * sizeof(float) : 0);
 }
 // The pressure each stream thread carries to the next plane (the -z neighbour) lives in shared
-// memory where it fits beside the tiles (in registers it would crowd out the loads in flight),
-// else in registers (FP64 at nx = 1024).
+// memory where it fits beside the tiles (in registers it would crowd out the loads), else in
+// registers (FP64 at nx = 1024).
 template <typename T, int M, bool INC> __host__ __device__ constexpr bool xc_pz_shared() {
   return xc_tile_bytes<T, M, INC>() + (size_t)xc_ns<M>() * xc_ppt<M>() * 16 <= 227 * 1024;
 }
 template <typename T, int M, bool INC> __host__ __device__ constexpr size_t xc_smem() {
   return xc_tile_bytes<T, M, INC>() + (xc_pz_shared<T, M, INC>() ? (size_t)xc_ns<M>() * xc_ppt<M>() * 16 : 0);
 }
-// x pairs a stream thread loads before computing any of them
+// where the loads go through registers: x pairs a stream thread loads before computing any of them
 template <typename T, int M, bool INC> __host__ __device__ constexpr int xc_pb() {
   return xc_pz_shared<T, M, INC>() ? 7 : 2;
 }
