@@ -299,7 +299,12 @@ k_fftx_inv(const Cx<T>* __restrict__ spec, T* __restrict__ p, const Cx<T>* __res
 // instead of two for 8 x 8 x 8: y passes 0.222 / 0.231 against 0.269 / 0.271 ms at 512^3 (with
 // 256 threads, half of them idle in the 32-point stage: 0.237 / 0.246).  The z solve keeps
 // 8 x 8 x 8: 16 x 32 holds two transforms' registers across the divide and spills (0.63 against
-// 0.57 ms with 128 threads; 0.81 ms with 256, half of them idle in the 32-point stages).
+// 0.57 ms with 128 threads; 0.81 ms with 256, half of them idle in the 32-point stages).  With
+// 128 threads and fewer blocks per SM it spills less and loses warps: three blocks (168
+// registers, 24 bytes spilled) 0.61 against 0.59 ms, two (201 registers, none spilled) 0.81 ms.
+// The 8 x 8 x 8 solve spills 88 bytes per thread at its 64-register bound and is still faster:
+// the pass needs the 32 warps per SM more than it loses to the spills.  The y passes at three
+// blocks per SM instead of four: no change.
 struct ColRadix512f { static constexpr int ns = 2; static constexpr int r[3] = {16, 32, 0}; };
 template <typename T, int N, int MODE> struct ColSched {
   using S = Radix<N>;
