@@ -275,11 +275,13 @@ __global__ void __launch_bounds__(PNT, PMINB) k_phase_batch(const __grid_constan
 }
 
 int phase_zchunk(const Geo& g, int requested) {
-  // Default chunk: 128 planes where that still leaves eight waves of one block on each of the
-  // 148 SMs (the four planes of warm-up below a chunk cost 3% instead of 6%: 2.667 against
-  // 2.723 ms at 512^3), otherwise PZC.  Results do not depend on the chunk.
+  // Default chunk: 256 planes where that still leaves six waves of one block on each of the 148
+  // SMs (the four planes of warm-up below a chunk cost 1.6%: 2.27 against 2.31 ms at 512^3 with
+  // 128 planes), else 128 planes where that leaves eight waves (3% instead of 6%: 2.667 against
+  // 2.723 ms at 512^3 with 64), otherwise PZC.  Results do not depend on the chunk.
   if (requested > 0) return requested;
   const long long cols = (long long)((g.nx + PTX - 1) / PTX) * ((g.ny + PTY - 1) / PTY);
+  if (cols * ((g.nz + 255) / 256) >= 6 * 148) return 256;
   return cols * ((g.nz + 127) / 128) >= 8 * 148 ? 128 : PZC;
 }
 

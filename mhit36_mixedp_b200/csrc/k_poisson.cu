@@ -36,6 +36,14 @@ template <> __device__ __forceinline__ void store2<float>(float* p, float a, flo
 
 // x-pass threads: one butterfly of the largest radix per thread (as the column passes)
 template <typename T, int M> __host__ __device__ constexpr int xpass_threads() { return fft_threads<M, Tile<T>::B>(); }
+// Resident blocks the forward x pass is compiled for (0: no bound).  The FP32 256-point pass
+// (nx = 512) asks for four blocks of 256 threads, which lets it use 64 registers instead of the
+// 48 / 56 it is given otherwise, at the same 32 warps per SM: the residual source (the
+// incremental solve's right-hand side) 0.90 against 0.96 ms at 512^3, the same bits; the
+// divergence source unchanged (0.71 ms).  Other lengths and FP64 keep the compiler's choice.
+template <typename T, int M> __host__ __device__ constexpr int xpass_minblocks() {
+  return (sizeof(T) == 4 && M == 256) ? 4 : 0;
+}
 
 // ------------------------------------------------------------------ forward x + divergence
 // SRC 0: the divergence of u*; SRC 2: the real FP64 field `u` (the energy spectrum of a
@@ -43,7 +51,7 @@ template <typename T, int M> __host__ __device__ constexpr int xpass_threads() {
 // `rr` (L_h the 7-point Laplacian, the operator whose symbol the modified divide uses), rounded
 // to FP32 -- the right-hand side of the refinement sweep and of the incremental solve.
 template <typename T, int M, int SRC>
-__global__ void __launch_bounds__(xpass_threads<T, M>())
+__global__ void __launch_bounds__(xpass_threads<T, M>(), xpass_minblocks<T, M>())
 k_div_fftx(const double* __restrict__ u, const double* __restrict__ v, const double* __restrict__ w,
            const float* __restrict__ rr, Cx<T>* __restrict__ spec, const Cx<T>* __restrict__ twx, Geo g,
            double cdiv) {

@@ -9,7 +9,7 @@ inputs:
 * the 256^3 NS+ACDI case (64 drops of radius 0.3 at seeded centres, eps = dx, We = 1,
   nu = 0.003, seeded solenoidal velocity), 20 steps;
 * the 512^3 benchmark workload itself (the same recipe at 512^3, ``acdi_clamp=1``), 3 steps,
-  which exercises the 128-plane ``k_phase`` chunk and the 64-plane ``k_mom`` / ``k_correct``
+  which exercises the 256-plane ``k_phase`` chunk and the 64-plane ``k_mom`` / ``k_correct``
   chunks that only grids of 512^3 and up select;
 * a 192^3 NS+ACDI box advanced inside an ensemble next to a 64^3 box (the radix-3 schedules of
   the ensemble configuration), 10 steps.
