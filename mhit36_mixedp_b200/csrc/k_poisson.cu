@@ -37,8 +37,9 @@ template <> __device__ __forceinline__ void store2<float>(float* p, float a, flo
 // x-pass threads: one butterfly of the largest radix per thread (as the column passes)
 template <typename T, int M> __host__ __device__ constexpr int xpass_threads() { return fft_threads<M, Tile<T>::B>(); }
 // Resident blocks the forward x pass is compiled for (0: no bound).  The FP32 256-point pass
-// (nx = 512) asks for four blocks of 256 threads, which lets it use 64 registers instead of the
-// 48 / 56 it is given otherwise, at the same 32 warps per SM: the residual source (the
+// (nx = 512) asks for four blocks of 256 threads, the residency its 33 KB tiles allow anyway,
+// which lets it use 64 registers instead of the 48 / 56 the compiler picks without the bound, at
+// the same 32 warps per SM: the residual source (the
 // incremental solve's right-hand side) 0.90 against 0.96 ms at 512^3, the same bits; the
 // divergence source unchanged (0.71 ms).  Other lengths and FP64 keep the compiler's choice.
 template <typename T, int M> __host__ __device__ constexpr int xpass_minblocks() {
